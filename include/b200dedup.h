@@ -1,0 +1,141 @@
+/*
+ * b200dedup.h -- C ABI of the B200 tree-approach incremental-checkpoint deduplicator.
+ *
+ * Drop-in for the reference's TreeDeduplicator (TauferLab/Reproducibility_ICPP23_Scalable_GPU_
+ * Deduplication, include/tree_approach.hpp:16-205 over include/deduplicator_interface.hpp:
+ * 14-184).  Plain pointers and sizes only; every call returns an int status (B2D_OK = 0,
+ * negative on error, see b2d_strerror) and no C++ exception crosses this boundary.
+ *
+ * Diff format (".hashtree.incr_chkpt", little endian; src/tree_approach.cpp:777-780):
+ *   header_t {u32 ref_id; u32 chkpt_id; u64 datalen; u32 chunk_size; u32 num_first_ocur;
+ *             u32 num_prior_chkpts; u32 num_shift_dupl}                 (include/utils.hpp:29-37)
+ *   u32 first-occurrence region root  x num_first_ocur
+ *   (u32 checkpoint id, u32 count)    x num_prior_chkpts
+ *   (u32 node, u32 source node)       x num_shift_dupl
+ *   chunk data of the first-occurrence regions
+ * The bytes are identical to the reference's output run sequentially (its parallel atomics
+ * only permute them).
+ *
+ * Threading: one handle per host thread; a handle is not thread-safe.  All device work of a
+ * handle runs on one CUDA stream (its own, or the one given to b2d_set_stream).  Device
+ * pointers passed in must belong to the current device.
+ */
+#ifndef B200DEDUP_H
+#define B200DEDUP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct b2d_dedup b2d_dedup;
+
+enum b2d_status {
+  B2D_OK = 0,
+  B2D_ERR_ARG = -1,            /* invalid argument */
+  B2D_ERR_CUDA = -2,           /* a CUDA runtime call failed */
+  B2D_ERR_NOMEM = -3,          /* device or host allocation failed */
+  B2D_ERR_FORMAT = -4,         /* a diff is truncated or its header is inconsistent */
+  B2D_ERR_IO = -5,             /* file open/read/write failed */
+  B2D_ERR_MAP_FULL = -6,       /* digest map probe sequence exhausted (should not happen) */
+  B2D_ERR_TIMEOUT = -7,        /* a bounded device wait gave up */
+  B2D_ERR_INTERNAL = -8,       /* an invariant of the algorithm did not hold */
+  B2D_ERR_RESTART_RANGE = -9,  /* restart met an index/offset outside its buffers (corrupt
+                                  diff, or the reference's non-power-of-two region quirk);
+                                  the offending copies were skipped */
+  B2D_ERR_LEN_CHANGED = -10,   /* buffer length changed without make_baseline */
+  B2D_ERR_UNSUPPORTED = -11    /* outside the supported range (e.g. > 8192 checkpoints per baseline) */
+};
+
+enum b2d_hash_kind {
+  B2D_HASH_MURMUR3 = 0, /* reference default: include/hash_functions.hpp:19 */
+  B2D_HASH_MD5 = 1      /* the commented alternative: include/hash_functions.hpp:18 */
+};
+
+/* TreeDeduplicator(uint32_t bytes_per_chunk) -- src/tree_approach.cpp:5-9.  The hash is a
+ * compile-time choice in the reference (include/hash_functions.hpp:16-20); here a parameter. */
+int b2d_create(uint32_t chunk_size, int hash_kind, b2d_dedup** out);
+/* ~TreeDeduplicator() -- src/tree_approach.cpp:11 */
+int b2d_destroy(b2d_dedup* d);
+/* Run all device work of this handle on `cuda_stream` (a cudaStream_t; NULL = the handle's
+ * own stream).  No reference counterpart (Kokkos uses its default execution space). */
+int b2d_set_stream(b2d_dedup* d, void* cuda_stream);
+
+/* checkpoint(header_t&, uint8_t* data_ptr, size_t len, HostMirror& diff_h, bool make_baseline)
+ * -- src/tree_approach.cpp:1577-1689, minus the device->host copy: the diff stays in device
+ * memory owned by the handle (b2d_diff_device / b2d_copy_diff).  advance_id != 0 also does the
+ * `current_id += 1` of the other overloads (:1723, :1747, :1775).  `d_data` is a device buffer
+ * of `len` bytes; it is only read. */
+int b2d_checkpoint_device(b2d_dedup* d, const void* d_data, uint64_t len, int make_baseline, int advance_id,
+                          uint64_t* diff_len);
+/* Device address and size of the last diff (valid until the next checkpoint on this handle). */
+int b2d_diff_device(b2d_dedup* d, const void** d_diff, uint64_t* diff_len);
+/* Copy the last diff to host memory `dst` of `cap` bytes (timers[3] of the reference). */
+int b2d_copy_diff(b2d_dedup* d, void* dst, uint64_t cap);
+
+/* checkpoint(uint8_t* data_ptr, size_t len, HostMirror& diff_h, bool make_baseline)
+ * -- src/tree_approach.cpp:1740-1748.  *diff points at pinned host memory owned by the handle,
+ * valid until the next call on it. */
+int b2d_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, int make_baseline, const uint8_t** diff,
+                   uint64_t* diff_len);
+/* checkpoint(uint8_t* data_ptr, size_t len, HostMirror& diff_h, std::string& logname,
+ * bool make_baseline) -- src/tree_approach.cpp:1765-1776 (writes the three CSV logs). */
+int b2d_checkpoint_log(b2d_dedup* d, const void* d_data, uint64_t len, const char* logname, int make_baseline,
+                       const uint8_t** diff, uint64_t* diff_len);
+/* checkpoint(uint8_t* data_ptr, size_t len, std::string& filename, std::string& logname,
+ * bool make_baseline) -- src/tree_approach.cpp:1705-1724 (diff written to `filename`). */
+int b2d_checkpoint_file(b2d_dedup* d, const void* d_data, uint64_t len, const char* filename, const char* logname,
+                        int make_baseline);
+
+/* restart(uint8_t* data_ptr, size_t len, vector<HostMirror>& chkpts, std::string& logname,
+ * uint32_t chkpt_id) -- src/tree_approach.cpp:1807-1813 -> restart_chkpt :712-1128.
+ * Rebuilds checkpoint `chkpt_id` into the device buffer `d_out` (len >= the header's datalen;
+ * datalen bytes are written, the rest untouched) from host diffs[0..num_diffs).  `logname`
+ * may be NULL (no restart log). */
+int b2d_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* diffs, const uint64_t* sizes,
+                uint32_t num_diffs, uint32_t chkpt_id, const char* logname);
+/* restart(View data, vector<string>& chkpt_filenames, std::string& logname, uint32_t chkpt_id)
+ * -- src/tree_approach.cpp:1827-1838: reads "<name>.hashtree.incr_chkpt" for each name.
+ * Offsets are 64-bit (the host-view semantics); the reference's file path computes them in
+ * 32 bits (:1265-1290) and breaks above 4 GiB. */
+int b2d_restart_files(b2d_dedup* d, void* d_out, uint64_t len, const char* const* chkpt_filenames,
+                      uint32_t num_files, uint32_t chkpt_id, const char* logname);
+
+/* num_first_ocur() / num_shift_dupl() -- include/tree_approach.hpp:53-59 */
+int b2d_num_first_ocur(b2d_dedup* d, uint64_t* out);
+int b2d_num_shift_dupl(b2d_dedup* d, uint64_t* out);
+/* BaseDeduplicator state (include/deduplicator_interface.hpp:16-23) */
+int b2d_current_id(b2d_dedup* d, uint32_t* out);
+int b2d_baseline_id(b2d_dedup* d, uint32_t* out);
+/* timers[4]: setup, comparison (dedup), gather, copy diff to host -- seconds */
+int b2d_timers(b2d_dedup* d, double out[4]);
+/* restart_timers[2]: copy time, total restart time -- seconds */
+int b2d_restart_timers(b2d_dedup* d, double out[2]);
+/* datasizes: (data bytes incl. header, metadata bytes) of the last diff (:707-709) */
+int b2d_datasizes(b2d_dedup* d, uint64_t out[2]);
+/* Device time (seconds, CUDA events on the handle's stream) of the last checkpoint's three
+ * stages: chunk hashing + labelling, Merkle forest, diff assembly.  *leaf_path (nullable) is 1
+ * when the TMA-staged hashing kernel ran, 0 for the byte-granular one.  No reference
+ * counterpart (the reference times whole phases on the host, src/tree_approach.cpp:1640-1688). */
+int b2d_phase_times(b2d_dedup* d, double out[3], int* leaf_path);
+/* device kernels launched by the last checkpoint/restart call on this handle */
+int b2d_last_launch_count(b2d_dedup* d, uint32_t* out);
+
+/* Introspection for tests: copy `nodes` tree digests (16 B each) / labels (1 B each) of the
+ * last checkpoint to host memory. */
+int b2d_debug_tree(b2d_dedup* d, void* dst, uint64_t nodes);
+int b2d_debug_labels(b2d_dedup* d, void* dst, uint64_t nodes);
+/* Digest of each `chunk_size` chunk of a device buffer into d_out (16 B per chunk), the
+ * reference's hash() (include/hash_functions.hpp:16-20) as a standalone kernel. */
+int b2d_hash_chunks(int hash_kind, const void* d_data, uint64_t len, uint32_t chunk_size, void* d_out,
+                    void* cuda_stream);
+
+const char* b2d_strerror(int status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B200DEDUP_H */

@@ -1,0 +1,394 @@
+// Diff assembly on the device: the reference's collect_diff (src/tree_approach.cpp:511-710).
+//
+// Output order is the reference's sequential order (what its atomics produce with one
+// thread): region roots by (level descending, node ascending); the repeat table by
+// checkpoint id; shifted-duplicate entries stably bucketed by source checkpoint.
+//   1. compaction of the push flags in that canonical order (reduce-then-scan, 3 launches)
+//   2. first-occurrence region sizes -> exclusive chunk offsets (3 launches)
+//   3. shift entries: source NodeID lookup + per-CTA histograms (1 launch)
+//   4. layout: bucket starts, repeat table, header, byte offsets (1 launch, 1 CTA)
+//   5. stable bucket scatter of the shift entries (1 launch, one warp per range)
+//   6. first-occurrence metadata + 16-byte vectorised chunk gather (1 launch)
+// Diff layout (include/utils.hpp:29-37, src/tree_approach.cpp:777-780):
+//   [header 32 B][u32 first node x F][(u32 ckpt, u32 count) x P][(u32 node, u32 prev) x S][data]
+// It is placed `delta` bytes into the device buffer so the data section is 16-byte aligned.
+#include "dedup_kernels.cuh"
+#include "map.cuh"
+#include "scan.cuh"
+
+namespace b2d {
+
+constexpr uint32_t COMPACT_THREADS = 512;
+constexpr uint32_t SHIFT_GRID = 1184;   // 8 x 148 ranges for the shift-entry passes
+
+// node at canonical position p: level D (possibly partial) first, then full levels D-1..0
+__device__ __forceinline__ uint32_t canon_node(uint64_t p, uint32_t N, uint32_t D) {
+  const uint64_t first_deep = (1ull << D) - 1ull;
+  const uint64_t cnt_deep = (uint64_t)N - first_deep;
+  if (p < cnt_deep) return (uint32_t)(first_deep + p);
+  const uint64_t q = p - cnt_deep;
+  const uint64_t s = (1ull << D) - q;   // >= 2
+  const uint32_t L = 63u - (uint32_t)__clzll((long long)(s - 1ull));
+  return (uint32_t)(((1ull << L) - 1ull) + (q - ((1ull << D) - (1ull << (L + 1)))));
+}
+
+__global__ void __launch_bounds__(COMPACT_THREADS) compact_count_kernel(DiffArgs a) {
+  __shared__ uint32_t sh[COMPACT_THREADS / 32 + 1];
+  uint64_t beg, end;
+  cta_range(a.N, blockIdx.x, gridDim.x, beg, end);
+  uint32_t cf = 0, cs = 0;
+  for (uint64_t p = beg + threadIdx.x; p < end; p += blockDim.x) {
+    const uint8_t f = a.push[canon_node(p, a.N, a.D)];
+    cf += f == PUSH_FIRST;
+    cs += f == PUSH_SHIFT;
+  }
+  const uint32_t tf = block_reduce_sum(cf, sh);
+  const uint32_t ts = block_reduce_sum(cs, sh);
+  if (threadIdx.x == 0) {
+    a.partial2[2 * blockIdx.x] = tf;
+    a.partial2[2 * blockIdx.x + 1] = ts;
+  }
+}
+
+__global__ void __launch_bounds__(1024) compact_scan_kernel(DiffArgs a, uint32_t g) {
+  __shared__ uint32_t sh[33];
+  uint32_t tf, ts;
+  const uint32_t i = threadIdx.x;
+  const uint32_t vf = i < g ? a.partial2[2 * i] : 0u, vs = i < g ? a.partial2[2 * i + 1] : 0u;
+  const uint32_t ef = block_excl_scan(vf, sh, &tf);
+  const uint32_t es = block_excl_scan(vs, sh, &ts);
+  if (i < g) {
+    a.partial2[2 * i] = ef;
+    a.partial2[2 * i + 1] = es;
+  }
+  if (i == 0) {
+    a.meta->F = tf;
+    a.meta->S = ts;
+  }
+}
+
+__global__ void __launch_bounds__(COMPACT_THREADS) compact_write_kernel(DiffArgs a) {
+  __shared__ uint32_t sh[COMPACT_THREADS / 32 + 1];
+  uint64_t beg, end;
+  cta_range(a.N, blockIdx.x, gridDim.x, beg, end);
+  uint32_t bf = a.partial2[2 * blockIdx.x], bs = a.partial2[2 * blockIdx.x + 1];
+  for (uint64_t t0 = beg; t0 < end; t0 += blockDim.x) {
+    const uint64_t p = t0 + threadIdx.x;
+    uint32_t node = 0;
+    uint8_t f = PUSH_NONE;
+    if (p < end) {
+      node = canon_node(p, a.N, a.D);
+      f = a.push[node];
+    }
+    uint32_t tf, ts;
+    const uint32_t rf = block_excl_scan(f == PUSH_FIRST, sh, &tf);
+    const uint32_t rs = block_excl_scan(f == PUSH_SHIFT, sh, &ts);
+    if (f == PUSH_FIRST) a.first_list[bf + rf] = node;
+    if (f == PUSH_SHIFT) a.shift_list[bs + rs] = node;
+    bf += tf;
+    bs += ts;
+  }
+}
+
+// ---------------------------------------------------------------- region sizes and offsets
+__global__ void __launch_bounds__(COMPACT_THREADS) region_count_kernel(DiffArgs a) {
+  __shared__ uint32_t sh[COMPACT_THREADS / 32 + 1];
+  uint64_t beg, end;
+  cta_range(a.meta->F, blockIdx.x, gridDim.x, beg, end);
+  uint32_t c = 0;
+  for (uint64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
+    const uint32_t node = a.first_list[i];
+    c += num_leaf_descendents(node, a.N);
+    // collect_diff keeps a first-occurrence region only when the map names it as the
+    // owner of its digest (:548-556); the labelling guarantees it, so check it here
+    const uint64_t slot = map_find(a.map, a.tree[node]);
+    if (slot > a.map.cap || map_node(a.map, slot) != node || map_tree(a.map, slot) != a.cur)
+      set_error(a.st, DERR_INTERNAL, 20);
+  }
+  const uint32_t t = block_reduce_sum(c, sh);
+  if (threadIdx.x == 0) a.partial2[blockIdx.x] = t;
+}
+
+__global__ void __launch_bounds__(1024) region_scan_kernel(DiffArgs a, uint32_t g) {
+  __shared__ uint32_t sh[33];
+  uint32_t tot;
+  const uint32_t i = threadIdx.x;
+  const uint32_t v = i < g ? a.partial2[i] : 0u;
+  const uint32_t e = block_excl_scan(v, sh, &tot);
+  if (i < g) a.partial2[i] = e;
+  if (i == 0) a.meta->T = tot;
+}
+
+__global__ void __launch_bounds__(COMPACT_THREADS) region_write_kernel(DiffArgs a) {
+  __shared__ uint32_t sh[COMPACT_THREADS / 32 + 1];
+  uint64_t beg, end;
+  cta_range(a.meta->F, blockIdx.x, gridDim.x, beg, end);
+  uint32_t base = a.partial2[blockIdx.x];
+  for (uint64_t t0 = beg; t0 < end; t0 += blockDim.x) {
+    const uint64_t i = t0 + threadIdx.x;
+    const uint32_t len = i < end ? num_leaf_descendents(a.first_list[i], a.N) : 0u;
+    uint32_t tot;
+    const uint32_t e = block_excl_scan(len, sh, &tot);
+    if (i < end) a.region_off[i] = base + e;
+    base += tot;
+  }
+}
+
+// ---------------------------------------------------------------- shifted duplicates
+// source NodeID of each entry (:572-580, :672-674) and per-range histograms by checkpoint
+__global__ void __launch_bounds__(128) shift_prev_kernel(DiffArgs a, uint32_t B) {
+  extern __shared__ uint32_t hs[];
+  uint64_t beg, end;
+  cta_range(a.meta->S, blockIdx.x, gridDim.x, beg, end);
+  for (uint32_t t = threadIdx.x; t < B; t += blockDim.x) hs[t] = 0;
+  __syncthreads();
+  for (uint64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
+    const uint32_t node = a.shift_list[i];
+    const uint64_t slot = map_find(a.map, a.tree[node]);
+    uint32_t pn = 0, pt = 0;
+    if (slot <= a.map.cap) {
+      pn = map_node(a.map, slot);
+      pt = map_tree(a.map, slot);
+    } else {
+      set_error(a.st, DERR_INTERNAL, 30);
+    }
+    if (pt >= B) {
+      set_error(a.st, DERR_INTERNAL, 31);
+      pt = 0;
+    }
+    a.sprev[i] = pn;
+    a.skey[i] = pt;
+    atomicAdd(&hs[pt], 1u);
+  }
+  __syncthreads();
+  for (uint32_t t = threadIdx.x; t < B; t += blockDim.x) {
+    const uint32_t v = hs[t];
+    a.partial[(uint64_t)t * gridDim.x + blockIdx.x] = v;
+    if (v) atomicAdd(&a.hist[t], v);
+  }
+}
+
+// one CTA: bucket starts, repeat table, per-range scatter bases, header, byte layout
+__global__ void __launch_bounds__(1024) layout_kernel(DiffArgs a, uint32_t B, uint32_t g) {
+  __shared__ uint32_t sh[33];
+  __shared__ uint32_t carry_start, carry_rows;
+  if (threadIdx.x == 0) { carry_start = 0; carry_rows = 0; }
+  __syncthreads();
+  const DevMeta m0 = *a.meta;
+  // count P first so the table position is known
+  for (uint32_t t0 = 0; t0 < B; t0 += blockDim.x) {
+    const uint32_t t = t0 + threadIdx.x;
+    const uint32_t h = t < B ? a.hist[t] : 0u;
+    uint32_t tot_h, tot_r;
+    const uint32_t eh = block_excl_scan(h, sh, &tot_h);
+    const uint32_t er = block_excl_scan(h ? 1u : 0u, sh, &tot_r);
+    if (t < B) a.bucket_start[t] = carry_start + eh;
+    __syncthreads();
+    if (threadIdx.x == 0) { carry_start += tot_h; carry_rows += tot_r; }
+    __syncthreads();
+    (void)er;
+  }
+  const uint32_t P = carry_rows;
+  const uint64_t F = m0.F, S = m0.S, T = m0.T;
+  const uint64_t meta_bytes = 4 * F + 8 * (uint64_t)P + 8 * S;
+  const uint32_t delta = (uint32_t)((16u - ((32u + meta_bytes) & 15u)) & 15u);
+  const uint64_t first_off = delta + 32ull;
+  const uint64_t count_off = first_off + 4 * F;
+  const uint64_t shift_off = count_off + 8ull * P;
+  const uint64_t data_off = shift_off + 8 * S;
+  // repeat table rows (ckpt id, count) in ascending id order (:656-665)
+  __shared__ uint32_t row_carry;
+  if (threadIdx.x == 0) row_carry = 0;
+  __syncthreads();
+  for (uint32_t t0 = 0; t0 < B; t0 += blockDim.x) {
+    const uint32_t t = t0 + threadIdx.x;
+    const uint32_t h = t < B ? a.hist[t] : 0u;
+    uint32_t tot_r;
+    const uint32_t er = block_excl_scan(h ? 1u : 0u, sh, &tot_r);
+    if (h) {
+      uint32_t* row = reinterpret_cast<uint32_t*>(a.diff + count_off + 8ull * (row_carry + er));
+      row[0] = t;
+      row[1] = h;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) row_carry += tot_r;
+    __syncthreads();
+  }
+  // per-range scatter bases: bucket start + counts of earlier ranges.  `partial` is
+  // bucket-major (partial[t * g + range]); one warp scans one bucket's g range counts.
+  {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (uint32_t t = warp; t < B; t += nw) {
+      uint32_t carry = a.bucket_start[t];
+      uint32_t* row = a.partial + (uint64_t)t * g;
+#pragma unroll 4
+      for (uint32_t j = 0; j < g; j += 32) {
+        const uint32_t b = j + lane;
+        const uint32_t v = b < g ? row[b] : 0u;
+        const uint32_t inc = warp_incl_scan(v);
+        if (b < g) row[b] = carry + inc - v;
+        carry += __shfl_sync(0xffffffffu, inc, 31);
+      }
+    }
+  }
+  if (threadIdx.x == 0) {
+    uint32_t* h32 = reinterpret_cast<uint32_t*>(a.diff + delta);
+    h32[0] = a.baseline_id;                 // ref_id
+    h32[1] = a.cur;                         // chkpt_id
+    h32[2] = (uint32_t)a.len;               // datalen (u64, little endian)
+    h32[3] = (uint32_t)(a.len >> 32);
+    h32[4] = a.cs;                          // chunk_size
+    h32[5] = (uint32_t)F;                   // num_first_ocur
+    h32[6] = P;                             // num_prior_chkpts
+    h32[7] = (uint32_t)S;                   // num_shift_dupl
+    DevMeta* m = a.meta;
+    m->P = P;
+    m->delta = delta;
+    m->first_off = first_off;
+    m->count_off = count_off;
+    m->shift_off = shift_off;
+    m->data_off = data_off;
+    m->diff_len = 32ull + meta_bytes + T * a.cs;
+    m->map_size = *a.map.size;
+  }
+}
+
+// stable scatter of shift entries: one warp walks its range in order
+__global__ void __launch_bounds__(32) shift_write_kernel(DiffArgs a, uint32_t B) {
+  extern __shared__ uint32_t run[];
+  uint64_t beg, end;
+  cta_range(a.meta->S, blockIdx.x, gridDim.x, beg, end);
+  if (beg >= end) return;
+  for (uint32_t t = threadIdx.x; t < B; t += 32) run[t] = a.partial[(uint64_t)t * gridDim.x + blockIdx.x];
+  __syncwarp();
+  const uint64_t shift_off = a.meta->shift_off;
+  const uint32_t lane = threadIdx.x;
+  for (uint64_t t0 = beg; t0 < end; t0 += 32) {
+    const uint64_t i = t0 + lane;
+    const bool act = i < end;
+    const uint32_t key = act ? a.skey[i] : 0xffffffffu;
+    const uint32_t peers = __match_any_sync(0xffffffffu, key);
+    const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+    uint32_t pos = 0;
+    if (act) pos = run[key] + rank;
+    __syncwarp();
+    if (act && rank == 0) run[key] += __popc(peers);
+    __syncwarp();
+    if (act) {
+      uint32_t* e = reinterpret_cast<uint32_t*>(a.diff + shift_off + 8ull * pos);
+      e[0] = a.shift_list[i];
+      e[1] = a.sprev[i];
+    }
+  }
+}
+
+// ---------------------------------------------------------------- metadata + data gather
+__device__ __forceinline__ uint32_t find_region(const uint32_t* off, uint32_t F, uint64_t k) {
+  uint32_t lo = 0, hi = F;   // largest i with off[i] <= k
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (off[mid] <= k) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// LPC lanes copy one chunk with 16-byte vectors (chunk size a multiple of 16, 16-byte
+// aligned source and destination); the short last chunk is zero-padded (:643-645).
+template <uint32_t LPC>
+__global__ void __launch_bounds__(256) gather_vec_kernel(DiffArgs a) {
+  const DevMeta m = *a.meta;
+  uint8_t* dst_base = a.diff + m.data_off;
+  uint32_t* first_meta = reinterpret_cast<uint32_t*>(a.diff + m.first_off);
+  const uint64_t gtid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t nthr = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = gtid; i < m.F; i += nthr) first_meta[i] = a.first_list[i];
+  const uint32_t units = a.cs / 16u;
+  const uint64_t group = gtid / LPC, ngroups = nthr / LPC;
+  const uint32_t sub = (uint32_t)(gtid % LPC);
+  for (uint64_t k = group; k < m.T; k += ngroups) {
+    const uint32_t r = find_region(a.region_off, m.F, k);
+    const uint32_t node = a.first_list[r];
+    const uint64_t chunk = (uint64_t)(leftmost_leaf(node, a.N) - (a.n - 1u)) + (k - a.region_off[r]);
+    if (chunk >= a.n) { set_error(a.st, DERR_INTERNAL, 40); continue; }
+    const uint64_t src_off = chunk * a.cs;
+    const uint4* src = reinterpret_cast<const uint4*>(a.data + src_off);
+    uint4* dst = reinterpret_cast<uint4*>(dst_base + k * a.cs);
+    const uint64_t avail = (chunk == a.n - 1u) ? a.len - src_off : a.cs;
+    if (avail == a.cs) {
+      for (uint32_t u = sub; u < units; u += LPC) dst[u] = __ldg(src + u);
+    } else {
+      const uint32_t full = (uint32_t)(avail / 16u);
+      for (uint32_t u = sub; u < units; u += LPC) {
+        if (u < full) {
+          dst[u] = __ldg(src + u);
+        } else {
+          uint8_t tmp[16];
+          const uint8_t* s8 = a.data + src_off + 16ull * u;
+          for (uint32_t b = 0; b < 16; b++) tmp[b] = (16ull * u + b < avail) ? s8[b] : 0u;
+          uint4 v;
+          memcpy(&v, tmp, 16);
+          dst[u] = v;
+        }
+      }
+    }
+  }
+}
+
+// any chunk size / alignment: one thread per chunk, byte copies
+__global__ void __launch_bounds__(256) gather_bytes_kernel(DiffArgs a) {
+  const DevMeta m = *a.meta;
+  uint8_t* dst_base = a.diff + m.data_off;
+  uint8_t* first_meta = a.diff + m.first_off;
+  const uint64_t gtid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t nthr = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = gtid; i < m.F; i += nthr) {
+    const uint32_t v = a.first_list[i];
+    memcpy(first_meta + 4 * i, &v, 4);
+  }
+  for (uint64_t k = gtid; k < m.T; k += nthr) {
+    const uint32_t r = find_region(a.region_off, m.F, k);
+    const uint32_t node = a.first_list[r];
+    const uint64_t chunk = (uint64_t)(leftmost_leaf(node, a.N) - (a.n - 1u)) + (k - a.region_off[r]);
+    if (chunk >= a.n) { set_error(a.st, DERR_INTERNAL, 41); continue; }
+    const uint64_t src_off = chunk * a.cs;
+    const uint64_t avail = (chunk == a.n - 1u) ? a.len - src_off : a.cs;
+    uint8_t* d = dst_base + k * a.cs;
+    const uint8_t* s = a.data + src_off;
+    for (uint64_t b = 0; b < a.cs; b++) d[b] = b < avail ? s[b] : 0u;
+  }
+}
+
+cudaError_t launch_collect_diff(const DiffArgs& a, int sm_count, cudaStream_t stream) {
+  const uint32_t g = SCAN_GRID;
+  const uint32_t B = a.cur + 1u;
+  if (B > MAX_BUCKETS) return cudaErrorInvalidValue;
+  compact_count_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);
+  compact_scan_kernel<<<1, 1024, 0, stream>>>(a, g);
+  compact_write_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);
+  region_count_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);
+  region_scan_kernel<<<1, 1024, 0, stream>>>(a, g);
+  region_write_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);
+  cudaError_t e = cudaMemsetAsync(a.hist, 0, sizeof(uint32_t) * B, stream);
+  if (e != cudaSuccess) return e;
+  const size_t hsm = sizeof(uint32_t) * B;   // <= 32 KB for MAX_BUCKETS
+  shift_prev_kernel<<<SHIFT_GRID, 128, hsm, stream>>>(a, B);
+  layout_kernel<<<1, 1024, 0, stream>>>(a, B, SHIFT_GRID);
+  shift_write_kernel<<<SHIFT_GRID, 32, hsm, stream>>>(a, B);
+  const uint32_t gblocks = (uint32_t)sm_count * 4u;
+  const bool vec = (a.cs % 16u == 0) && ((reinterpret_cast<uintptr_t>(a.data) & 15u) == 0) &&
+                   ((reinterpret_cast<uintptr_t>(a.diff) & 15u) == 0);
+  if (vec) {
+    const uint32_t units = a.cs / 16u;
+    if (units >= 32) gather_vec_kernel<32><<<gblocks, 256, 0, stream>>>(a);
+    else if (units >= 16) gather_vec_kernel<16><<<gblocks, 256, 0, stream>>>(a);
+    else if (units >= 8) gather_vec_kernel<8><<<gblocks, 256, 0, stream>>>(a);
+    else if (units >= 4) gather_vec_kernel<4><<<gblocks, 256, 0, stream>>>(a);
+    else if (units >= 2) gather_vec_kernel<2><<<gblocks, 256, 0, stream>>>(a);
+    else gather_vec_kernel<1><<<gblocks, 256, 0, stream>>>(a);
+  } else {
+    gather_bytes_kernel<<<gblocks, 256, 0, stream>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace b2d

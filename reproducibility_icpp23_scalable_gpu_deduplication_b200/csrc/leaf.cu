@@ -1,0 +1,323 @@
+// Leaf stage: hash every chunk, label it FIXED / FIRST / SHIFT against the prior checkpoint,
+// record first occurrences in the digest map.
+//
+// Restates the reference's "Leaves" kernels (src/tree_approach.cpp:54-94 baseline,
+// :305-351 incremental).  Two implementations share the per-leaf decision (leaf_finish):
+//   * leaf_tma_kernel: persistent, warp-specialised.  One producer warp streams the buffer
+//     into shared memory with TMA tensor copies (cp.async.bulk.tensor, 128/64/32-byte
+//     swizzle so each lane's chunk row is read without bank conflicts) through an mbarrier
+//     ring; eight consumer warps hash one chunk per lane.  Used when the chunk size is a
+//     multiple of 16 bytes (MD5: 64) and the buffer is 16-byte aligned.
+//   * leaf_generic_kernel: one thread per chunk with byte-granular loads, for any chunk
+//     size or alignment, and for the short last chunk.
+#include <cuda.h>
+#include "dedup_kernels.cuh"
+#include "hash.cuh"
+#include "map.cuh"
+
+namespace b2d {
+
+// Per-leaf decision, same order of tests as the reference:
+//  baseline:    insert, then compare with the (fresh, all-zero) tree entry
+//  incremental: compare with the prior digest first; FIXED leaves skip the insert because
+//               their digest is already present from the checkpoint that stored it.
+__device__ __forceinline__ void leaf_finish(const LeafArgs& a, uint32_t chunk, const Digest& d) {
+  const uint32_t leaf = a.n - 1u + chunk;
+  uint8_t label = DONE;
+  if (a.baseline) {
+    const MapRef r = map_insert(a.map, d, (unsigned long long)leaf, a.cur, a.st);
+    if (digest_zero(d)) label = FIXED_DUPL;
+    else if (r.inserted) label = FIRST_OCUR;
+    else if (r.found) label = map_merge_current(a.map, r.slot, leaf, a.cur) ? FIRST_OCUR : SHIFT_DUPL;
+    a.tree[leaf] = d;
+  } else {
+    const Digest old = a.tree[leaf];
+    if (digest_eq(d, old)) {
+      label = FIXED_DUPL;
+    } else {
+      const MapRef r = map_insert(a.map, d, (unsigned long long)leaf, a.cur, a.st);
+      if (r.inserted) {
+        label = FIRST_OCUR;
+        a.tree[leaf] = d;
+      } else if (r.found) {
+        label = map_merge_current(a.map, r.slot, leaf, a.cur) ? FIRST_OCUR : SHIFT_DUPL;
+        a.tree[leaf] = d;
+      }
+    }
+  }
+  a.lab[leaf] = label;
+}
+
+__global__ void leaf_generic_kernel(LeafArgs a, uint32_t c_begin, uint32_t c_end) {
+  for (uint64_t c = (uint64_t)c_begin + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < c_end;
+       c += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t off = c * a.cs;
+    const uint64_t nb = (c == a.n - 1u) ? a.len - off : a.cs;
+    const Digest d = hash_bytes(a.kind, a.data + off, nb);
+    leaf_finish(a, (uint32_t)c, d);
+  }
+}
+
+// ------------------------------------------------------------------ PTX helpers (sm_90+)
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: gives up after `limit` polls (each try_wait may suspend for a while in
+// hardware), records the timeout and returns false.  Never spins forever.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, DevStatus* st,
+                                                  volatile int* abort_flag) {
+  const uint32_t limit = 1u << 24;
+  for (uint32_t i = 0; i < limit; i++) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 1023u) == 1023u && *abort_flag) return false;
+  }
+  set_error(st, DERR_WAIT_TIMEOUT, 1);
+  *abort_flag = 1;
+  return false;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1,
+                                            int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], "
+      "[%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+
+// physical shared-memory offset of logical byte offset `o` under the tensor map's swizzle
+template <int U>
+__device__ __forceinline__ uint32_t swz(uint32_t o) {
+  if constexpr (U == 128) return o ^ (((o >> 7) & 7u) << 4);
+  else if constexpr (U == 64) return o ^ (((o >> 7) & 3u) << 4);
+  else if constexpr (U == 32) return o ^ (((o >> 7) & 1u) << 4);
+  else return o;
+}
+
+// Tile = R = 32 * TMA_CONSUMER_WARPS chunks; stage = one U-byte segment of each chunk of a
+// tile (R x U bytes); a chunk of cs bytes takes S = cs / U stages.
+template <int U, int KIND>
+__global__ void __launch_bounds__((TMA_CONSUMER_WARPS + 1) * 32)
+    leaf_tma_kernel(const __grid_constant__ CUtensorMap tmap, LeafArgs a, uint32_t nfull, uint32_t S,
+                    uint32_t stages) {
+  constexpr uint32_t R = 32u * TMA_CONSUMER_WARPS;
+  constexpr uint32_t STAGE_BYTES = R * U;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023u) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)stages * STAGE_BYTES);
+  uint64_t* empty = full + stages;
+  __shared__ int abort_flag;
+
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  if (threadIdx.x == 0) {
+    abort_flag = 0;
+    for (uint32_t s = 0; s < stages; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], TMA_CONSUMER_WARPS);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+
+  const uint32_t ntiles = (nfull + R - 1) / R;
+  if (warp == TMA_CONSUMER_WARPS) {
+    // ---------------- producer warp: one elected lane issues the TMA copies
+    if (lane == 0) {
+      asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmap)) : "memory");
+      uint32_t k = 0;
+      bool ok = true;
+      for (uint32_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        for (uint32_t g = 0; g < S; g++, k++) {
+          const uint32_t s = k % stages, ph = (k / stages) & 1u;
+          if (k >= stages && !mbar_wait_bounded(&empty[s], ph ^ 1u, a.st, &abort_flag)) { ok = false; break; }
+          mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
+          tma_load_3d(smem + (size_t)s * STAGE_BYTES, &tmap, &full[s], 0, (int)g, (int)(t * R));
+        }
+      }
+      // wait for this CTA's copies still in flight before the CTA may exit
+      const uint32_t issued = k;
+      const uint32_t first = issued > stages ? issued - stages : 0;
+      for (uint32_t q = first; q < issued; q++)
+        mbar_wait_bounded(&full[q % stages], (q / stages) & 1u, a.st, &abort_flag);
+      // the short last chunk (len not a multiple of cs) is hashed here with byte loads
+      if (blockIdx.x == 0 && nfull < a.n) {
+        for (uint64_t c = nfull; c < a.n; c++) {
+          const uint64_t off = c * a.cs;
+          const uint64_t nb = (c == a.n - 1u) ? a.len - off : a.cs;
+          leaf_finish(a, (uint32_t)c, hash_bytes(a.kind, a.data + off, nb));
+        }
+      }
+    }
+    return;
+  }
+
+  // ---------------- consumer warps: lane = chunk row of the tile
+  uint32_t k = 0;
+  const uint32_t row = warp * 32u + lane;
+  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const uint32_t chunk = t * R + row;
+    const bool valid = chunk < nfull;
+    Murmur3 mm;
+    mm.init();
+    uint32_t md[4];
+    md5_init(md);
+    for (uint32_t g = 0; g < S; g++, k++) {
+      const uint32_t s = k % stages, ph = (k / stages) & 1u;
+      if (!mbar_wait_bounded(&full[s], ph, a.st, &abort_flag)) return;
+      const uint8_t* stage = smem + (size_t)s * STAGE_BYTES;
+      if (valid) {
+        const uint32_t base = row * U;
+        if constexpr (KIND == HASH_MD5) {
+#pragma unroll
+          for (uint32_t blk = 0; blk < U / 64u; blk++) {
+            uint32_t m[16];
+#pragma unroll
+            for (uint32_t j = 0; j < 4; j++) {
+              const uint4 v = *reinterpret_cast<const uint4*>(stage + swz<U>(base + blk * 64u + 16u * j));
+              m[4 * j + 0] = v.x; m[4 * j + 1] = v.y; m[4 * j + 2] = v.z; m[4 * j + 3] = v.w;
+            }
+            md5_compress(md, m);
+          }
+        } else {
+#pragma unroll
+          for (uint32_t j = 0; j < U / 16u; j++) {
+            const uint4 v = *reinterpret_cast<const uint4*>(stage + swz<U>(base + 16u * j));
+            mm.block_words(v.x, v.y, v.z, v.w);
+          }
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+    }
+    if (valid) {
+      Digest d;
+      if constexpr (KIND == HASH_MD5) {
+        md5_pad_block64(md, a.cs);
+        d = md5_digest(md);
+      } else {
+        d = mm.finish(a.cs);
+      }
+      leaf_finish(a, chunk, d);
+    }
+  }
+}
+
+// ------------------------------------------------------------------ host side
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn get_encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+static int choose_unit(uint32_t cs, int kind) {
+  if (kind == HASH_MD5) {
+    if (cs % 128u == 0) return 128;
+    if (cs % 64u == 0) return 64;
+    return 0;
+  }
+  if (cs % 128u == 0) return 128;
+  if (cs % 64u == 0) return 64;
+  if (cs % 32u == 0) return 32;
+  if (cs % 16u == 0) return 16;
+  return 0;
+}
+
+template <int U, int KIND>
+static cudaError_t launch_tma(const CUtensorMap& map, const LeafArgs& a, uint32_t nfull, uint32_t S,
+                              int sm_count, cudaStream_t stream) {
+  constexpr uint32_t R = 32u * TMA_CONSUMER_WARPS;
+  constexpr uint32_t STAGE_BYTES = R * U;
+  uint32_t stages = (96u * 1024u) / STAGE_BYTES;
+  if (stages < 2) stages = 2;
+  if (stages > 16) stages = 16;
+  const size_t smem = (size_t)stages * STAGE_BYTES + 2 * stages * sizeof(uint64_t) + 1024;
+  auto kern = leaf_tma_kernel<U, KIND>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const uint32_t ntiles = (nfull + R - 1) / R;
+  uint32_t grid = (uint32_t)sm_count * 2u;
+  if (grid > ntiles) grid = ntiles;
+  if (grid == 0) grid = 1;
+  kern<<<grid, (TMA_CONSUMER_WARPS + 1) * 32, smem, stream>>>(map, a, nfull, S, stages);
+  return cudaGetLastError();
+}
+
+// Returns 1 if the staged TMA path was used, 0 for the generic path, negative on error.
+int launch_leaves(const LeafArgs& a, int sm_count, bool allow_tma, cudaStream_t stream) {
+  const uint32_t nfull = (uint32_t)(a.len / a.cs);
+  const int U = choose_unit(a.cs, a.kind);
+  const bool aligned = (reinterpret_cast<uintptr_t>(a.data) & 15u) == 0;
+  EncodeTiledFn enc = get_encode_fn();
+  if (allow_tma && U > 0 && aligned && nfull > 0 && enc != nullptr) {
+    CUtensorMap map;
+    const cuuint64_t S = a.cs / (uint32_t)U;
+    cuuint64_t dims[3] = {(cuuint64_t)U, S, (cuuint64_t)nfull};
+    cuuint64_t strides[2] = {(cuuint64_t)U, (cuuint64_t)a.cs};
+    cuuint32_t box[3] = {(cuuint32_t)U, 1u, 32u * TMA_CONSUMER_WARPS};
+    cuuint32_t estr[3] = {1u, 1u, 1u};
+    CUtensorMapSwizzle sw = U == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
+                          : U == 64  ? CU_TENSOR_MAP_SWIZZLE_64B
+                          : U == 32  ? CU_TENSOR_MAP_SWIZZLE_32B
+                                     : CU_TENSOR_MAP_SWIZZLE_NONE;
+    CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<uint8_t*>(a.data), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r == CUDA_SUCCESS) {
+      cudaError_t e;
+      const uint32_t s32 = (uint32_t)S;
+      if (a.kind == HASH_MD5) {
+        e = U == 128 ? launch_tma<128, HASH_MD5>(map, a, nfull, s32, sm_count, stream)
+                     : launch_tma<64, HASH_MD5>(map, a, nfull, s32, sm_count, stream);
+      } else {
+        switch (U) {
+          case 128: e = launch_tma<128, HASH_MURMUR3>(map, a, nfull, s32, sm_count, stream); break;
+          case 64: e = launch_tma<64, HASH_MURMUR3>(map, a, nfull, s32, sm_count, stream); break;
+          case 32: e = launch_tma<32, HASH_MURMUR3>(map, a, nfull, s32, sm_count, stream); break;
+          default: e = launch_tma<16, HASH_MURMUR3>(map, a, nfull, s32, sm_count, stream); break;
+        }
+      }
+      return e == cudaSuccess ? 1 : -1;
+    }
+  }
+  const uint32_t threads = 256;
+  uint64_t blocks = ceil_div_u64(a.n, threads);
+  const uint64_t cap = (uint64_t)sm_count * 16u;
+  if (blocks > cap) blocks = cap;
+  if (blocks == 0) blocks = 1;
+  leaf_generic_kernel<<<(uint32_t)blocks, threads, 0, stream>>>(a, 0u, a.n);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+}  // namespace b2d

@@ -1,0 +1,168 @@
+// Open-addressing device map: 128-bit chunk/node digest -> NodeID{node, checkpoint}.
+//
+// Replaces the reference's DigestNodeIDDeviceMap (include/map_helpers.hpp:105-113, a
+// Kokkos::UnorderedMap<HashDigest, NodeID>).  Contract kept from the reference tree path:
+//   insert(key, value): insert-if-absent; reports inserted vs existing plus the slot;
+//   the slot's value stays mutable for the lowest-index update (tree_approach.cpp:85,339).
+//
+// Slot layout (32 bytes, one quarter of a 128-byte line):
+//   key  : two u64 words, claimed with one 128-bit atomicCAS (EMPTY = all ones)
+//   val  : u64 = (priority << 32) | node.  Every insert of the current checkpoint applies
+//          atomicMin to it, so the value left behind is the one the reference's sequential
+//          execution order inserts first (leaves by index, then first-occurrence parents by
+//          level and index, then the baseline's per-level inserts).  node = low 32 bits.
+//   tree : checkpoint id of the first insert; UINT32_MAX while the inserting thread has
+//          claimed the key but not yet stored it (readers treat that as "this checkpoint").
+// The digest equal to the EMPTY pattern is kept in one extra slot at index `cap`.
+#pragma once
+#include "common.cuh"
+
+namespace b2d {
+
+struct __align__(32) MapSlot {
+  unsigned long long key_lo;
+  unsigned long long key_hi;
+  unsigned long long val;
+  uint32_t tree;
+  uint32_t pad;
+};
+static_assert(sizeof(MapSlot) == 32, "slot must be 32 bytes");
+
+struct __align__(16) Key128 {
+  unsigned long long lo, hi;
+};
+
+constexpr unsigned long long MAP_EMPTY = ~0ull;
+constexpr uint32_t MAP_TREE_PENDING = 0xffffffffu;
+
+struct MapView {
+  MapSlot* slots;      // cap + 1 slots
+  uint64_t cap;        // power of two
+  uint64_t mask;
+  unsigned long long* size;   // device counter of occupied slots
+};
+
+struct MapRef {
+  uint64_t slot;       // valid when found
+  bool found;
+  bool inserted;
+};
+
+__device__ __forceinline__ Key128 digest_key(const Digest& d) {
+  Key128 k;
+  k.lo = (unsigned long long)d.w[0] | ((unsigned long long)d.w[1] << 32);
+  k.hi = (unsigned long long)d.w[2] | ((unsigned long long)d.w[3] << 32);
+  return k;
+}
+__device__ __forceinline__ bool key_is_empty_pattern(const Key128& k) {
+  return k.lo == MAP_EMPTY && k.hi == MAP_EMPTY;
+}
+__device__ __forceinline__ uint64_t map_home(const Key128& k, uint64_t mask) {
+  // digests are uniformly distributed; fold both halves so a table of any size mixes all bits
+  unsigned long long h = k.lo ^ (k.hi * 0x9E3779B97F4A7C15ull);
+  h ^= h >> 31;
+  return (uint64_t)h & mask;
+}
+
+// Find without concurrent inserters on the probed path (all lookups in this library happen
+// either in a later kernel than the inserts, or for keys whose probe path was complete
+// before the launch).  Returns cap+1 when absent.
+__device__ __forceinline__ uint64_t map_find(const MapView& m, const Digest& d) {
+  const Key128 k = digest_key(d);
+  if (key_is_empty_pattern(k)) {
+    const MapSlot& s = m.slots[m.cap];
+    return s.pad ? m.cap : m.cap + 1;
+  }
+  uint64_t i = map_home(k, m.mask);
+  for (uint64_t probe = 0; probe <= m.mask; probe++) {
+    const MapSlot* s = &m.slots[i];
+    const unsigned long long lo = s->key_lo, hi = s->key_hi;
+    if (lo == k.lo && hi == k.hi) return i;
+    if (lo == MAP_EMPTY && hi == MAP_EMPTY) return m.cap + 1;
+    i = (i + 1) & m.mask;
+  }
+  return m.cap + 1;
+}
+
+__device__ __forceinline__ Key128 atomic_cas_key(MapSlot* s, Key128 cmp, Key128 val) {
+  return atomicCAS(reinterpret_cast<Key128*>(&s->key_lo), cmp, val);
+}
+
+// Insert-if-absent.  On success the caller's value is merged with atomicMin and the
+// checkpoint id stored.  On an existing key nothing is written here; the caller decides
+// (through map_merge_current) whether the entry belongs to the current checkpoint.
+__device__ __forceinline__ MapRef map_insert(const MapView& m, const Digest& d, unsigned long long val,
+                                             uint32_t cur, DevStatus* st) {
+  const Key128 k = digest_key(d);
+  MapRef r{0, false, false};
+  if (key_is_empty_pattern(k)) {
+    MapSlot* s = &m.slots[m.cap];
+    const uint32_t old = atomicCAS(&s->pad, 0u, 1u);
+    atomicMin(&s->val, val);
+    r.slot = m.cap;
+    r.found = true;
+    r.inserted = (old == 0u);
+    if (r.inserted) {
+      atomicExch(&s->tree, cur);
+      atomicAdd(m.size, 1ull);
+    }
+    return r;
+  }
+  // a key with an all-ones half could be confused with a half-written slot: always CAS
+  const bool cas_only = (k.lo == MAP_EMPTY) || (k.hi == MAP_EMPTY);
+  const Key128 empty{MAP_EMPTY, MAP_EMPTY};
+  uint64_t i = map_home(k, m.mask);
+  for (uint64_t probe = 0; probe <= m.mask; probe++) {
+    MapSlot* s = &m.slots[i];
+    bool try_cas = true;
+    if (!cas_only) {
+      const unsigned long long lo = *reinterpret_cast<volatile unsigned long long*>(&s->key_lo);
+      const unsigned long long hi = *reinterpret_cast<volatile unsigned long long*>(&s->key_hi);
+      if (lo == k.lo && hi == k.hi) {
+        r.slot = i; r.found = true; r.inserted = false;
+        return r;
+      }
+      // a slot holding a complete other key can be skipped; anything with an all-ones half
+      // may be empty or mid-claim and is resolved by the CAS
+      try_cas = (lo == MAP_EMPTY) || (hi == MAP_EMPTY);
+    }
+    if (try_cas) {
+      const Key128 old = atomic_cas_key(s, empty, k);
+      if (old.lo == MAP_EMPTY && old.hi == MAP_EMPTY) {
+        atomicMin(&s->val, val);
+        atomicExch(&s->tree, cur);
+        atomicAdd(m.size, 1ull);
+        r.slot = i; r.found = true; r.inserted = true;
+        return r;
+      }
+      if (old.lo == k.lo && old.hi == k.hi) {
+        r.slot = i; r.found = true; r.inserted = false;
+        return r;
+      }
+    }
+    i = (i + 1) & m.mask;
+  }
+  set_error(st, DERR_MAP_FULL, 0);
+  return r;
+}
+
+// An existing entry belongs to the current checkpoint when its id is `cur` or still
+// pending (claimed by a concurrent inserter of this launch).  In that case the lower
+// (priority, node) value wins, matching "first insert in sequential order".
+__device__ __forceinline__ bool map_merge_current(const MapView& m, uint64_t slot, unsigned long long val,
+                                                  uint32_t cur) {
+  MapSlot* s = &m.slots[slot];
+  const uint32_t t = *reinterpret_cast<volatile uint32_t*>(&s->tree);
+  if (t == cur || t == MAP_TREE_PENDING) {
+    atomicMin(&s->val, val);
+    return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ uint32_t map_node(const MapView& m, uint64_t slot) {
+  return (uint32_t)(m.slots[slot].val & 0xffffffffull);
+}
+__device__ __forceinline__ uint32_t map_tree(const MapView& m, uint64_t slot) { return m.slots[slot].tree; }
+
+}  // namespace b2d

@@ -1,0 +1,177 @@
+"""GPU parity: the CUDA path through the C ABI against the oracle and the golden fixtures.
+
+Bit-exact comparisons throughout: digests, diff bytes (header, metadata order, data) and
+restarted buffers.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from reproducibility_icpp23_scalable_gpu_deduplication_b200 import HASH_MD5, HASH_MURMUR3, TreeDeduplicator, synth
+from reproducibility_icpp23_scalable_gpu_deduplication_b200.tree import hash_chunks, parse_header
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def load(name):
+    with open(os.path.join(GOLDEN, name)) as f:
+        return json.load(f)
+
+
+def to_dev(a):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def run_both(bufs, cs, kind=HASH_MURMUR3, baselines=None, restart=True, tma=True):
+    """checkpoint every buffer on the GPU and in the oracle; assert identical diffs and restarts"""
+    import torch
+
+    old = os.environ.get("B2D_DISABLE_TMA")
+    if not tma:
+        os.environ["B2D_DISABLE_TMA"] = "1"
+    try:
+        g = TreeDeduplicator(cs, kind)
+    finally:
+        if old is None:
+            os.environ.pop("B2D_DISABLE_TMA", None)
+        else:
+            os.environ["B2D_DISABLE_TMA"] = old
+    o = O.OracleTreeDeduplicator(cs, kind)
+    gd, od = [], []
+    for i, b in enumerate(bufs):
+        mb = (i == 0) if baselines is None else bool(baselines[i])
+        x = to_dev(b)
+        gd.append(g.checkpoint(x, mb))
+        od.append(o.checkpoint(b, mb))
+        assert len(gd[-1]) == len(od[-1]), (i, parse_header(gd[-1]), parse_header(od[-1]))
+        assert gd[-1] == od[-1], (i, parse_header(gd[-1]))
+        assert (g.num_first_ocur(), g.num_shift_dupl()) == (o.num_first_ocur(), o.num_shift_dupl())
+    if restart:
+        for i, b in enumerate(bufs):
+            want, rc = O.restart(od, i)
+            out = torch.zeros(len(b), dtype=torch.uint8, device="cuda")
+            grc = g.restart(out, gd, i, check_status=False)
+            assert (grc == 0) == (rc == 0), (i, grc, rc)
+            assert out.cpu().numpy().tobytes() == want.tobytes(), i
+    g.close()
+    return gd
+
+
+def test_hash_kat_gpu(cuda):
+    import torch
+
+    for e in load("hash_kat.json")["kat"]:
+        L = e["len"]
+        if L == 0:
+            continue
+        x = torch.frombuffer(bytearray.fromhex(e["data"]), dtype=torch.uint8).cuda()
+        assert hash_chunks(x, L, HASH_MURMUR3).cpu().numpy().tobytes().hex() == e["murmur3"], L
+        assert hash_chunks(x, L, HASH_MD5).cpu().numpy().tobytes().hex() == e["md5"], L
+
+
+@pytest.mark.parametrize("case", sorted(load("test_cases.json")))
+def test_reference_test_cases_gpu(cuda, case):
+    c = load("test_cases.json")[case]
+    bufs = [np.frombuffer(c["step0"].encode(), np.uint8), np.frombuffer(c["step1"].encode(), np.uint8)]
+    gd = run_both(bufs, 1)
+    assert gd[0].hex() == c["diff0"] and gd[1].hex() == c["diff1"]
+
+
+@pytest.mark.parametrize("name", sorted(load("series.json")))
+@pytest.mark.parametrize("tma", [True, False])
+def test_series_golden_gpu(cuda, name, tma):
+    g = load("series.json")[name]
+    plan = synth.plan_plain_64m if g["generator"] == "plain_64m" else synth.plan_plain_4g
+    s = synth.ByteSeries(g["nbytes"], g["chunk_size"], plan, 1, 0)
+    bufs = [s.next().copy() for _ in range(g["checkpoints"])]
+    gd = run_both(bufs, g["chunk_size"], g["hash"], tma=tma)
+    assert [hashlib.sha256(x).hexdigest() for x in gd] == g["sha256"]
+
+
+def test_plain_64m_full_size(cuda):
+    """The CPU-runnable benchmark case at its full size: 64 MiB, chunk 128 B, 5 checkpoints."""
+    s = synth.plain_64m()
+    bufs = [s.next().copy() for _ in range(5)]
+    run_both(bufs, 128)
+    # restart reproduces every checkpoint (power-of-two chunk count)
+    import torch
+
+    o = O.OracleTreeDeduplicator(128)
+    diffs = [o.checkpoint(b, i == 0) for i, b in enumerate(bufs)]
+    g = TreeDeduplicator(128)
+    out = torch.zeros(len(bufs[0]), dtype=torch.uint8, device="cuda")
+    for i, b in enumerate(bufs):
+        g.restart(out, diffs, i)
+        assert torch.equal(out.cpu(), torch.from_numpy(b))
+
+
+@pytest.mark.parametrize("cs", [1, 7, 16, 32, 48, 64, 100, 128, 192, 256, 512, 4096])
+@pytest.mark.parametrize("kind", [HASH_MURMUR3, HASH_MD5])
+def test_chunk_sizes(cuda, cs, kind):
+    nbytes = 96 * 1024 + 37 if cs > 1 else 3000
+    s = synth.ByteSeries(nbytes, cs, synth.plan_plain_64m, 1, cs)
+    bufs = [s.next().copy() for _ in range(4)]
+    run_both(bufs, cs, kind)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 8, 13, 100, 1000, 4097])
+def test_small_and_non_power_of_two_trees(cuda, n):
+    cs = 64
+    s = synth.ByteSeries(n * cs, cs, synth.plan_plain_64m, 1, 1000 + n)
+    bufs = [s.next().copy() for _ in range(4)]
+    run_both(bufs, cs)
+
+
+def test_duplicate_heavy_and_zero_pages(cuda):
+    """Many equal chunks and equal subtrees at several depths: first-insert-wins order."""
+    rng = np.random.default_rng(11)
+    cs, n = 64, 3 * 1024 + 5
+    bufs = []
+    base = np.zeros(n * cs, np.uint8)
+    for k in range(5):
+        b = base.copy()
+        pat = rng.integers(0, 4, n)
+        for v in range(1, 4):
+            b.reshape(n, cs)[pat == v] = v + k
+        bufs.append(b)
+    run_both(bufs, cs)
+    run_both(bufs, cs, HASH_MD5)
+
+
+def test_make_baseline_mid_sequence(cuda):
+    s = synth.ByteSeries(256 * 1024, 128, synth.plan_plain_64m, 1, 77)
+    bufs = [s.next().copy() for _ in range(6)]
+    run_both(bufs, 128, baselines=[1, 0, 0, 1, 0, 0])
+
+
+def test_whole_buffer_shift_bug_compatible(cuda):
+    rng = np.random.default_rng(3)
+    a = rng.integers(0, 256, 8 * 64, dtype=np.uint8)
+    b = rng.integers(0, 256, 8 * 64, dtype=np.uint8)
+    run_both([a, b, a], 64)
+
+
+def test_len_change_without_baseline_rejected(cuda):
+    import torch
+
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import B2DError
+
+    g = TreeDeduplicator(128)
+    g.checkpoint(torch.zeros(4096, dtype=torch.uint8, device="cuda"), True)
+    with pytest.raises(B2DError):
+        g.checkpoint(torch.zeros(8192, dtype=torch.uint8, device="cuda"), False)
+    g.checkpoint(torch.ones(8192, dtype=torch.uint8, device="cuda"), True)
+
+
+def test_md5_float_series(cuda):
+    """The MD5 training-state workload at reduced size (64 MiB): float32 with noise, zero pages, repeats."""
+    s = synth.FloatSeries(64 << 20)
+    bufs = [s.next().copy() for _ in range(4)]
+    run_both(bufs, 256, HASH_MD5)
