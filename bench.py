@@ -47,6 +47,8 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--cpu-sample-bytes", type=int, default=512 << 20)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--leaf-stages", type=int, default=0, help="TMA ring depth (0 = library default)")
+    p.add_argument("--leaf-ctas", type=int, default=0, help="hashing CTAs per SM (0 = library default)")
     return p.parse_args()
 
 
@@ -187,6 +189,10 @@ def main():
 
     series = synth.plain_4g(nbytes=nbytes, chunk_size=cs, device=dev, seed=synth.SEED + rank)
     dd = TreeDeduplicator(cs)
+    if args.leaf_stages:
+        dd.set_param("leaf_stages", args.leaf_stages)
+    if args.leaf_ctas:
+        dd.set_param("leaf_ctas_per_sm", args.leaf_ctas)
     dd.checkpoint_device(series.next(), make_baseline=True)          # checkpoint 0: baseline
     for _ in range(args.warmup):
         dd.checkpoint_device(series.next())
@@ -239,7 +245,7 @@ def main():
     te = torch.tensor([e_ms], device=dev)
     if world > 1:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * len(e2e_bufs) * nbytes / (float(te.item()) * 1e-3) / GB
+    e2e_value = world * len(e2e_bufs) * nbytes / (float(te.item()) * 1e-3) / GB if e2e_bufs else None
 
     peak, peak_kind = measured_peak()
     alg_leaf = nbytes + 32 * n_chunks              # read the buffer, read + write a digest per chunk
@@ -259,8 +265,8 @@ def main():
         "config": {"workload": "plain_4g", "nbytes": nbytes, "chunk_size": cs, "hash": "murmur3",
                    "checkpoints": 1 + args.warmup + args.steps, "l2": "inputs 4 GiB > L2, no flush",
                    "parallelism": f"replicas x{world}"},
-        "e2e": {"value": round(e2e_value, 2), "unit": "GB/s", "h2d_bytes_per_step": nbytes,
-                "d2h_bytes_per_step": int(statistics.mean(d2h))},
+        "e2e": {"value": round(e2e_value, 2) if e2e_value else None, "unit": "GB/s", "h2d_bytes_per_step": nbytes,
+                "d2h_bytes_per_step": int(statistics.mean(d2h)) if d2h else 0},
         "gpu_launches": launches,
         "roofline": roofline,
         "clocks": clk.summary(),

@@ -63,6 +63,13 @@ int b2d_destroy(b2d_dedup* d);
  * own stream).  No reference counterpart (Kokkos uses its default execution space). */
 int b2d_set_stream(b2d_dedup* d, void* cuda_stream);
 
+/* Tuning knobs (no reference counterpart; output bytes never depend on them):
+ *   "leaf_tma"          1 = TMA-staged chunk hashing when the chunk size allows (default), 0 = off
+ *   "leaf_stages"       TMA ring depth per CTA, 2..16 (0 = default)
+ *   "leaf_ctas_per_sm"  resident hashing CTAs per SM, 1..8 (0 = default 2)
+ *   "map_max_load_pct"  digest-map load factor that triggers growth, 10..90 (default 75) */
+int b2d_set_param(b2d_dedup* d, const char* name, int64_t value);
+
 /* checkpoint(header_t&, uint8_t* data_ptr, size_t len, HostMirror& diff_h, bool make_baseline)
  * -- src/tree_approach.cpp:1577-1689, minus the device->host copy: the diff stays in device
  * memory owned by the handle (b2d_diff_device / b2d_copy_diff).  advance_id != 0 also does the
@@ -123,10 +130,11 @@ int b2d_phase_times(b2d_dedup* d, double out[3], int* leaf_path);
 /* device kernels launched by the last checkpoint/restart call on this handle */
 int b2d_last_launch_count(b2d_dedup* d, uint32_t* out);
 
-/* Introspection for tests: copy `nodes` tree digests (16 B each) / labels (1 B each) of the
- * last checkpoint to host memory. */
+/* Introspection for tests: copy the first `nodes` tree digests (16 B each, heap order) or the
+ * labels of the first `leaves` leaves (1 B each, chunk order; Label values of
+ * include/utils.hpp:51-57) of the last checkpoint to host memory. */
 int b2d_debug_tree(b2d_dedup* d, void* dst, uint64_t nodes);
-int b2d_debug_labels(b2d_dedup* d, void* dst, uint64_t nodes);
+int b2d_debug_labels(b2d_dedup* d, void* dst, uint64_t leaves);
 /* Digest of each `chunk_size` chunk of a device buffer into d_out (16 B per chunk), the
  * reference's hash() (include/hash_functions.hpp:16-20) as a standalone kernel. */
 int b2d_hash_chunks(int hash_kind, const void* d_data, uint64_t len, uint32_t chunk_size, void* d_out,

@@ -26,6 +26,7 @@ SIGNATURES = [
     ("b2d_create", _int, [_u32, _int, ctypes.POINTER(_vp)]),
     ("b2d_destroy", _int, [_vp]),
     ("b2d_set_stream", _int, [_vp, _vp]),
+    ("b2d_set_param", _int, [_vp, _cc, ctypes.c_int64]),
     ("b2d_checkpoint_device", _int, [_vp, _vp, _u64, _int, _int, ctypes.POINTER(_u64)]),
     ("b2d_diff_device", _int, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_u64)]),
     ("b2d_copy_diff", _int, [_vp, _vp, _u64]),

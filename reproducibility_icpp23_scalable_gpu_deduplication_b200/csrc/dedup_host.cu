@@ -120,8 +120,9 @@ __global__ void hash_chunks_kernel(int kind, const uint8_t* data, uint64_t len, 
 struct DevState {
   DevStatus status;
   int zero_exists;
-  int pad;
+  unsigned int pad;
   DevMeta meta;
+  StraddleInfo straddle;
 };
 
 }  // namespace b2d
@@ -145,7 +146,8 @@ struct b2d_dedup {
   double phase[3] = {0, 0, 0};   // device time of leaves, forest, diff assembly (last checkpoint)
   bool leaf_tma = false;
   bool have_tree = false;
-  bool allow_tma = true;
+  LeafTuning tune;
+  double map_max_load = 0.75;
 
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
@@ -154,11 +156,12 @@ struct b2d_dedup {
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
   DevBuf<Digest> tree;
-  DevBuf<uint8_t> lab, push;
+  DevBuf<uint8_t> lab, leaflab, push, dupflag;
   DevBuf<MapSlot> map_slots;
   uint64_t map_cap = 0;           // power of two; slots hold map_cap + 1 entries
   uint64_t map_size_host = 0;     // occupied slots after the last checkpoint
   DevBuf<unsigned long long> map_size;
+  DevBuf<uint32_t> tmp_first, tmp_shift, levels;
   DevBuf<uint32_t> first_list, shift_list, region_off, sprev, skey, hist, bucket_start, partial, partial2;
   DevBuf<uint8_t> diff;
   DevBuf<DevState> state;
@@ -211,11 +214,12 @@ uint64_t pow2_at_least(uint64_t x) {
 }
 
 // capacity policy: the reference rehashes when capacity < size + num_nodes (:1622-1623); here
-// the table keeps load <= 0.75 with that reservation and grows to load <= 0.375
+// the table keeps load <= map_max_load (default 0.75) with that reservation and grows to half
+// of it
 int map_ensure(b2d_dedup* d) {
   const uint64_t need = d->map_size_host + d->N;
-  if (d->map_slots.p && (double)need <= 0.75 * (double)d->map_cap) return B2D_OK;
-  const uint64_t cap = pow2_at_least((uint64_t)((double)need / 0.375) + 1);
+  if (d->map_slots.p && (double)need <= d->map_max_load * (double)d->map_cap) return B2D_OK;
+  const uint64_t cap = pow2_at_least((uint64_t)((double)need / (0.5 * d->map_max_load)) + 1);
   if (!d->map_slots.p || d->map_size_host == 0) return map_reset(d, cap);
   DevBuf<MapSlot> fresh;
   B2D_CU(fresh.reserve(cap + 1));
@@ -269,9 +273,19 @@ int do_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, bool make_base
   // setup (:1594-1623): tree, labels, map, scratch
   B2D_CU(d->tree.reserve(d->N));
   B2D_CU(d->lab.reserve(d->N));
-  B2D_CU(d->push.reserve(d->N));
+  B2D_CU(d->leaflab.reserve((uint64_t)d->n + 16u));
+  if (d->dupflag.n < d->n || !d->dupflag.p) {
+    // duplicate flags stay all-zero between checkpoints (phase 1 clears what it reads)
+    B2D_CU(d->dupflag.reserve(d->n));
+    B2D_CU(cudaMemsetAsync(d->dupflag.p, 0, d->dupflag.n, d->stream));
+  }
+  if (d->push.n < d->N + 16ull || !d->push.p) {
+    // flags stay all-zero between checkpoints (the compaction clears what it reads)
+    B2D_CU(d->push.reserve(((uint64_t)d->N + 15ull) / 16ull * 16ull + 16ull));
+    B2D_CU(cudaMemsetAsync(d->push.p, 0, d->push.n, d->stream));
+  }
   if (baseline) {
-    int rc = map_reset(d, pow2_at_least((uint64_t)((double)d->N / 0.375) + 1));
+    int rc = map_reset(d, pow2_at_least((uint64_t)((double)d->N / (0.5 * d->map_max_load)) + 1));
     if (rc) return rc;
     d->have_tree = true;
     d->baseline_id = d->current_id;
@@ -282,6 +296,9 @@ int do_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, bool make_base
   const uint32_t B = d->current_id + 1u;
   B2D_CU(d->first_list.reserve(d->n));
   B2D_CU(d->shift_list.reserve(d->n));
+  B2D_CU(d->tmp_first.reserve(d->n));
+  B2D_CU(d->tmp_shift.reserve(d->n));
+  B2D_CU(d->levels.reserve(68));
   B2D_CU(d->region_off.reserve(d->n));
   B2D_CU(d->sprev.reserve(d->n));
   B2D_CU(d->skey.reserve(d->n));
@@ -303,29 +320,33 @@ int do_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, bool make_base
   B2D_CU(cudaEventRecord(d->ev[0], d->stream));
   // dedup_data_baseline (:13-259) / dedup_data (:261-509)
   LeafArgs la{static_cast<const uint8_t*>(d_data), len, d->chunk_size, d->n, d->kind, baseline ? 1 : 0,
-              d->current_id, d->tree.p, d->lab.p, m, &ds->status};
-  const int leaf_path = launch_leaves(la, d->sm_count, d->allow_tma, d->stream);
+              d->current_id, d->tree.p, d->leaflab.p, d->dupflag.p, m, &ds->status};
+  const int leaf_path = launch_leaves(la, d->sm_count, d->tune, d->stream);
   if (leaf_path < 0) return B2D_ERR_CUDA;
   d->leaf_tma = leaf_path == 1;
   d->launches += 1;
   B2D_CU(cudaEventRecord(d->ev[3], d->stream));
-  ForestArgs fa{d->tree.p, d->lab.p, d->push.p, m, &ds->status, &ds->zero_exists, d->n, d->N, d->D,
-                d->current_id, d->kind, baseline ? 1 : 0};
+  ForestArgs fa{d->tree.p, d->lab.p, d->leaflab.p, d->push.p, m, &ds->status, &ds->zero_exists, d->dupflag.p,
+                d->n, d->N, d->D, d->current_id, d->kind, baseline ? 1 : 0};
   B2D_CU(launch_forest(fa, 1, d->stream));
   if (baseline) {
     B2D_CU(launch_zero_exists(m, &ds->zero_exists, d->stream));
     d->launches += 1;
   }
   B2D_CU(launch_forest(fa, 2, d->stream));
-  d->launches += 2 * ((d->D + FOREST_BAND_LEVELS) / FOREST_BAND_LEVELS);
+  if (baseline) {
+    B2D_CU(launch_baseline_inserts(fa, d->sm_count, d->stream));
+    d->launches += 1;
+  }
+  d->launches += 2 * forest_launch_count(d->D);
   B2D_CU(cudaEventRecord(d->ev[1], d->stream));
   // collect_diff (:511-710)
   DiffArgs ga{static_cast<const uint8_t*>(d_data), len, d->chunk_size, d->n, d->N, d->D, d->current_id,
               d->baseline_id, d->tree.p, d->push.p, m, &ds->status, &ds->meta, d->first_list.p,
-              d->shift_list.p, d->region_off.p, d->sprev.p, d->skey.p, d->hist.p, d->bucket_start.p,
+              d->shift_list.p, d->tmp_first.p, d->tmp_shift.p, d->levels.p, d->region_off.p, d->sprev.p, d->skey.p, d->hist.p, d->bucket_start.p,
               d->partial.p, d->partial2.p, d->diff.p};
   B2D_CU(launch_collect_diff(ga, d->sm_count, d->stream));
-  d->launches += 12;
+  d->launches += 14;
   B2D_CU(cudaEventRecord(d->ev[2], d->stream));
   B2D_CU(cudaMemcpyAsync(d->state_h.p, d->state.p, sizeof(DevState), cudaMemcpyDeviceToHost, d->stream));
   B2D_CU(cudaStreamSynchronize(d->stream));
@@ -342,7 +363,13 @@ int do_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, bool make_base
   d->timers[3] = 0;
   int rc = status_code(st.status);
   d->map_size_host = st.meta.map_size;
-  if (rc) return rc;
+  if (rc) {
+    // a failed checkpoint may leave region flags behind; they must be zero for the next one
+    cudaMemsetAsync(d->push.p, 0, d->push.n, d->stream);
+    cudaMemsetAsync(d->dupflag.p, 0, d->dupflag.n, d->stream);
+    cudaStreamSynchronize(d->stream);
+    return rc;
+  }
   d->F = st.meta.F;
   d->S = st.meta.S;
   d->diff_len = st.meta.diff_len;
@@ -473,50 +500,6 @@ bool parse_hdr(const uint8_t* b, uint64_t size, HostHdr& h) {
   return h.data_off <= size && h.cs > 0 && h.datalen > 0;
 }
 
-// The one first-occurrence region (if any) whose root spans two leaf depths: only possible
-// when the chunk count is not a power of two (see r_straddle_kernel).
-StraddleInfo find_straddle(const uint8_t* b, const HostHdr& h, uint32_t n, uint32_t N) {
-  StraddleInfo sd{0, 0, 0, 0, 0};
-  if (n < 3 || (n & (n - 1)) == 0) return sd;
-  const uint32_t D = node_level(N - 1);
-  // straddling nodes: common ancestors of the last inner node and the first leaf of level D-1
-  std::vector<uint32_t> anc;
-  uint32_t x = n - 2, y = n - 1;
-  while (x != y) {
-    if (x > y) x = (x - 1) / 2; else y = (y - 1) / 2;
-  }
-  for (;;) {
-    anc.push_back(x);
-    if (x == 0) break;
-    x = (x - 1) / 2;
-  }
-  uint32_t run = 0;
-  for (uint32_t i = 0; i < h.F; i++) {
-    uint32_t node;
-    memcpy(&node, b + h.first_off + 4ull * i, 4);
-    bool hit = false;
-    for (uint32_t a : anc) hit |= (a == node);
-    if (hit) {
-      const uint32_t k = (D - 1) - node_level(node);
-      const uint64_t lo_all = ((uint64_t)node << k) + (1ull << k) - 1ull;
-      const uint64_t hi_all = lo_all + (1ull << k) - 1ull;
-      const uint64_t lo = lo_all > (uint64_t)n - 1 ? lo_all : (uint64_t)n - 1;
-      const uint64_t lvl_end = (1ull << D) - 2ull;
-      const uint64_t hi = hi_all < lvl_end ? hi_all : lvl_end;
-      if (lo <= hi) {
-        sd.present = 1;
-        sd.root = node;
-        sd.region_off = run;
-        sd.lo = (uint32_t)lo;
-        sd.hi = (uint32_t)hi;
-      }
-      return sd;
-    }
-    run += num_leaf_descendents(node, N);
-  }
-  return sd;
-}
-
 int do_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* diffs, const uint64_t* sizes,
                uint32_t count, uint32_t id) {
   using clk = std::chrono::high_resolution_clock;
@@ -613,9 +596,8 @@ int do_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* di
     a.is_main = idx == (int)id;
     a.cum = d->r_cum.p;
     a.ncum = (uint32_t)ncum;
-    const StraddleInfo sd = find_straddle(diffs[idx], hh, n, N);
-    B2D_CU(launch_restart_diff(a, sd, d->sm_count, d->stream));
-    d->launches += 9 + (sd.present ? 1 : 0);
+    B2D_CU(launch_restart_diff(a, &d->state.p->straddle, d->sm_count, d->stream));
+    d->launches += 9 + (straddle_query(n).count ? 2 : 0);
     if (bad_row) {
       B2D_CU(cudaStreamSynchronize(d->stream));
       d->restart_timers[0] = copy_time;
@@ -673,8 +655,6 @@ int b2d_create(uint32_t chunk_size, int hash_kind, b2d_dedup** out) {
       return cuda_status(e);
     }
     d->stream = d->own_stream;
-    const char* env = getenv("B2D_DISABLE_TMA");
-    d->allow_tma = !(env && env[0] == '1');
     *out = d;
     return B2D_OK;
   })
@@ -796,6 +776,17 @@ int b2d_restart_files(b2d_dedup* d, void* d_out, uint64_t len, const char* const
   })
 }
 
+int b2d_set_param(b2d_dedup* d, const char* name, int64_t value) {
+  if (!d || !name) return B2D_ERR_ARG;
+  const std::string k(name);
+  if (k == "leaf_tma") d->tune.allow_tma = value != 0;
+  else if (k == "leaf_stages" && value >= 0 && value <= 16) d->tune.stages = (int)value;
+  else if (k == "leaf_ctas_per_sm" && value >= 0 && value <= 8) d->tune.ctas_per_sm = (int)value;
+  else if (k == "map_max_load_pct" && value >= 10 && value <= 90) d->map_max_load = value / 100.0;
+  else return B2D_ERR_ARG;
+  return B2D_OK;
+}
+
 int b2d_num_first_ocur(b2d_dedup* d, uint64_t* out) {
   if (!d || !out) return B2D_ERR_ARG;
   *out = d->F;
@@ -850,9 +841,9 @@ int b2d_debug_tree(b2d_dedup* d, void* dst, uint64_t nodes) {
   B2D_CU(cudaStreamSynchronize(d->stream));
   return B2D_OK;
 }
-int b2d_debug_labels(b2d_dedup* d, void* dst, uint64_t nodes) {
-  if (!d || !dst || nodes > d->N || !d->lab.p) return B2D_ERR_ARG;
-  B2D_CU(cudaMemcpyAsync(dst, d->lab.p, nodes, cudaMemcpyDeviceToHost, d->stream));
+int b2d_debug_labels(b2d_dedup* d, void* dst, uint64_t leaves) {
+  if (!d || !dst || leaves > d->n || !d->leaflab.p) return B2D_ERR_ARG;
+  B2D_CU(cudaMemcpyAsync(dst, d->leaflab.p, leaves, cudaMemcpyDeviceToHost, d->stream));
   B2D_CU(cudaStreamSynchronize(d->stream));
   return B2D_OK;
 }

@@ -19,18 +19,21 @@ struct LeafArgs {
   int baseline;
   uint32_t cur;
   Digest* tree;
-  uint8_t* lab;
+  uint8_t* leaflab;   // per chunk: label of leaf n-1+c
+  uint8_t* dupflag;   // per chunk: leaf shares a new digest with another leaf (see leaf.cu)
   MapView map;
   DevStatus* st;
 };
 
 struct ForestArgs {
   Digest* tree;
-  uint8_t* lab;
+  uint8_t* lab;             // per node: labels handed from one band to the next
+  uint8_t* leaflab;         // per chunk: leaf labels (relabelled in place by phase 1)
   uint8_t* push;
   MapView map;
   DevStatus* st;
   const int* zero_exists;   // baseline: does the all-zero digest exist in the map
+  uint8_t* dupflag;         // per chunk, set by the leaf stage, cleared by phase 1
   uint32_t n, N, D;         // chunks, nodes, deepest level
   uint32_t cur;
   int kind;
@@ -54,12 +57,15 @@ struct DiffArgs {
   uint64_t len;
   uint32_t cs, n, N, D, cur, baseline_id;
   Digest* tree;
-  const uint8_t* push;
+  uint8_t* push;          // cleared by the compaction
   MapView map;
   DevStatus* st;
   DevMeta* meta;
   uint32_t* first_list;   // F node ids, canonical order
   uint32_t* shift_list;   // S node ids, canonical order
+  uint32_t* tmp_first;    // F node ids, node order
+  uint32_t* tmp_shift;    // S node ids, node order
+  uint32_t* levels;       // 2 x 34 level-run starts of the node-order lists
   uint32_t* region_off;   // F exclusive chunk offsets, then T
   uint32_t* sprev;        // S source node ids
   uint32_t* skey;         // S source checkpoint ids
@@ -70,9 +76,17 @@ struct DiffArgs {
   uint8_t* diff;          // device diff buffer
 };
 
-int launch_leaves(const LeafArgs& a, int sm_count, bool allow_tma, cudaStream_t stream);
+// Tunables of the staged leaf kernel (0 = default).  Chosen per workload by the autotuner.
+struct LeafTuning {
+  int allow_tma = 1;
+  int stages = 0;        // TMA ring depth per CTA (default: a 64 KB ring)
+  int ctas_per_sm = 0;   // resident CTAs per SM (default 3)
+};
+int launch_leaves(const LeafArgs& a, int sm_count, const LeafTuning& tune, cudaStream_t stream);
 cudaError_t launch_forest(const ForestArgs& a, int phase, cudaStream_t stream);
+int forest_launch_count(uint32_t D);
 cudaError_t launch_zero_exists(const MapView& m, int* flag, cudaStream_t stream);
+cudaError_t launch_baseline_inserts(const ForestArgs& a, int sm_count, cudaStream_t stream);
 cudaError_t launch_collect_diff(const DiffArgs& a, int sm_count, cudaStream_t stream);
 
 }  // namespace b2d

@@ -1,11 +1,16 @@
 // Merkle forest stages, level-fused.
 //
 // The reference walks the heap one level per launch, twice (src/tree_approach.cpp:116-224
-// baseline, :371-477 incremental): ~2 log2(N) launches.  Here a launch covers a band of up to
-// FOREST_BAND_LEVELS levels: each CTA owns the subtree under one node of the band's top
-// level, keeps the labels of the level it is working on in shared memory, and climbs the
-// band with one __syncthreads per level.  Labels cross band boundaries through `lab` (only
-// the band-top nodes are written).  A 2^25-chunk tree needs three bands per stage.
+// baseline, :371-477 incremental): ~2 log2(N) launches.  Here one launch reduces 12 levels:
+// a CTA of 256 threads owns the subtree of 4096 input nodes under one node 12 levels up;
+//   * each thread folds 16 consecutive input labels through 4 levels in registers,
+//   * each warp folds its 32 thread results through 5 levels with shuffles,
+//   * warp 0 folds the 8 warp results through the last 3 levels.
+// Labels cross band boundaries through `lab` (only band outputs are written).  A subtree whose
+// 16 inputs are all FIXED (phase 2) or contain no first occurrence (phase 1) is folded without
+// touching memory, which is the common case of an incremental checkpoint.  The few levels left
+// above the last full band (and trees with fewer than 12 levels) use forest_band_kernel, which
+// walks a band level by level through shared memory.
 //
 // Phase 1 (FIRST forest): relabel leaves whose digest's lowest-index owner is another leaf
 //   ("Choose first occurrences", :100-114 / :353-369), then every inner node with two
@@ -17,6 +22,8 @@
 //   every inner node (:218-224); this is reproduced with `zero_exists`.
 // Map priorities reproduce the sequential insert order: leaves 0, phase-1 parents
 // 1 + height, baseline per-level inserts 64 + height (height = D - level).
+// `push` holds only nonzero flags: it is all-zero between checkpoints (the compaction clears
+// what it reads), so a region-free subtree writes nothing.
 #include "dedup_kernels.cuh"
 #include "hash.cuh"
 #include "map.cuh"
@@ -24,77 +31,90 @@
 namespace b2d {
 
 constexpr uint32_t FOREST_THREADS = 512;
+constexpr uint32_t FAST_THREADS = 256;
+constexpr uint32_t FAST_LEVELS = 12;      // 4 in-thread + 5 warp + 3 CTA
+constexpr uint8_t NONE_LABEL = 5;         // node index beyond the tree
 
 __device__ __forceinline__ uint8_t push_flag(uint8_t label) {
   return label == SHIFT_DUPL ? PUSH_SHIFT : (label == FIRST_OCUR ? PUSH_FIRST : PUSH_NONE);
 }
 
+// phase-1 parent insert, priority 1 + height (:133, :390).  The rare heavy paths (hashing,
+// map probes) are kept out of line so the label folds stay small in the instruction cache.
+__device__ __noinline__ void insert_first_parent(const ForestArgs& a, uint32_t x, const Digest& d) {
+  const uint32_t height = a.D - node_level(x);
+  const unsigned long long v = ((unsigned long long)(1u + height) << 32) | x;
+  const MapRef ref = map_insert(a.map, d, v, a.cur, a.st);
+  if (ref.found && !ref.inserted) map_merge_current(a.map, ref.slot, v, a.cur);
+}
+
+__device__ __noinline__ void hash_first_parent(const ForestArgs& a, uint32_t x) {
+  const Digest d = hash_pair(a.kind, a.tree[2u * x + 1u], a.tree[2u * x + 2u]);
+  a.tree[x] = d;
+  insert_first_parent(a, x, d);
+}
+
+// two shifted children: the parent is a shifted duplicate only if its digest is already known;
+// the baseline tests the stale (zero) digest instead (:202 vs :459)
+__device__ __noinline__ uint8_t shift_pair(const ForestArgs& a, uint32_t x) {
+  const uint32_t l = 2u * x + 1u, r = 2u * x + 2u;
+  bool exists;
+  if (a.baseline) {
+    exists = *a.zero_exists != 0;
+  } else {
+    const Digest d = hash_pair(a.kind, a.tree[l], a.tree[r]);
+    a.tree[x] = d;
+    exists = map_find(a.map, d) <= a.map.cap;
+  }
+  if (exists) return SHIFT_DUPL;
+  a.push[l] = PUSH_SHIFT;
+  a.push[r] = PUSH_SHIFT;
+  return DONE;
+}
+
+__device__ __noinline__ void hash_baseline_parent(const ForestArgs& a, uint32_t x) {
+  a.tree[x] = hash_pair(a.kind, a.tree[2u * x + 1u], a.tree[2u * x + 2u]);   // inserted by baseline_insert_kernel
+}
+
 template <int PHASE>
 __device__ __forceinline__ uint8_t forest_node(const ForestArgs& a, uint32_t x, uint8_t ll, uint8_t rl) {
-  const uint32_t l = 2u * x + 1u, r = 2u * x + 2u;
-  const uint32_t height = a.D - node_level(x);
   if constexpr (PHASE == 1) {
     if (ll == FIRST_OCUR && rl == FIRST_OCUR) {
-      const Digest d = hash_pair(a.kind, a.tree[l], a.tree[r]);
-      a.tree[x] = d;
-      const unsigned long long v = ((unsigned long long)(1u + height) << 32) | x;
-      const MapRef ref = map_insert(a.map, d, v, a.cur, a.st);
-      if (ref.found && !ref.inserted) map_merge_current(a.map, ref.slot, v, a.cur);
+      hash_first_parent(a, x);
       return FIRST_OCUR;
     }
     return DONE;
   } else {
-    uint8_t out = DONE;
-    uint8_t pl = PUSH_NONE, pr = PUSH_NONE;
+    uint8_t out;
     if (ll != rl) {
       out = DONE;
-      pl = push_flag(ll);
-      pr = push_flag(rl);
-    } else if (ll == FIXED_DUPL) {
-      out = FIXED_DUPL;
+      const uint8_t pl = push_flag(ll), pr = push_flag(rl);
+      if (pl) a.push[2u * x + 1u] = pl;
+      if (pr) a.push[2u * x + 2u] = pr;
     } else if (ll == SHIFT_DUPL) {
-      bool exists;
-      if (a.baseline) {
-        exists = *a.zero_exists != 0;
-      } else {
-        const Digest d = hash_pair(a.kind, a.tree[l], a.tree[r]);
-        a.tree[x] = d;
-        exists = map_find(a.map, d) <= a.map.cap;
-      }
-      if (exists) {
-        out = SHIFT_DUPL;
-      } else {
-        out = DONE;
-        pl = PUSH_SHIFT;
-        pr = PUSH_SHIFT;
-      }
-    } else if (ll == FIRST_OCUR) {
-      out = FIRST_OCUR;
+      out = shift_pair(a, x);
+    } else {
+      out = ll;   // FIXED, FIRST or DONE pairs keep the label
     }
-    a.push[l] = pl;
-    a.push[r] = pr;
-    if (a.baseline) {
-      const Digest d = hash_pair(a.kind, a.tree[l], a.tree[r]);
-      a.tree[x] = d;
-      const unsigned long long v = ((unsigned long long)(64u + height) << 32) | x;
-      const MapRef ref = map_insert(a.map, d, v, a.cur, a.st);
-      if (ref.found && !ref.inserted) map_merge_current(a.map, ref.slot, v, a.cur);
-    }
+    if (a.baseline) hash_baseline_parent(a, x);
     return out;
   }
 }
 
-// label of a leaf as seen by this phase (phase 1 applies the lowest-index relabel)
+// label of a leaf as seen by this phase: phase 1 applies the lowest-index relabel to the
+// few first occurrences the leaf stage flagged as sharing their digest; every other first
+// occurrence is already its digest's owner
 template <int PHASE>
-__device__ __forceinline__ uint8_t forest_leaf(const ForestArgs& a, uint32_t x) {
-  uint8_t lab = a.lab[x];
+__device__ __forceinline__ uint8_t leaf_view(const ForestArgs& a, uint32_t x, uint8_t lab) {
   if constexpr (PHASE == 1) {
-    if (lab == FIRST_OCUR) {
+    const uint32_t c = x - (a.n - 1u);
+    if (lab == FIRST_OCUR && a.dupflag[c]) {
+      a.dupflag[c] = 0;
       const uint64_t slot = map_find(a.map, a.tree[x]);
       if (slot <= a.map.cap) {
         if (map_tree(a.map, slot) == a.cur && map_node(a.map, slot) != x) {
           lab = SHIFT_DUPL;
-          a.lab[x] = lab;
+          a.leaflab[c] = lab;
         }
       } else {
         set_error(a.st, DERR_INTERNAL, 10);
@@ -103,8 +123,258 @@ __device__ __forceinline__ uint8_t forest_leaf(const ForestArgs& a, uint32_t x) 
   }
   return lab;
 }
+template <int PHASE>
+__device__ __forceinline__ uint8_t forest_leaf(const ForestArgs& a, uint32_t x) {
+  return leaf_view<PHASE>(a, x, a.leaflab[x - (a.n - 1u)]);
+}
 
-// One band: levels [top, bot] (top <= bot <= D).  CTA b owns node (2^top - 1 + b).
+// label of node x given its children's labels: absent node, leaf (level D-1 leaves of a tree
+// whose chunk count is not a power of two), or inner node
+template <int PHASE>
+__device__ __forceinline__ uint8_t combine(const ForestArgs& a, uint64_t x, uint8_t ll, uint8_t rl) {
+  if (x >= a.N) return NONE_LABEL;
+  if (x >= (uint64_t)a.n - 1u) return forest_leaf<PHASE>(a, (uint32_t)x);
+  return forest_node<PHASE>(a, (uint32_t)x, ll, rl);
+}
+
+// label of an input node of a band: a leaf, or the output of the band below
+template <int PHASE>
+__device__ __forceinline__ uint8_t input_label(const ForestArgs& a, uint64_t x) {
+  if (x >= a.N) return NONE_LABEL;
+  if (x >= (uint64_t)a.n - 1u) return forest_leaf<PHASE>(a, (uint32_t)x);
+  return a.lab[x];
+}
+
+// band output: hand the label to the next band, or settle the whole-tree region at the root
+// (first = [0] when the root is a first occurrence, :127-129 / :392-399)
+template <int PHASE>
+__device__ __forceinline__ void band_output(const ForestArgs& a, uint64_t x, uint8_t lab) {
+  if (x == 0) {
+    if (PHASE == 2 && a.n >= 2u && lab == FIRST_OCUR) a.push[0] = PUSH_FIRST;
+  } else if (x < (uint64_t)a.n - 1u) {
+    a.lab[x] = lab;
+  }
+}
+
+// pair-AND of a bit mask: bit j of the result = bits 2j and 2j+1 of m (m has 2w bits)
+__device__ __forceinline__ uint32_t pair_and(uint32_t m, int w) {
+  uint32_t r = 0;
+#pragma unroll
+  for (int j = 0; j < 8; j++)
+    if (j < w) r |= ((m >> (2 * j)) & (m >> (2 * j + 1)) & 1u) << j;
+  return r;
+}
+
+// Phase-1 band: 12 levels above inputs at level `in`.  The first-occurrence labels are folded
+// as bit masks (a parent is a first occurrence iff both children are); the parents found are
+// recorded in a per-CTA bit set, and only then hashed and inserted level by level with all
+// threads of the CTA, so a run of new chunks costs one hash per node spread over the CTA
+// instead of a serial chain per thread.
+constexpr uint32_t FF_WORDS = 128;   // 4095 bits: heights 1..12 of a 4096-input band
+__device__ __forceinline__ uint32_t ff_base(uint32_t k) {   // first bit of band height k
+  return 4096u - (8192u >> k);
+}
+__global__ void __launch_bounds__(FAST_THREADS) forest_first_kernel(ForestArgs a, uint32_t in) {
+  __shared__ uint32_t ff[FF_WORDS];
+  __shared__ uint32_t wbits[FAST_THREADS / 32];
+  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+  if (t < FF_WORDS) ff[t] = 0;
+  __syncthreads();
+  const uint64_t root = ((1ull << (in - FAST_LEVELS)) - 1ull) + blockIdx.x;
+  const uint64_t x0 = (root << FAST_LEVELS) + ((1ull << FAST_LEVELS) - 1ull) + 16ull * t;
+  const uint64_t p0 = (x0 - 1ull) >> 1;   // first height-1 node of this thread
+  uint32_t m0 = 0;        // first-occurrence inputs
+  uint32_t m1 = 0;        // first-occurrence height-1 nodes (leaf or inner)
+  uint32_t inner1 = 0xffu;
+  if (in == a.D && (a.n & (a.n - 1u)) == 0) {
+    const uint4 w = *reinterpret_cast<const uint4*>(a.leaflab + (x0 - (a.n - 1u)));
+    const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      // exact per-byte zero test (FIRST = 0): no borrow crosses bytes
+      const uint32_t z = ~(((ws[k] & 0x7f7f7f7fu) + 0x7f7f7f7fu) | ws[k] | 0x7f7f7f7fu);
+      m0 |= ((z >> 7) & 1u | (z >> 14) & 2u | (z >> 21) & 4u | (z >> 28) & 8u) << (4 * k);
+    }
+    if (m0) {   // lowest-index relabel of the first occurrences flagged by the leaf stage
+      for (int j = 0; j < 16; j++)
+        if ((m0 >> j) & 1u)
+          if (leaf_view<1>(a, (uint32_t)(x0 + j), FIRST_OCUR) != FIRST_OCUR) m0 &= ~(1u << j);
+    }
+    m1 = pair_and(m0, 8);
+  } else {
+#pragma unroll
+    for (int j = 0; j < 16; j++) m0 |= (uint32_t)(input_label<1>(a, x0 + j) == FIRST_OCUR) << j;
+    const uint32_t both = pair_and(m0, 8);
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const uint64_t p = p0 + j;
+      uint32_t bit;
+      if (p >= a.N) { bit = 0; inner1 &= ~(1u << j); }
+      else if (p >= (uint64_t)a.n - 1u) { bit = forest_leaf<1>(a, (uint32_t)p) == FIRST_OCUR; inner1 &= ~(1u << j); }
+      else bit = (both >> j) & 1u;
+      m1 |= bit << j;
+    }
+  }
+  const uint32_t m2 = pair_and(m1, 4), m3 = pair_and(m2, 2), m4 = pair_and(m3, 1);
+  // record parents to hash (inner nodes only): heights 1..4 of this thread
+  if (m1 & inner1) atomicOr(&ff[(ff_base(1) + 8u * t) >> 5], (m1 & inner1) << ((8u * t) & 31u));
+  if (m2) atomicOr(&ff[(ff_base(2) + 4u * t) >> 5], m2 << ((4u * t) & 31u));
+  if (m3) atomicOr(&ff[(ff_base(3) + 2u * t) >> 5], m3 << ((2u * t) & 31u));
+  if (m4) atomicOr(&ff[(ff_base(4) + t) >> 5], 1u << (t & 31u));
+  // warp: heights 5..9
+  uint32_t b = m4;
+#pragma unroll
+  for (int s = 0; s < 5; s++) {
+    const uint32_t rb = __shfl_down_sync(0xffffffffu, b, 1u << s);
+    if ((lane & ((2u << s) - 1u)) == 0) {
+      b &= rb;
+      if (b) {
+        const uint32_t idx = t >> (s + 1);
+        atomicOr(&ff[(ff_base(5 + s) + idx) >> 5], 1u << ((ff_base(5 + s) + idx) & 31u));
+      }
+    }
+  }
+  if (lane == 0) wbits[warp] = b;
+  __syncthreads();
+  if (warp == 0) {
+    b = lane < FAST_THREADS / 32 ? wbits[lane] : 0u;
+#pragma unroll
+    for (int s = 0; s < 3; s++) {
+      const uint32_t rb = __shfl_down_sync(0xffffffffu, b, 1u << s);
+      if ((lane & ((2u << s) - 1u)) == 0 && lane < FAST_THREADS / 32) {
+        b &= rb;
+        if (b) {
+          const uint32_t idx = lane >> (s + 1);
+          atomicOr(&ff[(ff_base(10 + s) + idx) >> 5], 1u << ((ff_base(10 + s) + idx) & 31u));
+        }
+      }
+    }
+    if (lane == 0) band_output<1>(a, root, b ? FIRST_OCUR : DONE);
+  }
+  __syncthreads();
+  if (!__syncthreads_or(t < FF_WORDS && ff[t] != 0)) return;
+  // hash the recorded parents one height at a time (a parent needs its children's digests);
+  // the map inserts wait until every digest is known, then run spread evenly over the CTA
+  for (uint32_t k = 1; k <= FAST_LEVELS; k++) {
+    const uint32_t cnt = 4096u >> k, base = ff_base(k);
+    const uint64_t first = (root << (FAST_LEVELS - k)) + (1ull << (FAST_LEVELS - k)) - 1ull;
+    for (uint32_t i = t; i < cnt; i += FAST_THREADS) {
+      const uint32_t bit = base + i;
+      if ((ff[bit >> 5] >> (bit & 31u)) & 1u) {
+        const uint32_t x = (uint32_t)(first + i);
+        a.tree[x] = hash_pair(a.kind, a.tree[2u * x + 1u], a.tree[2u * x + 2u]);
+      }
+    }
+    __syncthreads();
+  }
+  // inserts: rank the set bits (prefix of per-word counts), thread t takes ranks t, t+256, ...
+  __shared__ uint32_t wpre[FF_WORDS + 1];
+  if (t < FF_WORDS) wpre[t + 1] = __popc(ff[t]);
+  if (t == 0) wpre[0] = 0;
+  __syncthreads();
+  if (t == 0)
+    for (uint32_t w = 1; w <= FF_WORDS; w++) wpre[w] += wpre[w - 1];
+  __syncthreads();
+  const uint32_t total = wpre[FF_WORDS];
+  for (uint32_t r = t; r < total; r += FAST_THREADS) {
+    uint32_t lo = 0, hi = FF_WORDS;   // word with wpre[w] <= r < wpre[w+1]
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (wpre[mid] <= r) lo = mid; else hi = mid;
+    }
+    uint32_t word = ff[lo], skip = r - wpre[lo];
+    while (skip--) word &= word - 1u;   // drop the lower set bits
+    const uint32_t bit = lo * 32u + (__ffs(word) - 1u);
+    uint32_t k = 1;                     // band height of this bit
+    while (k < FAST_LEVELS && bit >= ff_base(k + 1)) k++;
+    const uint64_t first = (root << (FAST_LEVELS - k)) + (1ull << (FAST_LEVELS - k)) - 1ull;
+    const uint32_t x = (uint32_t)(first + (bit - ff_base(k)));
+    insert_first_parent(a, x, a.tree[x]);
+  }
+}
+
+// Fast band: inputs at level `in`, outputs at level in - 12.
+template <int PHASE>
+__global__ void __launch_bounds__(FAST_THREADS) forest_fast_kernel(ForestArgs a, uint32_t in) {
+  __shared__ uint8_t wlab[FAST_THREADS / 32];
+  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+  const uint64_t root = ((1ull << (in - FAST_LEVELS)) - 1ull) + blockIdx.x;
+  const uint64_t x0 = (root << FAST_LEVELS) + ((1ull << FAST_LEVELS) - 1ull) + 16ull * t;
+  uint8_t v[16];
+  bool fast = !a.baseline;
+  if (in == a.D && (a.n & (a.n - 1u)) == 0) {
+    // power-of-two leaf count, leaf band: the 16 inputs are chunks 16t.. of this CTA's 4096,
+    // one aligned 16-byte load; FIXED = 0x01 bytes, FIRST = 0x00 bytes
+    const uint4 w = *reinterpret_cast<const uint4*>(a.leaflab + (x0 - (a.n - 1u)));
+    if (PHASE == 2) {
+      fast = fast && w.x == 0x01010101u && w.y == 0x01010101u && w.z == 0x01010101u && w.w == 0x01010101u;
+    } else {
+      const uint32_t zx = (w.x - 0x01010101u) & ~w.x, zy = (w.y - 0x01010101u) & ~w.y;
+      const uint32_t zz = (w.z - 0x01010101u) & ~w.z, zw = (w.w - 0x01010101u) & ~w.w;
+      fast = fast && (((zx | zy | zz | zw) & 0x80808080u) == 0);   // no zero byte at all: no FIRST
+    }
+    if (!fast) {
+      const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+      for (int j = 0; j < 16; j++) v[j] = leaf_view<PHASE>(a, (uint32_t)(x0 + j), (uint8_t)(ws[j >> 2] >> (8 * (j & 3))));
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 16; j++) v[j] = input_label<PHASE>(a, x0 + j);
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+      if (PHASE == 2) fast = fast && v[j] == FIXED_DUPL;
+      else fast = fast && v[j] != FIRST_OCUR && v[j] != NONE_LABEL;
+    }
+  }
+  uint8_t lab;
+  if (fast) {
+    lab = PHASE == 2 ? FIXED_DUPL : DONE;
+  } else {
+    uint64_t first = x0;
+#pragma unroll
+    for (int width = 8; width >= 1; width >>= 1) {
+      first = (first - 1ull) >> 1;
+#pragma unroll
+      for (int j = 0; j < width; j++) v[j] = combine<PHASE>(a, first + j, v[2 * j], v[2 * j + 1]);
+    }
+    lab = v[0];
+  }
+  // warp: 5 levels
+  uint64_t y = (root << 8) + 255ull + t;
+#pragma unroll
+  for (int s = 0; s < 5; s++) {
+    __syncwarp();   // digests written by the partner lane at the previous level are visible
+    const uint8_t rl = (uint8_t)__shfl_down_sync(0xffffffffu, (uint32_t)lab, 1u << s);
+    if ((lane & ((2u << s) - 1u)) == 0) {
+      y = (y - 1ull) >> 1;
+      if (!(PHASE == 2 && !a.baseline && lab == FIXED_DUPL && rl == FIXED_DUPL) &&
+          !(PHASE == 1 && !a.baseline && lab != FIRST_OCUR && lab != NONE_LABEL && rl != NONE_LABEL))
+        lab = combine<PHASE>(a, y, lab, rl);
+      else if (PHASE == 1)
+        lab = DONE;
+    }
+  }
+  if (lane == 0) wlab[warp] = lab;
+  __syncthreads();
+  if (warp == 0) {
+    lab = lane < FAST_THREADS / 32 ? wlab[lane] : NONE_LABEL;
+    y = (root << 3) + 7ull + lane;
+#pragma unroll
+    for (int s = 0; s < 3; s++) {
+      __syncwarp();
+      const uint8_t rl = (uint8_t)__shfl_down_sync(0xffffffffu, (uint32_t)lab, 1u << s);
+      if ((lane & ((2u << s) - 1u)) == 0 && lane < FAST_THREADS / 32) {
+        y = (y - 1ull) >> 1;
+        lab = combine<PHASE>(a, y, lab, rl);
+      }
+    }
+    if (lane == 0) band_output<PHASE>(a, root, lab);
+  }
+}
+
+// General band: levels [top, bot] (top <= bot <= D), level by level through shared memory.
+// Nodes at level `bot` are leaves or combine children at level bot+1 read from `lab`.
 template <int PHASE>
 __global__ void __launch_bounds__(FOREST_THREADS) forest_band_kernel(ForestArgs a, uint32_t top, uint32_t bot) {
   __shared__ uint8_t buf[2][1u << (FOREST_BAND_LEVELS - 1)];
@@ -117,32 +387,15 @@ __global__ void __launch_bounds__(FOREST_THREADS) forest_band_kernel(ForestArgs 
     const uint64_t base = (root << k) + width - 1ull;
     for (uint64_t i = threadIdx.x; i < width; i += blockDim.x) {
       const uint64_t x = base + i;
-      uint8_t lab = DONE;
-      if (x < a.N) {
-        if (x >= (uint64_t)a.n - 1u) {
-          lab = forest_leaf<PHASE>(a, (uint32_t)x);
-        } else {
-          uint8_t ll, rl;
-          if (k == (int)H) {   // children belong to the band below (written to lab)
-            ll = a.lab[2u * (uint32_t)x + 1u];
-            rl = a.lab[2u * (uint32_t)x + 2u];
-          } else {
-            ll = below[2 * i];
-            rl = below[2 * i + 1];
-          }
-          lab = forest_node<PHASE>(a, (uint32_t)x, ll, rl);
-        }
+      uint8_t lab;
+      if (k == (int)H) {
+        if (x >= a.N || x >= (uint64_t)a.n - 1u) lab = input_label<PHASE>(a, x);
+        else lab = combine<PHASE>(a, x, a.lab[2 * x + 1], a.lab[2 * x + 2]);
+      } else {
+        lab = combine<PHASE>(a, x, below[2 * i], below[2 * i + 1]);
       }
       if (k > 0) here[i] = lab;
-      else if (x < a.N) {
-        // band top: hand the label to the next band up; the tree root decides the
-        // whole-buffer first-occurrence region (:127-129 / :392-399)
-        if (x == 0) {
-          if (PHASE == 2) a.push[0] = (a.n >= 2u && lab == FIRST_OCUR) ? PUSH_FIRST : PUSH_NONE;
-        } else {
-          if (x < (uint64_t)a.n - 1u) a.lab[x] = lab;   // leaves already hold their label
-        }
-      }
+      else band_output<PHASE>(a, x, lab);
     }
     __syncthreads();
     uint8_t* t = below;
@@ -152,11 +405,19 @@ __global__ void __launch_bounds__(FOREST_THREADS) forest_band_kernel(ForestArgs 
 }
 
 cudaError_t launch_forest(const ForestArgs& a, int phase, cudaStream_t stream) {
-  if (a.N <= 1) {   // one chunk: no inner nodes; the reference never pushes a region
-    if (phase == 2) return cudaMemsetAsync(a.push, 0, 1, stream);
-    return cudaSuccess;
+  if (a.N <= 1) return cudaSuccess;   // one chunk: no inner nodes; the reference never pushes a region
+  uint32_t in = a.D;                  // labels at level `in` are known (leaves, or a band's output)
+  while (in >= FAST_LEVELS) {
+    const uint32_t ctas = 1u << (in - FAST_LEVELS);
+    if (phase == 1) forest_first_kernel<<<ctas, FAST_THREADS, 0, stream>>>(a, in);
+    else forest_fast_kernel<2><<<ctas, FAST_THREADS, 0, stream>>>(a, in);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    in -= FAST_LEVELS;
   }
-  int bot = (int)a.D;
+  if (in == 0) return cudaSuccess;    // the root was a fast band output
+  // remaining levels [0, bot]: bot = D when no fast band ran (start from the leaves), else in-1
+  int bot = (in == a.D) ? (int)a.D : (int)in - 1;
   while (bot >= 0) {
     int top = bot - (int)FOREST_BAND_LEVELS + 1;
     if (top < 0) top = 0;
@@ -170,6 +431,22 @@ cudaError_t launch_forest(const ForestArgs& a, int phase, cudaStream_t stream) {
   return cudaSuccess;
 }
 
+int forest_launch_count(uint32_t D) {
+  if (D == 0) return 0;
+  int c = 0;
+  uint32_t in = D;
+  while (in >= FAST_LEVELS) { c++; in -= FAST_LEVELS; }
+  if (in == 0) return c;
+  int bot = (in == D) ? (int)D : (int)in - 1;
+  while (bot >= 0) {
+    int top = bot - (int)FOREST_BAND_LEVELS + 1;
+    if (top < 0) top = 0;
+    c++;
+    bot = top - 1;
+  }
+  return c;
+}
+
 __global__ void zero_exists_kernel(MapView m, int* flag) {
   Digest z;
   z.w[0] = z.w[1] = z.w[2] = z.w[3] = 0u;
@@ -178,6 +455,21 @@ __global__ void zero_exists_kernel(MapView m, int* flag) {
 
 cudaError_t launch_zero_exists(const MapView& m, int* flag, cudaStream_t stream) {
   zero_exists_kernel<<<1, 1, 0, stream>>>(m, flag);
+  return cudaGetLastError();
+}
+
+// baseline "Insert entries" (:218-224): every inner node, priority 64 + height
+__global__ void baseline_insert_kernel(ForestArgs a) {
+  for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x + 1u < a.n; x += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t height = a.D - node_level((uint32_t)x);
+    const unsigned long long v = ((unsigned long long)(64u + height) << 32) | x;
+    const MapRef ref = map_insert(a.map, a.tree[x], v, a.cur, a.st);
+    if (ref.found && !ref.inserted) map_merge_current(a.map, ref.slot, v, a.cur);
+  }
+}
+
+cudaError_t launch_baseline_inserts(const ForestArgs& a, int sm_count, cudaStream_t stream) {
+  baseline_insert_kernel<<<(unsigned)sm_count * 8u, 256, 0, stream>>>(a);
   return cudaGetLastError();
 }
 

@@ -21,26 +21,36 @@ namespace b2d {
 constexpr uint32_t COMPACT_THREADS = 512;
 constexpr uint32_t SHIFT_GRID = 1184;   // 8 x 148 ranges for the shift-entry passes
 
-// node at canonical position p: level D (possibly partial) first, then full levels D-1..0
-__device__ __forceinline__ uint32_t canon_node(uint64_t p, uint32_t N, uint32_t D) {
-  const uint64_t first_deep = (1ull << D) - 1ull;
-  const uint64_t cnt_deep = (uint64_t)N - first_deep;
-  if (p < cnt_deep) return (uint32_t)(first_deep + p);
-  const uint64_t q = p - cnt_deep;
-  const uint64_t s = (1ull << D) - q;   // >= 2
-  const uint32_t L = 63u - (uint32_t)__clzll((long long)(s - 1ull));
-  return (uint32_t)(((1ull << L) - 1ull) + (q - ((1ull << D) - (1ull << (L + 1)))));
+// Region roots are flagged in `push` (node-indexed, zero-padded to a multiple of 16 nodes,
+// all-zero between checkpoints).  Compaction runs in node order with 16-byte loads; since the
+// canonical order is "level descending, node ascending" and node order is "level ascending,
+// node ascending", the canonical list is the node-order list with its per-level runs reversed,
+// which compact_permute_kernel applies after a per-level split of the node-order lists.
+__device__ __forceinline__ uint4 ld_push16(const uint8_t* push, uint64_t g) {
+  return reinterpret_cast<const uint4*>(push)[g];
+}
+__device__ __forceinline__ void count16(uint4 v, uint32_t& cf, uint32_t& cs) {
+  const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      const uint32_t f = (w[k] >> (8 * b)) & 0xffu;
+      cf += f == PUSH_FIRST;
+      cs += f == PUSH_SHIFT;
+    }
+  }
 }
 
 __global__ void __launch_bounds__(COMPACT_THREADS) compact_count_kernel(DiffArgs a) {
   __shared__ uint32_t sh[COMPACT_THREADS / 32 + 1];
+  const uint64_t groups = ((uint64_t)a.N + 15u) / 16u;
   uint64_t beg, end;
-  cta_range(a.N, blockIdx.x, gridDim.x, beg, end);
+  cta_range(groups, blockIdx.x, gridDim.x, beg, end);
   uint32_t cf = 0, cs = 0;
-  for (uint64_t p = beg + threadIdx.x; p < end; p += blockDim.x) {
-    const uint8_t f = a.push[canon_node(p, a.N, a.D)];
-    cf += f == PUSH_FIRST;
-    cs += f == PUSH_SHIFT;
+  for (uint64_t g = beg + threadIdx.x; g < end; g += blockDim.x) {
+    const uint4 v = ld_push16(a.push, g);
+    if (v.x | v.y | v.z | v.w) count16(v, cf, cs);
   }
   const uint32_t tf = block_reduce_sum(cf, sh);
   const uint32_t ts = block_reduce_sum(cs, sh);
@@ -67,26 +77,108 @@ __global__ void __launch_bounds__(1024) compact_scan_kernel(DiffArgs a, uint32_t
   }
 }
 
+// node-order lists of first / shift roots; clears the flags it consumed.  Each thread owns
+// COMPACT_GROUPS consecutive 16-node groups of a tile, so one block scan covers
+// COMPACT_THREADS * COMPACT_GROUPS * 16 nodes and the loads of a thread are independent.
+constexpr uint32_t COMPACT_GROUPS = 4;   // tile of 32768 nodes keeps both packed 16-bit counts exact
 __global__ void __launch_bounds__(COMPACT_THREADS) compact_write_kernel(DiffArgs a) {
   __shared__ uint32_t sh[COMPACT_THREADS / 32 + 1];
+  const uint64_t groups = ((uint64_t)a.N + 15u) / 16u;
   uint64_t beg, end;
-  cta_range(a.N, blockIdx.x, gridDim.x, beg, end);
+  cta_range(groups, blockIdx.x, gridDim.x, beg, end);
   uint32_t bf = a.partial2[2 * blockIdx.x], bs = a.partial2[2 * blockIdx.x + 1];
-  for (uint64_t t0 = beg; t0 < end; t0 += blockDim.x) {
-    const uint64_t p = t0 + threadIdx.x;
-    uint32_t node = 0;
-    uint8_t f = PUSH_NONE;
-    if (p < end) {
-      node = canon_node(p, a.N, a.D);
-      f = a.push[node];
+  constexpr uint32_t TILE = COMPACT_THREADS * COMPACT_GROUPS;
+  for (uint64_t t0 = beg; t0 < end; t0 += TILE) {
+    const uint64_t g0 = t0 + (uint64_t)threadIdx.x * COMPACT_GROUPS;
+    uint4 v[COMPACT_GROUPS];
+    uint32_t cf = 0, cs = 0, nzmask = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < COMPACT_GROUPS; j++) {
+      v[j] = make_uint4(0, 0, 0, 0);
+      if (g0 + j < end) v[j] = ld_push16(a.push, g0 + j);
     }
-    uint32_t tf, ts;
-    const uint32_t rf = block_excl_scan(f == PUSH_FIRST, sh, &tf);
-    const uint32_t rs = block_excl_scan(f == PUSH_SHIFT, sh, &ts);
-    if (f == PUSH_FIRST) a.first_list[bf + rf] = node;
-    if (f == PUSH_SHIFT) a.shift_list[bs + rs] = node;
-    bf += tf;
-    bs += ts;
+#pragma unroll
+    for (uint32_t j = 0; j < COMPACT_GROUPS; j++) {
+      if (v[j].x | v[j].y | v[j].z | v[j].w) {
+        nzmask |= 1u << j;
+        count16(v[j], cf, cs);
+      }
+    }
+    uint32_t tot;
+    const uint32_t ex = block_excl_scan((cf << 16) | cs, sh, &tot);
+    if (nzmask) {
+      uint32_t of = bf + (ex >> 16), os = bs + (ex & 0xffffu);
+#pragma unroll
+      for (uint32_t j = 0; j < COMPACT_GROUPS; j++) {
+        if (!((nzmask >> j) & 1u)) continue;
+        const uint32_t w[4] = {v[j].x, v[j].y, v[j].z, v[j].w};
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+#pragma unroll
+          for (int b = 0; b < 4; b++) {
+            const uint32_t f = (w[k] >> (8 * b)) & 0xffu;
+            const uint32_t node = (uint32_t)(16ull * (g0 + j)) + 4u * k + b;
+            if (f == PUSH_FIRST) a.tmp_first[of++] = node;
+            else if (f == PUSH_SHIFT) a.tmp_shift[os++] = node;
+          }
+        }
+        reinterpret_cast<uint4*>(a.push)[g0 + j] = make_uint4(0, 0, 0, 0);
+      }
+    }
+    bf += tot >> 16;
+    bs += tot & 0xffffu;
+  }
+}
+
+// warp-parallel lower bound: first index of sorted v[0..cnt) with v[idx] >= key (32-ary search)
+__device__ __forceinline__ uint32_t warp_lower_bound(const uint32_t* v, uint32_t cnt, uint64_t key) {
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t lo = 0, hi = cnt;
+  while (hi - lo > 32u) {
+    const uint32_t step = (hi - lo + 31u) / 32u;
+    const uint32_t probe = lo + lane * step;
+    const bool below = probe < hi && v[probe] < key;
+    const uint32_t c = __popc(__ballot_sync(0xffffffffu, below));
+    const uint32_t nlo = c ? lo + (c - 1u) * step + 1u : lo;
+    const uint32_t nhi = (c < 32u && lo + c * step < hi) ? lo + c * step : hi;
+    lo = nlo;
+    hi = nhi;
+  }
+  const bool below = lo + lane < hi && v[lo + lane] < key;
+  return lo + __popc(__ballot_sync(0xffffffffu, below));
+}
+
+// level runs of the node-order lists: levels[L] = start of level L in tmp_first,
+// levels[34 + L] in tmp_shift (L = 0..D+1); one warp per search
+__global__ void compact_levels_kernel(DiffArgs a) {
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t L = gw >> 1;
+  if (L > a.D + 1u) return;
+  const uint64_t key = (1ull << L) - 1ull;   // first node of level L
+  if ((gw & 1u) == 0) {
+    const uint32_t r = warp_lower_bound(a.tmp_first, a.meta->F, key);
+    if ((threadIdx.x & 31u) == 0) a.levels[L] = r;
+  } else {
+    const uint32_t r = warp_lower_bound(a.tmp_shift, a.meta->S, key);
+    if ((threadIdx.x & 31u) == 0) a.levels[34 + L] = r;
+  }
+}
+
+// canonical position of node-order entry i at level L: entries of deeper levels first
+__global__ void compact_permute_kernel(DiffArgs a) {
+  const uint32_t F = a.meta->F, S = a.meta->S;
+  const uint64_t tot = (uint64_t)F + S;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < tot; i += (uint64_t)gridDim.x * blockDim.x) {
+    const bool isf = i < F;
+    const uint32_t j = isf ? (uint32_t)i : (uint32_t)(i - F);
+    const uint32_t* lv = a.levels + (isf ? 0 : 34);
+    const uint32_t cnt = isf ? F : S;
+    const uint32_t node = isf ? a.tmp_first[j] : a.tmp_shift[j];
+    const uint32_t L = node_level(node);
+    // entries at levels deeper than L come first: cnt - (start of level L+1)
+    const uint32_t pos = (cnt - lv[L + 1]) + (j - lv[L]);
+    if (isf) a.first_list[pos] = node;
+    else a.shift_list[pos] = node;
   }
 }
 
@@ -292,8 +384,10 @@ __device__ __forceinline__ uint32_t find_region(const uint32_t* off, uint32_t F,
   return lo;
 }
 
-// LPC lanes copy one chunk with 16-byte vectors (chunk size a multiple of 16, 16-byte
-// aligned source and destination); the short last chunk is zero-padded (:643-645).
+// Data section: each warp owns a contiguous range of diff chunks.  The chunks of one region are
+// contiguous in both the buffer and the diff, so the warp finds the region of its first chunk
+// once and then walks forward; LPC lanes copy one chunk with 16-byte vectors (chunk size a
+// multiple of 16, both sides 16-byte aligned); the short last chunk is zero-padded (:643-645).
 template <uint32_t LPC>
 __global__ void __launch_bounds__(256) gather_vec_kernel(DiffArgs a) {
   const DevMeta m = *a.meta;
@@ -302,35 +396,50 @@ __global__ void __launch_bounds__(256) gather_vec_kernel(DiffArgs a) {
   const uint64_t gtid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   const uint64_t nthr = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t i = gtid; i < m.F; i += nthr) first_meta[i] = a.first_list[i];
+  if (m.T == 0) return;
+  constexpr uint32_t CPW = 32u / LPC;   // chunks per warp iteration
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t warp = gtid >> 5, nwarps = nthr >> 5;
+  uint64_t k0, k1;
+  cta_range(m.T, (uint32_t)warp, (uint32_t)nwarps, k0, k1);
+  if (k0 >= k1) return;
   const uint32_t units = a.cs / 16u;
-  const uint64_t group = gtid / LPC, ngroups = nthr / LPC;
-  const uint32_t sub = (uint32_t)(gtid % LPC);
-  for (uint64_t k = group; k < m.T; k += ngroups) {
-    const uint32_t r = find_region(a.region_off, m.F, k);
-    const uint32_t node = a.first_list[r];
-    const uint64_t chunk = (uint64_t)(leftmost_leaf(node, a.N) - (a.n - 1u)) + (k - a.region_off[r]);
-    if (chunk >= a.n) { set_error(a.st, DERR_INTERNAL, 40); continue; }
-    const uint64_t src_off = chunk * a.cs;
-    const uint4* src = reinterpret_cast<const uint4*>(a.data + src_off);
-    uint4* dst = reinterpret_cast<uint4*>(dst_base + k * a.cs);
-    const uint64_t avail = (chunk == a.n - 1u) ? a.len - src_off : a.cs;
-    if (avail == a.cs) {
-      for (uint32_t u = sub; u < units; u += LPC) dst[u] = __ldg(src + u);
-    } else {
-      const uint32_t full = (uint32_t)(avail / 16u);
-      for (uint32_t u = sub; u < units; u += LPC) {
-        if (u < full) {
-          dst[u] = __ldg(src + u);
+  uint32_t r = find_region(a.region_off, m.F, k0);
+  for (uint64_t k = k0; k < k1; k += CPW) {
+    const uint64_t kk = k + lane / LPC;
+    const uint32_t sub = lane % LPC;
+    uint32_t rr = r;
+    while (rr + 1u < m.F && a.region_off[rr + 1u] <= kk) rr++;
+    if (kk < k1) {
+      const uint32_t node = a.first_list[rr];
+      const uint64_t chunk = (uint64_t)(leftmost_leaf(node, a.N) - (a.n - 1u)) + (kk - a.region_off[rr]);
+      if (chunk >= a.n) {
+        set_error(a.st, DERR_INTERNAL, 40);
+      } else {
+        const uint64_t src_off = chunk * a.cs;
+        const uint4* src = reinterpret_cast<const uint4*>(a.data + src_off);
+        uint4* dst = reinterpret_cast<uint4*>(dst_base + kk * a.cs);
+        const uint64_t avail = (chunk == a.n - 1u) ? a.len - src_off : a.cs;
+        if (avail == a.cs) {
+          for (uint32_t u = sub; u < units; u += LPC) dst[u] = __ldg(src + u);
         } else {
-          uint8_t tmp[16];
-          const uint8_t* s8 = a.data + src_off + 16ull * u;
-          for (uint32_t b = 0; b < 16; b++) tmp[b] = (16ull * u + b < avail) ? s8[b] : 0u;
-          uint4 v;
-          memcpy(&v, tmp, 16);
-          dst[u] = v;
+          const uint32_t full = (uint32_t)(avail / 16u);
+          for (uint32_t u = sub; u < units; u += LPC) {
+            if (u < full) {
+              dst[u] = __ldg(src + u);
+            } else {
+              uint8_t tmp[16];
+              const uint8_t* s8 = a.data + src_off + 16ull * u;
+              for (uint32_t b = 0; b < 16; b++) tmp[b] = (16ull * u + b < avail) ? s8[b] : 0u;
+              uint4 v;
+              memcpy(&v, tmp, 16);
+              dst[u] = v;
+            }
+          }
         }
       }
     }
+    r = __reduce_max_sync(0xffffffffu, rr);
   }
 }
 
@@ -365,6 +474,8 @@ cudaError_t launch_collect_diff(const DiffArgs& a, int sm_count, cudaStream_t st
   compact_count_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);
   compact_scan_kernel<<<1, 1024, 0, stream>>>(a, g);
   compact_write_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);
+  compact_levels_kernel<<<(2u * (a.D + 2u) * 32u + 255u) / 256u, 256, 0, stream>>>(a);
+  compact_permute_kernel<<<(uint32_t)sm_count * 2u, 256, 0, stream>>>(a);
   region_count_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);
   region_scan_kernel<<<1, 1024, 0, stream>>>(a, g);
   region_write_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);

@@ -17,35 +17,50 @@
 
 namespace b2d {
 
+// Several leaves of this checkpoint with one new digest: the lowest index owns it ("Choose
+// first occurrences", :100-114 / :353-369).  Every atomicMin that finds a value already in the
+// slot flags both its own leaf and the value it saw, so after the launch every leaf that
+// shares a new digest is flagged; only flagged leaves need the owner lookup in the forest.
+__device__ __forceinline__ void flag_shared(const LeafArgs& a, uint32_t chunk, unsigned long long prev) {
+  if (prev != ~0ull) {
+    a.dupflag[chunk] = 1;
+    const uint32_t other = (uint32_t)prev - (a.n - 1u);
+    if (other < a.n) a.dupflag[other] = 1;
+  }
+}
+
 // Per-leaf decision, same order of tests as the reference:
 //  baseline:    insert, then compare with the (fresh, all-zero) tree entry
 //  incremental: compare with the prior digest first; FIXED leaves skip the insert because
 //               their digest is already present from the checkpoint that stored it.
-__device__ __forceinline__ void leaf_finish(const LeafArgs& a, uint32_t chunk, const Digest& d) {
+__device__ __forceinline__ void leaf_finish(const LeafArgs& a, uint32_t chunk, const Digest& d, const Digest& old) {
   const uint32_t leaf = a.n - 1u + chunk;
   uint8_t label = DONE;
-  if (a.baseline) {
+  const bool fixed = a.baseline ? digest_zero(d) : digest_eq(d, old);
+  if (a.baseline || !fixed) {
     const MapRef r = map_insert(a.map, d, (unsigned long long)leaf, a.cur, a.st);
-    if (digest_zero(d)) label = FIXED_DUPL;
-    else if (r.inserted) label = FIRST_OCUR;
-    else if (r.found) label = map_merge_current(a.map, r.slot, leaf, a.cur) ? FIRST_OCUR : SHIFT_DUPL;
-    a.tree[leaf] = d;
-  } else {
-    const Digest old = a.tree[leaf];
-    if (digest_eq(d, old)) {
-      label = FIXED_DUPL;
-    } else {
-      const MapRef r = map_insert(a.map, d, (unsigned long long)leaf, a.cur, a.st);
-      if (r.inserted) {
-        label = FIRST_OCUR;
-        a.tree[leaf] = d;
-      } else if (r.found) {
-        label = map_merge_current(a.map, r.slot, leaf, a.cur) ? FIRST_OCUR : SHIFT_DUPL;
-        a.tree[leaf] = d;
-      }
+    unsigned long long prev = ~0ull;
+    if (r.inserted) {
+      label = FIRST_OCUR;
+      prev = r.prev;
+    } else if (r.found) {
+      label = map_merge_current(a.map, r.slot, leaf, a.cur, &prev) ? FIRST_OCUR : SHIFT_DUPL;
     }
+    if (label == FIRST_OCUR && !fixed) flag_shared(a, chunk, prev);
+    if (r.found) a.tree[leaf] = d;
   }
-  a.lab[leaf] = label;
+  if (fixed) {
+    label = FIXED_DUPL;
+    if (a.baseline) a.tree[leaf] = d;
+  }
+  a.leaflab[chunk] = label;
+}
+
+// prior digest of a leaf (the incremental FIXED test); the baseline compares against zero
+__device__ __forceinline__ Digest prior_digest(const LeafArgs& a, uint64_t chunk) {
+  Digest z;
+  z.w[0] = z.w[1] = z.w[2] = z.w[3] = 0u;
+  return a.baseline ? z : a.tree[a.n - 1u + chunk];
 }
 
 __global__ void leaf_generic_kernel(LeafArgs a, uint32_t c_begin, uint32_t c_end) {
@@ -53,8 +68,9 @@ __global__ void leaf_generic_kernel(LeafArgs a, uint32_t c_begin, uint32_t c_end
        c += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t off = c * a.cs;
     const uint64_t nb = (c == a.n - 1u) ? a.len - off : a.cs;
+    const Digest old = prior_digest(a, c);
     const Digest d = hash_bytes(a.kind, a.data + off, nb);
-    leaf_finish(a, (uint32_t)c, d);
+    leaf_finish(a, (uint32_t)c, d, old);
   }
 }
 
@@ -164,7 +180,7 @@ __global__ void __launch_bounds__((TMA_CONSUMER_WARPS + 1) * 32)
         for (uint64_t c = nfull; c < a.n; c++) {
           const uint64_t off = c * a.cs;
           const uint64_t nb = (c == a.n - 1u) ? a.len - off : a.cs;
-          leaf_finish(a, (uint32_t)c, hash_bytes(a.kind, a.data + off, nb));
+          leaf_finish(a, (uint32_t)c, hash_bytes(a.kind, a.data + off, nb), prior_digest(a, c));
         }
       }
     }
@@ -177,6 +193,10 @@ __global__ void __launch_bounds__((TMA_CONSUMER_WARPS + 1) * 32)
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const uint32_t chunk = t * R + row;
     const bool valid = chunk < nfull;
+    // issue the prior-digest load now so its latency hides behind the hashing
+    Digest old;
+    old.w[0] = old.w[1] = old.w[2] = old.w[3] = 0u;
+    if (valid) old = prior_digest(a, chunk);
     Murmur3 mm;
     mm.init();
     uint32_t md[4];
@@ -217,7 +237,7 @@ __global__ void __launch_bounds__((TMA_CONSUMER_WARPS + 1) * 32)
       } else {
         d = mm.finish(a.cs);
       }
-      leaf_finish(a, chunk, d);
+      leaf_finish(a, chunk, d, old);
     }
   }
 }
@@ -256,18 +276,21 @@ static int choose_unit(uint32_t cs, int kind) {
 
 template <int U, int KIND>
 static cudaError_t launch_tma(const CUtensorMap& map, const LeafArgs& a, uint32_t nfull, uint32_t S,
-                              int sm_count, cudaStream_t stream) {
+                              int sm_count, const LeafTuning& tune, cudaStream_t stream) {
   constexpr uint32_t R = 32u * TMA_CONSUMER_WARPS;
   constexpr uint32_t STAGE_BYTES = R * U;
-  uint32_t stages = (96u * 1024u) / STAGE_BYTES;
+  // default: a 64 KB ring per CTA and 3 CTAs per SM (measured best for 128 B chunks: more
+  // resident consumer warps beat a deeper ring)
+  uint32_t stages = tune.stages > 0 ? (uint32_t)tune.stages : (64u * 1024u) / STAGE_BYTES;
   if (stages < 2) stages = 2;
   if (stages > 16) stages = 16;
+  while (stages > 2 && (size_t)stages * STAGE_BYTES > 200u * 1024u) stages--;
   const size_t smem = (size_t)stages * STAGE_BYTES + 2 * stages * sizeof(uint64_t) + 1024;
   auto kern = leaf_tma_kernel<U, KIND>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const uint32_t ntiles = (nfull + R - 1) / R;
-  uint32_t grid = (uint32_t)sm_count * 2u;
+  uint32_t grid = (uint32_t)sm_count * (uint32_t)(tune.ctas_per_sm > 0 ? tune.ctas_per_sm : 3);
   if (grid > ntiles) grid = ntiles;
   if (grid == 0) grid = 1;
   kern<<<grid, (TMA_CONSUMER_WARPS + 1) * 32, smem, stream>>>(map, a, nfull, S, stages);
@@ -275,12 +298,12 @@ static cudaError_t launch_tma(const CUtensorMap& map, const LeafArgs& a, uint32_
 }
 
 // Returns 1 if the staged TMA path was used, 0 for the generic path, negative on error.
-int launch_leaves(const LeafArgs& a, int sm_count, bool allow_tma, cudaStream_t stream) {
+int launch_leaves(const LeafArgs& a, int sm_count, const LeafTuning& tune, cudaStream_t stream) {
   const uint32_t nfull = (uint32_t)(a.len / a.cs);
   const int U = choose_unit(a.cs, a.kind);
   const bool aligned = (reinterpret_cast<uintptr_t>(a.data) & 15u) == 0;
   EncodeTiledFn enc = get_encode_fn();
-  if (allow_tma && U > 0 && aligned && nfull > 0 && enc != nullptr) {
+  if (tune.allow_tma && U > 0 && aligned && nfull > 0 && enc != nullptr) {
     CUtensorMap map;
     const cuuint64_t S = a.cs / (uint32_t)U;
     cuuint64_t dims[3] = {(cuuint64_t)U, S, (cuuint64_t)nfull};
@@ -298,14 +321,14 @@ int launch_leaves(const LeafArgs& a, int sm_count, bool allow_tma, cudaStream_t 
       cudaError_t e;
       const uint32_t s32 = (uint32_t)S;
       if (a.kind == HASH_MD5) {
-        e = U == 128 ? launch_tma<128, HASH_MD5>(map, a, nfull, s32, sm_count, stream)
-                     : launch_tma<64, HASH_MD5>(map, a, nfull, s32, sm_count, stream);
+        e = U == 128 ? launch_tma<128, HASH_MD5>(map, a, nfull, s32, sm_count, tune, stream)
+                     : launch_tma<64, HASH_MD5>(map, a, nfull, s32, sm_count, tune, stream);
       } else {
         switch (U) {
-          case 128: e = launch_tma<128, HASH_MURMUR3>(map, a, nfull, s32, sm_count, stream); break;
-          case 64: e = launch_tma<64, HASH_MURMUR3>(map, a, nfull, s32, sm_count, stream); break;
-          case 32: e = launch_tma<32, HASH_MURMUR3>(map, a, nfull, s32, sm_count, stream); break;
-          default: e = launch_tma<16, HASH_MURMUR3>(map, a, nfull, s32, sm_count, stream); break;
+          case 128: e = launch_tma<128, HASH_MURMUR3>(map, a, nfull, s32, sm_count, tune, stream); break;
+          case 64: e = launch_tma<64, HASH_MURMUR3>(map, a, nfull, s32, sm_count, tune, stream); break;
+          case 32: e = launch_tma<32, HASH_MURMUR3>(map, a, nfull, s32, sm_count, tune, stream); break;
+          default: e = launch_tma<16, HASH_MURMUR3>(map, a, nfull, s32, sm_count, tune, stream); break;
         }
       }
       return e == cudaSuccess ? 1 : -1;

@@ -46,6 +46,7 @@ struct MapRef {
   uint64_t slot;       // valid when found
   bool found;
   bool inserted;
+  unsigned long long prev;   // value before this insert's atomicMin (inserted only)
 };
 
 __device__ __forceinline__ Key128 digest_key(const Digest& d) {
@@ -94,11 +95,11 @@ __device__ __forceinline__ Key128 atomic_cas_key(MapSlot* s, Key128 cmp, Key128 
 __device__ __forceinline__ MapRef map_insert(const MapView& m, const Digest& d, unsigned long long val,
                                              uint32_t cur, DevStatus* st) {
   const Key128 k = digest_key(d);
-  MapRef r{0, false, false};
+  MapRef r{0, false, false, ~0ull};
   if (key_is_empty_pattern(k)) {
     MapSlot* s = &m.slots[m.cap];
     const uint32_t old = atomicCAS(&s->pad, 0u, 1u);
-    atomicMin(&s->val, val);
+    r.prev = atomicMin(&s->val, val);
     r.slot = m.cap;
     r.found = true;
     r.inserted = (old == 0u);
@@ -129,7 +130,7 @@ __device__ __forceinline__ MapRef map_insert(const MapView& m, const Digest& d, 
     if (try_cas) {
       const Key128 old = atomic_cas_key(s, empty, k);
       if (old.lo == MAP_EMPTY && old.hi == MAP_EMPTY) {
-        atomicMin(&s->val, val);
+        r.prev = atomicMin(&s->val, val);
         atomicExch(&s->tree, cur);
         atomicAdd(m.size, 1ull);
         r.slot = i; r.found = true; r.inserted = true;
@@ -150,11 +151,12 @@ __device__ __forceinline__ MapRef map_insert(const MapView& m, const Digest& d, 
 // pending (claimed by a concurrent inserter of this launch).  In that case the lower
 // (priority, node) value wins, matching "first insert in sequential order".
 __device__ __forceinline__ bool map_merge_current(const MapView& m, uint64_t slot, unsigned long long val,
-                                                  uint32_t cur) {
+                                                  uint32_t cur, unsigned long long* prev = nullptr) {
   MapSlot* s = &m.slots[slot];
   const uint32_t t = *reinterpret_cast<volatile uint32_t*>(&s->tree);
   if (t == cur || t == MAP_TREE_PENDING) {
-    atomicMin(&s->val, val);
+    const unsigned long long p = atomicMin(&s->val, val);
+    if (prev) *prev = p;
     return true;
   }
   return false;

@@ -126,7 +126,51 @@ __global__ void __launch_bounds__(R_THREADS) r_expand_first_kernel(RestartArgs a
 // when the chunk count is not a power of two): the reference inserts them with an offset
 // computed in wrapping u32 arithmetic (:844-846, :1016-1018).  Reproduced so later lookups
 // of those leaves behave the same.
-__global__ void r_straddle_kernel(RestartArgs a, uint32_t root, uint32_t region_off, uint32_t lo, uint32_t hi) {
+StraddleQuery straddle_query(uint32_t n) {
+  StraddleQuery q;
+  q.count = 0;
+  if (n < 3 || (n & (n - 1)) == 0) return q;
+  uint32_t x = n - 2, y = n - 1;
+  while (x != y) {
+    if (x > y) x = (x - 1) / 2;
+    else y = (y - 1) / 2;
+  }
+  for (;;) {
+    q.anc[q.count++] = x;
+    if (x == 0 || q.count == 32) break;
+    x = (x - 1) / 2;
+  }
+  return q;
+}
+
+__global__ void r_straddle_find_kernel(RestartArgs a, StraddleQuery q, StraddleInfo* sd) {
+  const uint32_t D = node_level(a.N - 1u);
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < a.F; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t node = rd_u32(a.diff + a.first_off + 4 * i);
+    bool hit = false;
+    for (uint32_t k = 0; k < q.count; k++) hit |= q.anc[k] == node;
+    if (!hit) continue;
+    // leaves of level D-1 under this root
+    const uint32_t k = (D - 1u) - node_level(node);
+    const uint64_t lo_all = ((uint64_t)node << k) + (1ull << k) - 1ull;
+    const uint64_t hi_all = lo_all + (1ull << k) - 1ull;
+    const uint64_t lo = lo_all > (uint64_t)a.n - 1u ? lo_all : (uint64_t)a.n - 1u;
+    const uint64_t lvl_end = (1ull << D) - 2ull;
+    const uint64_t hi = hi_all < lvl_end ? hi_all : lvl_end;
+    if (lo <= hi) {
+      sd->root = node;
+      sd->region_off = a.offs[i];
+      sd->lo = (uint32_t)lo;
+      sd->hi = (uint32_t)hi;
+      __threadfence();
+      sd->present = 1;
+    }
+  }
+}
+
+__global__ void r_straddle_kernel(RestartArgs a, const StraddleInfo* sd) {
+  if (!sd->present) return;
+  const uint32_t root = sd->root, region_off = sd->region_off, lo = sd->lo, hi = sd->hi;
   const uint32_t start = leftmost_leaf(root, a.N);
   for (uint64_t u = lo + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u <= hi; u += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t c = u - (a.n - 1u);
@@ -220,7 +264,7 @@ cudaError_t launch_restart_init(const RestartArgs& a, int sm_count, cudaStream_t
   return e;
 }
 
-cudaError_t launch_restart_diff(const RestartArgs& a, const StraddleInfo& sd, int sm_count, cudaStream_t s) {
+cudaError_t launch_restart_diff(const RestartArgs& a, StraddleInfo* sd, int sm_count, cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(a.dist, 0xff, sizeof(unsigned long long) * (size_t)a.n, s);
   if (e != cudaSuccess) return e;
   if (!a.is_main) {
@@ -233,7 +277,13 @@ cudaError_t launch_restart_diff(const RestartArgs& a, const StraddleInfo& sd, in
   r_scan_kernel<<<1, 1024, 0, s>>>(a, g);
   r_write_kernel<<<g, R_THREADS, 0, s>>>(a, 0);
   r_expand_first_kernel<<<grid_for(a.n, sm_count), R_THREADS, 0, s>>>(a);
-  if (sd.present) r_straddle_kernel<<<grid_for(sd.hi - sd.lo + 1, sm_count), R_THREADS, 0, s>>>(a, sd.root, sd.region_off, sd.lo, sd.hi);
+  const StraddleQuery q = straddle_query(a.n);
+  if (q.count) {
+    e = cudaMemsetAsync(sd, 0, sizeof(StraddleInfo), s);
+    if (e != cudaSuccess) return e;
+    r_straddle_find_kernel<<<grid_for(a.F, sm_count), R_THREADS, 0, s>>>(a, q, sd);
+    r_straddle_kernel<<<(uint32_t)sm_count * 4u, R_THREADS, 0, s>>>(a, sd);
+  }
   // shifted duplicates
   r_count_kernel<<<g, R_THREADS, 0, s>>>(a, 1);
   r_scan_kernel<<<1, 1024, 0, s>>>(a, g);

@@ -32,12 +32,22 @@ struct RestartArgs {
   DevStatus* st;
 };
 
+// The one first-occurrence region (if any) whose root spans two leaf depths (chunk count not a
+// power of two), found on the device after the region offsets are known.
 struct StraddleInfo {
   int present;
   uint32_t root, region_off, lo, hi;
 };
+// roots that can span two depths: the common ancestors of the last inner node (n-2) and the
+// first leaf of level D-1 (n-1), computed on the host from n alone
+struct StraddleQuery {
+  uint32_t count;
+  uint32_t anc[32];
+};
+StraddleQuery straddle_query(uint32_t n);
 
 cudaError_t launch_restart_init(const RestartArgs& a, int sm_count, cudaStream_t s);
-cudaError_t launch_restart_diff(const RestartArgs& a, const StraddleInfo& sd, int sm_count, cudaStream_t s);
+// `sd` is device memory for the straddling-region record of this diff
+cudaError_t launch_restart_diff(const RestartArgs& a, StraddleInfo* sd, int sm_count, cudaStream_t s);
 
 }  // namespace b2d

@@ -74,6 +74,10 @@ class TreeDeduplicator:
     def __exit__(self, *a):
         self.close()
 
+    def set_param(self, name, value):
+        """Tuning knob of the C ABI (b2d_set_param); output bytes never depend on it."""
+        check(lib().b2d_set_param(self._h, name.encode(), int(value)), f"b2d_set_param({name})")
+
     def _sync_stream(self):
         check(lib().b2d_set_stream(self._h, _stream_handle()), "b2d_set_stream")
 
@@ -200,9 +204,9 @@ class TreeDeduplicator:
         check(lib().b2d_debug_tree(self._h, ctypes.c_void_p(out.ctypes.data), nodes), "b2d_debug_tree")
         return out
 
-    def debug_labels(self, nodes):
-        out = np.empty(nodes, np.uint8)
-        check(lib().b2d_debug_labels(self._h, ctypes.c_void_p(out.ctypes.data), nodes), "b2d_debug_labels")
+    def debug_labels(self, leaves):
+        out = np.empty(leaves, np.uint8)
+        check(lib().b2d_debug_labels(self._h, ctypes.c_void_p(out.ctypes.data), leaves), "b2d_debug_labels")
         return out
 
 

@@ -33,16 +33,9 @@ def run_both(bufs, cs, kind=HASH_MURMUR3, baselines=None, restart=True, tma=True
     """checkpoint every buffer on the GPU and in the oracle; assert identical diffs and restarts"""
     import torch
 
-    old = os.environ.get("B2D_DISABLE_TMA")
+    g = TreeDeduplicator(cs, kind)
     if not tma:
-        os.environ["B2D_DISABLE_TMA"] = "1"
-    try:
-        g = TreeDeduplicator(cs, kind)
-    finally:
-        if old is None:
-            os.environ.pop("B2D_DISABLE_TMA", None)
-        else:
-            os.environ["B2D_DISABLE_TMA"] = old
+        g.set_param("leaf_tma", 0)
     o = O.OracleTreeDeduplicator(cs, kind)
     gd, od = [], []
     for i, b in enumerate(bufs):
