@@ -110,6 +110,19 @@ int b2d_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* d
 int b2d_restart_files(b2d_dedup* d, void* d_out, uint64_t len, const char* const* chkpt_filenames,
                       uint32_t num_files, uint32_t chkpt_id, const char* logname);
 
+/* Restart that allocates nothing (no counterpart in the reference).  For callers that cannot
+ * call cudaMalloc: a process restoring a checkpoint after the device ran out of memory, or a
+ * runtime whose device memory is all owned by its own pool and budget.  Same result as
+ * b2d_restart, but the diffs are device-resident (d_diffs[i]: device pointer, sizes[i]: bytes)
+ * and no handle is needed.  The scratch is one fixed __device__ array in the library (about
+ * 7.4 MB on every GPU that loads it, held until exit): at most 2^18 chunks per checkpoint and
+ * checkpoint ids below 4096, else B2D_ERR_UNSUPPORTED.  The first call on a device looks up
+ * that array's address and should come before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller.  Work runs on
+ * `cuda_stream` (NULL = legacy default stream) and the call returns after it completes. */
+int b2d_restart_noalloc(void* d_out, uint64_t len, const void* const* d_diffs, const uint64_t* sizes,
+                        uint32_t num_diffs, uint32_t chkpt_id, void* cuda_stream);
+
 /* num_first_ocur() / num_shift_dupl() -- include/tree_approach.hpp:53-59 */
 int b2d_num_first_ocur(b2d_dedup* d, uint64_t* out);
 int b2d_num_shift_dupl(b2d_dedup* d, uint64_t* out);

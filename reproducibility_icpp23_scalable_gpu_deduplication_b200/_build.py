@@ -9,7 +9,7 @@ import sys
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PKG_DIR, "csrc")
 LIB_PATH = os.path.join(PKG_DIR, "libb200dedup.so")
-SOURCES = ["leaf.cu", "forest.cu", "gather.cu", "restart.cu", "dedup_host.cu", "batch.cu"]
+SOURCES = ["leaf.cu", "forest.cu", "gather.cu", "restart.cu", "dedup_host.cu", "batch.cu", "restart_noalloc.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

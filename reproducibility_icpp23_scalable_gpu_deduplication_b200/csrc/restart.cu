@@ -252,6 +252,33 @@ __global__ void r_fill_older_kernel(RestartArgs a) {
   }
 }
 
+// running shift counts per checkpoint id from a device-resident diff's (ckpt, count) table:
+// the last row for an id wins, then an inclusive scan over ids (:871-885); rows naming an id
+// beyond the diff's own are outside the reference's array and are reported
+__global__ void r_cum_kernel(RestartArgs a) {
+  unsigned long long* cum = const_cast<unsigned long long*>(a.cum);
+  for (uint32_t t = threadIdx.x; t < a.ncum; t += blockDim.x) cum[t] = 0;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (uint32_t i = 0; i < a.P; i++) {
+      const uint32_t ck = rd_u32(a.diff + a.count_off + 8ull * i);
+      const uint32_t cnt = rd_u32(a.diff + a.count_off + 8ull * i + 4);
+      if (ck < a.ncum) cum[ck] = cnt;
+      else set_error(a.st, DERR_RESTART_RANGE, 5);
+    }
+    unsigned long long run = 0;
+    for (uint32_t t = 0; t < a.ncum; t++) {
+      run += cum[t];
+      cum[t] = run;
+    }
+  }
+}
+
+cudaError_t launch_restart_cum(const RestartArgs& a, cudaStream_t s) {
+  r_cum_kernel<<<1, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
 static uint32_t grid_for(uint64_t work, int sm_count) {
   uint64_t b = ceil_div_u64(work ? work : 1, R_THREADS);
   const uint64_t cap = (uint64_t)sm_count * 8u;

@@ -47,6 +47,8 @@ struct StraddleQuery {
 StraddleQuery straddle_query(uint32_t n);
 
 cudaError_t launch_restart_init(const RestartArgs& a, int sm_count, cudaStream_t s);
+// fills a.cum (device) from the repeat table of the device-resident diff a.diff
+cudaError_t launch_restart_cum(const RestartArgs& a, cudaStream_t s);
 // `sd` is device memory for the straddling-region record of this diff
 cudaError_t launch_restart_diff(const RestartArgs& a, StraddleInfo* sd, int sm_count, cudaStream_t s);
 
