@@ -49,6 +49,16 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--leaf-stages", type=int, default=0, help="TMA ring depth (0 = library default)")
     p.add_argument("--leaf-ctas", type=int, default=0, help="hashing CTAs per SM (0 = library default)")
+    p.add_argument("--form", default="plain", choices=["plain", "batched", "served"],
+                   help="plain: one 4 GiB buffer (default); batched: 256 uneven buffers per step through "
+                        "b2d_batch_checkpoint vs one at a time; served: Poisson request loop")
+    p.add_argument("--buffers", type=int, default=256, help="batched form: number of buffers")
+    p.add_argument("--max-buffer", type=int, default=512 << 20, help="batched form: largest buffer size")
+    p.add_argument("--no-autotune", action="store_true")
+    p.add_argument("--clients", type=int, default=64, help="served form: clients")
+    p.add_argument("--requests", type=int, default=1000, help="served form: requests in the stream")
+    p.add_argument("--rate", type=float, default=200.0, help="served form: aggregate arrivals per second")
+    p.add_argument("--hbm-budget", type=float, default=150e9, help="served form: device bytes for client state")
     return p.parse_args()
 
 
@@ -163,6 +173,206 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def batched_series(sizes, dev, seed):
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import synth
+
+    return [synth.varied(n, 128, max_run=256, config_id=4, buf_id=i, device=dev, seed=seed)
+            for i, n in enumerate(sizes)]
+
+
+def run_batched(args, rank, world, dev):
+    """256 buffers of log-uniform sizes: the batch API against the same buffers one at a time."""
+    import torch
+
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import CheckpointBatch, TreeDeduplicator, synth
+
+    sizes = synth.batched_sizes(count=args.buffers, hi=args.max_buffer)
+    total = sum(sizes)
+    chunks = sum((n + 127) // 128 for n in sizes)
+    stream = torch.cuda.current_stream()
+    seed = synth.SEED + rank
+    ckpts = 1 + args.warmup + args.steps
+
+    def series_pass(step_fn, tune_fn=None):
+        ss = batched_series(sizes, dev, seed)
+        hs = [TreeDeduplicator(128) for _ in sizes]
+        times, sums, launches = [], [], 0
+        for c in range(ckpts):
+            bufs = [s.next() for s in ss]
+            torch.cuda.synchronize()
+            if world > 1:
+                import torch.distributed as dist
+
+                dist.barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            nl = step_fn(hs, bufs, c == 0)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if c > args.warmup:
+                times.append(e0.elapsed_time(e1))
+                launches += nl
+            sums.append([h.diff_checksum() for h in hs])
+        for h in hs:
+            h.close()
+        del ss, bufs
+        torch.cuda.empty_cache()
+        return times, sums, launches
+
+    def plain_step(hs, bufs, base):
+        n = 0
+        for h, b in zip(hs, bufs):
+            h.checkpoint_device(b, base)
+            n += h.last_launch_count()
+        return n
+
+    batch = CheckpointBatch()
+    if not args.no_autotune:
+        # tuning series: a baseline, then incremental batches until the tuner settles
+        batch.set_param("autotune", 1)
+        ss = batched_series(sizes, dev, seed + 1000)
+        hs = [TreeDeduplicator(128) for _ in sizes]
+        for c in range(12):
+            batch.checkpoint(hs, [s.next() for s in ss])
+            if batch.get_param("tuned"):
+                break
+        for h in hs:
+            h.close()
+        del ss
+        torch.cuda.empty_cache()
+    tuned = {k: batch.get_param(k) for k in ("leaf_stages", "leaf_ctas_per_sm", "tiles_per_pop", "streams")}
+
+    def batch_step(hs, bufs, base):
+        batch.checkpoint(hs, bufs)
+        return batch.launch_count()
+
+    with ClockSampler(int(dev.index or 0)) as clk:
+        t_plain, s_plain, l_plain = series_pass(plain_step)
+        t_batch, s_batch, l_batch = series_pass(batch_step)
+    same = s_plain == s_batch
+    ms_b, ms_p = statistics.mean(t_batch), statistics.mean(t_plain)
+    tt = torch.tensor([ms_b, ms_p], device=dev)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    ms_b, ms_p = float(tt[0]), float(tt[1])
+    value = world * total / (ms_b * 1e-3) / GB
+    plain = world * total / (ms_p * 1e-3) / GB
+    peak, peak_kind = measured_peak()
+    alg = total + 32 * chunks
+    line = {
+        "metric": "tree-dedup batched ingest GB/s", "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
+        "steps": len(t_batch), "warmup": args.warmup, "ms_per_step": round(ms_b, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded; reference datasets unavailable)",
+        "config": {"workload": f"batched_{len(sizes)}", "buffers": len(sizes), "total_bytes": total,
+                   "min_buffer": min(sizes), "max_buffer": max(sizes), "chunk_size": 128, "hash": "murmur3",
+                   "checkpoints": ckpts, "change": "uniform [0.5%, 20%] in runs of 1-256 chunks + 1% shifted",
+                   "l2": f"inputs {total / 2**30:.1f} GiB > L2, no flush", "tuned": tuned},
+        "plain_same_workload": {"value": round(plain, 2), "unit": "GB/s", "ms_per_step": round(ms_p, 4),
+                                "gpu_launches": l_plain},
+        "speedup_vs_plain": round(value / plain, 3),
+        "parity": ("identical" if same else "MISMATCH") + f": diff checksums of {len(sizes)} buffers x {ckpts} "
+                  "checkpoints, batched vs one at a time",
+        "e2e": None,
+        "gpu_launches": l_batch,
+        "roofline": {"bound": "hbm", "kernel": "whole batch (graph)", "achieved": round(alg / (ms_b * 1e-3) / GB, 1),
+                     "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": round(alg / (ms_b * 1e-3) / GB / peak, 4), "traffic": None,
+                     "algorithmic_bytes": alg},
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    batch.close()
+    if not same:
+        sys.exit(3)
+
+
+def serve_stream(server_kw, sizes, clients, arrivals, dev, warm_rounds=2):
+    """Drive one CheckpointServer through a request stream; returns (requests, wall seconds)."""
+    import torch
+
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import synth
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200.serve import CheckpointServer
+
+    series = [synth.DeviceSeries(n, 128, c, device=dev) for c, n in enumerate(sizes)]
+    srv = CheckpointServer(**server_kw)
+    # every client's baseline and first incremental checkpoints before the stream (resident state)
+    for _ in range(warm_rounds):
+        for c in range(len(sizes)):
+            srv.submit(c, series[c].next())
+        srv.drain()
+    torch.cuda.synchronize()
+    srv.completed.clear()
+    clock = srv.clock
+    t0 = clock()
+    reqs = []
+    for c, a in zip(clients, arrivals):
+        t_arr = t0 + a
+        while clock() < t_arr:
+            srv.step()
+        while srv.busy(c):
+            srv.step()
+        reqs.append(srv.submit(int(c), series[c].next(), arrival=t_arr))
+    srv.drain()
+    wall = max(r.done for r in reqs) - t0
+    batches = srv.batches
+    srv.close()
+    del series
+    torch.cuda.empty_cache()
+    return reqs, wall, batches
+
+
+def run_served(args, rank, world, dev):
+    """64 clients, Poisson arrivals: the continuous-batching loop against the one-at-a-time loop."""
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import synth
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200.serve import percentile
+
+    sizes = synth.served_sizes(count=args.clients, hi=args.max_buffer if args.max_buffer != (512 << 20) else 2 << 30)
+    rng = np.random.default_rng(synth.SEED + rank)
+    n = args.requests
+    clients = rng.integers(0, len(sizes), n)
+    arrivals = synth.poisson_arrivals(args.rate, n, seed=synth.SEED + rank)
+    budget = args.hbm_budget
+    kw = {"hbm_budget": budget, "max_batch": 64, "max_inflight": 2}
+
+    def summarize(reqs, wall, batches):
+        lat = [1e3 * r.latency for r in reqs]
+        byt = sum(r.nbytes for r in reqs)
+        return {"value": round(byt / wall / GB, 2), "unit": "GB/s", "p50_ms": round(percentile(lat, 50), 3),
+                "p99_ms": round(percentile(lat, 99), 3), "max_ms": round(max(lat), 3), "requests": len(reqs),
+                "batches": batches, "failed": sum(1 for r in reqs if r.rc != 0), "wall_s": round(wall, 3)}
+
+    with ClockSampler(int(dev.index or 0)) as clk:
+        served = summarize(*serve_stream(kw, sizes, clients, arrivals, dev))
+        plain = summarize(*serve_stream(dict(kw, plain=True), sizes, clients, arrivals, dev))
+        # capacity: the same clients with every request already waiting (arrival rate unbounded)
+        m = min(n, 4 * len(sizes))
+        burst = np.zeros(m)
+        cap_served = summarize(*serve_stream(kw, sizes, clients[:m], burst, dev))
+        cap_plain = summarize(*serve_stream(dict(kw, plain=True), sizes, clients[:m], burst, dev))
+    line = {
+        "metric": "tree-dedup served GB/s", "value": served["value"], "unit": "GB/s", "n_gpus": world,
+        "steps": n, "warmup": 2, "ms_per_step": served["p50_ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded; reference datasets unavailable)",
+        "config": {"workload": f"served_{len(sizes)}_clients", "clients": len(sizes), "rate_hz": args.rate,
+                   "requests": n, "client_bytes_total": sum(sizes), "min_buffer": min(sizes),
+                   "max_buffer": max(sizes), "chunk_size": 128, "hash": "murmur3", "hbm_budget": budget,
+                   "change": "uniform [0.5%, 20%] in runs of 1-512 chunks + 1% shifted, edited on the device",
+                   "latency": "scheduled arrival -> diff ready on the device (includes the client's edit "
+                              "of its buffer queued at arrival)"},
+        "latency_ms": {"p50": served["p50_ms"], "p99": served["p99_ms"], "max": served["max_ms"]},
+        "served": served, "plain_same_stream": plain,
+        "capacity": {"served": cap_served, "plain": cap_plain,
+                     "speedup_vs_plain": round(cap_served["value"] / cap_plain["value"], 3)},
+        "e2e": None, "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -170,6 +380,23 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.form != "plain":
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dev = torch.device("cuda", local)
+        if world > 1:
+            import datetime
+
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+        if args.form == "batched":
+            run_batched(args, rank, world, dev)
+        else:
+            run_served(args, rank, world, dev)
+        if world > 1:
+            dist.destroy_process_group()
         return
 
     import torch
@@ -201,7 +428,7 @@ def main():
 
     stream = torch.cuda.current_stream()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    leaf_s, diff_bytes, launches = [], [], 0
+    leaf_s, forest_s, gather_s, diff_bytes, launches = [], [], [], [], 0
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -211,6 +438,8 @@ def main():
             diff_bytes.append(dd.checkpoint_device(b))
             ph, path = dd.phase_times()
             leaf_s.append(ph[0])
+            forest_s.append(ph[1])
+            gather_s.append(ph[2])
             launches += dd.last_launch_count()
         stop.record(stream)
         torch.cuda.synchronize()
@@ -271,6 +500,8 @@ def main():
         "roofline": roofline,
         "clocks": clk.summary(),
         "diff_bytes_per_step": int(statistics.mean(diff_bytes)),
+        "phases_ms": {"leaf": round(leaf_ms, 4), "forest": round(1e3 * statistics.mean(forest_s), 4),
+                      "gather": round(1e3 * statistics.mean(gather_s), 4)},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1

@@ -66,8 +66,11 @@ int b2d_set_stream(b2d_dedup* d, void* cuda_stream);
 /* Tuning knobs (no reference counterpart; output bytes never depend on them):
  *   "leaf_tma"          1 = TMA-staged chunk hashing when the chunk size allows (default), 0 = off
  *   "leaf_stages"       TMA ring depth per CTA, 2..16 (0 = default)
- *   "leaf_ctas_per_sm"  resident hashing CTAs per SM, 1..8 (0 = default 2)
- *   "map_max_load_pct"  digest-map load factor that triggers growth, 10..90 (default 75) */
+ *   "leaf_ctas_per_sm"  resident hashing CTAs per SM, 1..8 (0 = default 3)
+ *   "map_max_load_pct"  digest-map load limit, 10..90 (default 75): a checkpoint starts only
+ *                       when the map's entries plus every node of the tree fit under it
+ *   "map_headroom_pct"  size of a baseline's map over that minimum, 100..1000 (default 125);
+ *                       more headroom = fewer growths (allocate + rehash) in a long series */
 int b2d_set_param(b2d_dedup* d, const char* name, int64_t value);
 
 /* checkpoint(header_t&, uint8_t* data_ptr, size_t len, HostMirror& diff_h, bool make_baseline)
@@ -152,6 +155,54 @@ int b2d_debug_labels(b2d_dedup* d, void* dst, uint64_t leaves);
  * reference's hash() (include/hash_functions.hpp:16-20) as a standalone kernel. */
 int b2d_hash_chunks(int hash_kind, const void* d_data, uint64_t len, uint32_t chunk_size, void* d_out,
                     void* cuda_stream);
+
+/* Device bytes a handle holds now (its tree, map, scratch and diff buffers), and the bytes a
+ * handle will hold for checkpoints of a `len`-byte buffer (map_max_load_pct 0 = the default
+ * 75), for admission against a memory budget.  No reference counterpart. */
+int b2d_memory(b2d_dedup* d, uint64_t* bytes);
+/* Digest map statistics: out[0] slots, out[1] entries after the last checkpoint, out[2] times
+ * the map has grown (rehashed into a larger table), out[3] host seconds spent growing it,
+ * out[4] of which allocating the larger tables. */
+int b2d_map_stats(b2d_dedup* d, double out[5]);
+int b2d_estimate_memory(uint64_t len, uint32_t chunk_size, int map_max_load_pct, uint64_t* bytes);
+
+/* ---- Batched checkpoints (no counterpart in the reference, whose checkpoint() takes one
+ * buffer at a time: src/tree_approach.cpp:1705).  One call checkpoints `count` buffers, each
+ * through its own handle (its own tree, map and checkpoint ids), as one CUDA graph: a single
+ * persistent hashing kernel takes tiles of 256 chunks of every buffer from a work queue, then
+ * each handle's tree and diff work runs on parallel graph branches.  Per handle the result is
+ * exactly what b2d_checkpoint_device(handle, d_data[i], lens[i], make_baseline[i], 1, ..)
+ * would give: afterwards b2d_diff_device / b2d_copy_diff / b2d_num_first_ocur read it, and
+ * the handle's checkpoint id has advanced.  Handles must be distinct within a call.
+ * `make_baseline` may be NULL (no forced baselines); `rcs` (nullable) receives each handle's
+ * status.  The graph is rebuilt only when a handle's buffers or sizes change. */
+typedef struct b2d_batch b2d_batch;
+int b2d_batch_create(b2d_batch** out);
+int b2d_batch_destroy(b2d_batch* b);
+int b2d_batch_set_stream(b2d_batch* b, void* cuda_stream);
+/* Tuning: "leaf_stages" (staging ring depth, 0 = 64 KB ring), "leaf_ctas_per_sm" (0 = 3),
+ * "tiles_per_pop" (work-queue granule, tiles of 256 chunks), "streams" (graph branches for the
+ * per-handle work), "autotune" (1: coordinate descent over those knobs, one setting per
+ * incremental batch -- six batches -- measured by device time; "tuned" reads 1 once it has
+ * settled and the knobs then read the chosen values), "graph_cache" (instantiated graphs kept,
+ * one per batch composition, default 16).  Output never depends on them. */
+int b2d_batch_set_param(b2d_batch* b, const char* name, int64_t value);
+int b2d_batch_get_param(b2d_batch* b, const char* name, int64_t* value);
+int b2d_batch_checkpoint(b2d_batch* b, b2d_dedup* const* handles, const void* const* d_data, const uint64_t* lens,
+                         const int* make_baseline, uint32_t count, int* rcs);
+/* The same in two halves, for a caller that keeps several batches in flight (one per batch
+ * object, each on its own stream): launch returns once the batch's graph is launched; query
+ * sets *done to 1 when its device work has completed (0: running, -1: nothing in flight);
+ * wait blocks until then and completes every handle's checkpoint (rcs as above).  A batch
+ * object holds one batch at a time, and a handle may be in one batch in flight at a time. */
+int b2d_batch_launch(b2d_batch* b, b2d_dedup* const* handles, const void* const* d_data, const uint64_t* lens,
+                     const int* make_baseline, uint32_t count, int* rcs);
+int b2d_batch_query(b2d_batch* b, int* done);
+int b2d_batch_wait(b2d_batch* b, int* rcs);
+/* out[0]: device seconds of the last batch (CUDA events around the graph); out[1]: host
+ * seconds from the start of its launch to the end of its completion */
+int b2d_batch_times(b2d_batch* b, double out[2]);
+int b2d_batch_launch_count(b2d_batch* b, uint32_t* out);
 
 const char* b2d_strerror(int status);
 

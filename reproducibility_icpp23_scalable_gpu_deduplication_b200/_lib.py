@@ -48,6 +48,22 @@ SIGNATURES = [
     ("b2d_debug_tree", _int, [_vp, _vp, _u64]),
     ("b2d_debug_labels", _int, [_vp, _vp, _u64]),
     ("b2d_hash_chunks", _int, [_int, _vp, _u64, _u32, _vp, _vp]),
+    ("b2d_memory", _int, [_vp, ctypes.POINTER(_u64)]),
+    ("b2d_map_stats", _int, [_vp, ctypes.POINTER(ctypes.c_double)]),
+    ("b2d_estimate_memory", _int, [_u64, _u32, _int, ctypes.POINTER(_u64)]),
+    ("b2d_batch_create", _int, [ctypes.POINTER(_vp)]),
+    ("b2d_batch_destroy", _int, [_vp]),
+    ("b2d_batch_set_stream", _int, [_vp, _vp]),
+    ("b2d_batch_set_param", _int, [_vp, _cc, ctypes.c_int64]),
+    ("b2d_batch_get_param", _int, [_vp, _cc, ctypes.POINTER(ctypes.c_int64)]),
+    ("b2d_batch_checkpoint", _int, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.POINTER(_u64),
+                                    ctypes.POINTER(_int), _u32, ctypes.POINTER(_int)]),
+    ("b2d_batch_launch", _int, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.POINTER(_u64),
+                                ctypes.POINTER(_int), _u32, ctypes.POINTER(_int)]),
+    ("b2d_batch_query", _int, [_vp, ctypes.POINTER(_int)]),
+    ("b2d_batch_wait", _int, [_vp, ctypes.POINTER(_int)]),
+    ("b2d_batch_times", _int, [_vp, ctypes.POINTER(ctypes.c_double)]),
+    ("b2d_batch_launch_count", _int, [_vp, ctypes.POINTER(_u32)]),
     ("b2d_strerror", ctypes.c_char_p, [_int]),
 ]
 

@@ -15,6 +15,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <algorithm>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -123,6 +125,7 @@ struct DevState {
   unsigned int pad;
   DevMeta meta;
   StraddleInfo straddle;
+  RoundState round;
 };
 
 }  // namespace b2d
@@ -148,8 +151,10 @@ struct b2d_dedup {
   bool have_tree = false;
   LeafTuning tune;
   double map_max_load = 0.75;
+  double map_headroom = 1.25;     // baseline table size over its minimum (entries + N at max load)
 
   cudaStream_t own_stream = nullptr;
+  cudaStream_t cap_stream = nullptr;   // graph capture only
   cudaStream_t stream = nullptr;
   int device = 0;
   int sm_count = 148;
@@ -157,8 +162,11 @@ struct b2d_dedup {
 
   DevBuf<Digest> tree;
   DevBuf<uint8_t> lab, leaflab, push, dupflag;
-  DevBuf<MapSlot> map_slots;
-  uint64_t map_cap = 0;           // power of two; slots hold map_cap + 1 entries
+  MapSlot* map_slots = nullptr;   // map_cap + 1 slots, from the library's map pool
+  uint64_t map_cap = 0;
+  double map_grow_s = 0;          // host seconds spent growing the map (all checkpoints)
+  double map_alloc_s = 0;         // of which in allocating the larger table
+  uint32_t map_grows = 0;
   uint64_t map_size_host = 0;     // occupied slots after the last checkpoint
   DevBuf<unsigned long long> map_size;
   DevBuf<uint32_t> tmp_first, tmp_shift, levels;
@@ -166,6 +174,11 @@ struct b2d_dedup {
   DevBuf<uint8_t> diff;
   DevBuf<DevState> state;
   PinnedBuf<DevState> state_h;
+  PinnedBuf<RoundState> round_h;   // this checkpoint's RoundState, uploaded by the graph
+  const void* data = nullptr;      // buffer of the current checkpoint
+  uint32_t bcap = 0;               // source-checkpoint bucket capacity of the scratch
+  cudaGraphExec_t graph_exec = nullptr;
+  std::vector<uint64_t> graph_key;
   PinnedBuf<uint8_t> diff_h;
   uint64_t diff_len = 0;
   uint32_t diff_delta = 0;
@@ -179,66 +192,168 @@ struct b2d_dedup {
   DevBuf<uint8_t> r_diff;
   PinnedBuf<uint8_t> r_stage;
 
-  ~b2d_dedup() {
-    for (auto& e : ev)
-      if (e) cudaEventDestroy(e);
-    if (own_stream) cudaStreamDestroy(own_stream);
-  }
+  ~b2d_dedup();
 };
 
 namespace {
 
+// Device memory pool for digest maps (one per device).  Maps are the largest allocations and
+// the only ones that grow during a series: the pool keeps freed maps' memory for the next
+// growth instead of returning it to the driver, and its frees are stream-ordered, so growing
+// a map neither waits for the whole device nor maps fresh pages each time.  Unused memory
+// goes back to the driver when a handle is destroyed.
+cudaMemPool_t map_pool(int device) {
+  static std::mutex mu;
+  static std::vector<cudaMemPool_t> pools;
+  std::lock_guard<std::mutex> lock(mu);
+  if ((int)pools.size() <= device) pools.resize(device + 1, nullptr);
+  if (!pools[device]) {
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t p = nullptr;
+    if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[device] = p;
+  }
+  return pools[device];
+}
+
+}  // namespace
+
+b2d_dedup::~b2d_dedup() {
+  {
+    if (map_slots) {
+      cudaStream_t s = own_stream ? own_stream : stream;
+      cudaFreeAsync(map_slots, s);
+      cudaStreamSynchronize(s);
+      if (cudaMemPool_t p = map_pool(device)) cudaMemPoolTrimTo(p, 0);
+    }
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    if (own_stream) cudaStreamDestroy(own_stream);
+    if (cap_stream) cudaStreamDestroy(cap_stream);
+  }
+}
+
+namespace {
+
+// events that were never recorded (a failed launch) read as 0 and leave no error behind for
+// the next call's launch checks
+float elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+    (void)cudaGetLastError();
+    ms = 0.f;
+  }
+  return ms;
+}
+
+double secs(std::chrono::high_resolution_clock::time_point a, std::chrono::high_resolution_clock::time_point b) {
+  return std::chrono::duration<double>(b - a).count();
+}
+
+template <class T>
+uint64_t buf_bytes(const DevBuf<T>& b) {
+  return b.p ? (uint64_t)b.n * sizeof(T) : 0;
+}
+
+// device bytes a handle holds (everything it allocated with cudaMalloc)
+uint64_t handle_bytes(const b2d_dedup* d) {
+  return buf_bytes(d->tree) + buf_bytes(d->lab) + buf_bytes(d->leaflab) + buf_bytes(d->push) +
+         buf_bytes(d->dupflag) + (d->map_slots ? (d->map_cap + 1) * sizeof(MapSlot) : 0) +
+         buf_bytes(d->map_size) + buf_bytes(d->tmp_first) +
+         buf_bytes(d->tmp_shift) + buf_bytes(d->levels) + buf_bytes(d->first_list) + buf_bytes(d->shift_list) +
+         buf_bytes(d->region_off) + buf_bytes(d->sprev) + buf_bytes(d->skey) + buf_bytes(d->hist) +
+         buf_bytes(d->bucket_start) + buf_bytes(d->partial) + buf_bytes(d->partial2) + buf_bytes(d->diff) +
+         buf_bytes(d->state) + buf_bytes(d->r_node_list) + buf_bytes(d->r_rep) + buf_bytes(d->r_dist) +
+         buf_bytes(d->r_offs) + buf_bytes(d->r_partial) + buf_bytes(d->r_cum) + buf_bytes(d->r_total) +
+         buf_bytes(d->r_diff);
+}
+
 int map_view(b2d_dedup* d, MapView& m) {
-  m.slots = d->map_slots.p;
+  m.slots = d->map_slots;
   m.cap = d->map_cap;
-  m.mask = d->map_cap - 1;
   m.size = d->map_size.p;
+  m.pad = 0;
   return B2D_OK;
 }
 
+// a fresh map of `cap` slots (+ the special slot) on the handle's stream
+int map_alloc(b2d_dedup* d, uint64_t cap, MapSlot** out) {
+  cudaMemPool_t pool = map_pool(d->device);
+  if (!pool) return B2D_ERR_CUDA;
+  B2D_CU(cudaMallocFromPoolAsync(reinterpret_cast<void**>(out), sizeof(MapSlot) * (cap + 1), pool, d->stream));
+  B2D_CU(cudaMemsetAsync(*out, 0xff, sizeof(MapSlot) * (cap + 1), d->stream));
+  map_special_init_kernel<<<1, 1, 0, d->stream>>>(*out + cap);
+  return cuda_status(cudaGetLastError());
+}
+
 int map_reset(b2d_dedup* d, uint64_t cap) {
-  B2D_CU(d->map_slots.reserve(cap + 1));
-  d->map_cap = cap;
-  B2D_CU(cudaMemsetAsync(d->map_slots.p, 0xff, sizeof(MapSlot) * (cap + 1), d->stream));
-  map_special_init_kernel<<<1, 1, 0, d->stream>>>(d->map_slots.p + cap);
+  if (!d->map_slots || d->map_cap != cap) {
+    MapSlot* fresh = nullptr;
+    int rc = map_alloc(d, cap, &fresh);
+    if (rc) return rc;
+    if (d->map_slots) cudaFreeAsync(d->map_slots, d->stream);
+    d->map_slots = fresh;
+    d->map_cap = cap;
+  } else {
+    B2D_CU(cudaMemsetAsync(d->map_slots, 0xff, sizeof(MapSlot) * (cap + 1), d->stream));
+    map_special_init_kernel<<<1, 1, 0, d->stream>>>(d->map_slots + cap);
+  }
   B2D_CU(d->map_size.reserve(1));
   B2D_CU(cudaMemsetAsync(d->map_size.p, 0, sizeof(unsigned long long), d->stream));
   d->map_size_host = 0;
   return B2D_OK;
 }
 
-uint64_t pow2_at_least(uint64_t x) {
-  uint64_t c = 1024;
-  while (c < x) c <<= 1;
-  return c;
+// Capacity policy.  The reference rehashes when capacity < size + num_nodes
+// (src/tree_approach.cpp:1622-1623): room for every node of the next checkpoint to be new.
+// Here that room must fit under the load limit map_max_load (default 0.75), so no checkpoint
+// can push the table past it: a new table holds its entries plus N at that load, with
+// map_headroom (default 25%) extra at a baseline and 50% when it grows.  Growing allocates and
+// rehashes, so a series whose digests keep changing grows less often with more headroom.
+// Capacities are multiples of 1024, not powers of two.
+uint64_t map_capacity(uint64_t need, double max_load, double headroom) {
+  const uint64_t c = (uint64_t)((double)need * headroom / max_load) + 1;
+  return (c + 1023) / 1024 * 1024;
 }
 
-// capacity policy: the reference rehashes when capacity < size + num_nodes (:1622-1623); here
-// the table keeps load <= map_max_load (default 0.75) with that reservation and grows to half
-// of it
 int map_ensure(b2d_dedup* d) {
   const uint64_t need = d->map_size_host + d->N;
-  if (d->map_slots.p && (double)need <= d->map_max_load * (double)d->map_cap) return B2D_OK;
-  const uint64_t cap = pow2_at_least((uint64_t)((double)need / (0.5 * d->map_max_load)) + 1);
-  if (!d->map_slots.p || d->map_size_host == 0) return map_reset(d, cap);
-  DevBuf<MapSlot> fresh;
-  B2D_CU(fresh.reserve(cap + 1));
-  B2D_CU(cudaMemsetAsync(fresh.p, 0xff, sizeof(MapSlot) * (cap + 1), d->stream));
-  map_special_init_kernel<<<1, 1, 0, d->stream>>>(fresh.p + cap);
+  if (d->map_slots && (double)need <= d->map_max_load * (double)d->map_cap) return B2D_OK;
+  const uint64_t cap = map_capacity(need, d->map_max_load, 1.5);
+  if (!d->map_slots || d->map_size_host == 0) return map_reset(d, cap);
+  const auto t0 = std::chrono::high_resolution_clock::now();
+  MapSlot* fresh = nullptr;
+  int rc = map_alloc(d, cap, &fresh);
+  if (rc) return rc;
+  d->map_alloc_s += secs(t0, std::chrono::high_resolution_clock::now());
   DevBuf<unsigned long long> cnt;
   B2D_CU(cnt.reserve(1));
   B2D_CU(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long), d->stream));
   MapView from, to;
   map_view(d, from);
-  to.slots = fresh.p; to.cap = cap; to.mask = cap - 1; to.size = cnt.p;
+  to.slots = fresh; to.cap = cap; to.size = cnt.p; to.pad = 0;
   map_rehash_kernel<<<(unsigned)d->sm_count * 8u, 256, 0, d->stream>>>(from, to, &d->state.p->status);
-  B2D_CU(cudaGetLastError());
+  const cudaError_t ke = cudaGetLastError();
+  if (ke != cudaSuccess) {
+    cudaFreeAsync(fresh, d->stream);
+    return cuda_status(ke);
+  }
+  cudaFreeAsync(d->map_slots, d->stream);
   B2D_CU(cudaStreamSynchronize(d->stream));
-  std::swap(d->map_slots.p, fresh.p);
-  std::swap(d->map_slots.n, fresh.n);
+  d->map_slots = fresh;
   std::swap(d->map_size.p, cnt.p);
   std::swap(d->map_size.n, cnt.n);
   d->map_cap = cap;
+  d->map_grow_s += secs(t0, std::chrono::high_resolution_clock::now());
+  d->map_grows += 1;
   return B2D_OK;
 }
 
@@ -252,13 +367,23 @@ int status_code(const DevStatus& st) {
   }
 }
 
-double secs(std::chrono::high_resolution_clock::time_point a, std::chrono::high_resolution_clock::time_point b) {
-  return std::chrono::duration<double>(b - a).count();
+
+LeafArgs leaf_args(const b2d_dedup* d, const RoundState* rs_dev) {
+  MapView m;
+  m.slots = d->map_slots;
+  m.cap = d->map_cap;
+  m.size = d->map_size.p;
+  m.pad = 0;
+  return LeafArgs{static_cast<const uint8_t*>(d->data), d->data_len, d->chunk_size, d->n, d->kind, 0, 0,
+                  d->tree.p, d->leaflab.p, d->dupflag.p, m, &d->state.p->status, rs_dev};
 }
 
-int do_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, bool make_baseline, bool advance) {
-  using clk = std::chrono::high_resolution_clock;
-  const auto t0 = clk::now();
+// ------------------------------------------------------------------------------------------
+// One checkpoint = prepare (host: sizes, allocations, map reset/growth, per-checkpoint values)
+// + enqueue (device work, identical launch parameters for every checkpoint of a buffer, so it
+// is captured once into a CUDA graph and replayed) + finish (host: status and sizes).
+// ------------------------------------------------------------------------------------------
+int prepare_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, bool make_baseline) {
   if (!d_data || len == 0) return B2D_ERR_ARG;
   uint64_t nc = (len + d->chunk_size - 1) / d->chunk_size;
   if (nc > 0x7fffffffull) return B2D_ERR_ARG;
@@ -266,6 +391,7 @@ int do_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, bool make_base
   if (!baseline && (!d->have_tree || nc != d->n)) return B2D_ERR_LEN_CHANGED;
   if (d->current_id + 1u > MAX_BUCKETS) return B2D_ERR_UNSUPPORTED;   // source-checkpoint buckets
   d->diff_valid = false;
+  d->data = d_data;
   d->data_len = len;
   d->n = (uint32_t)nc;
   d->N = 2u * d->n - 1u;
@@ -285,7 +411,7 @@ int do_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, bool make_base
     B2D_CU(cudaMemsetAsync(d->push.p, 0, d->push.n, d->stream));
   }
   if (baseline) {
-    int rc = map_reset(d, pow2_at_least((uint64_t)((double)d->N / (0.5 * d->map_max_load)) + 1));
+    int rc = map_reset(d, map_capacity(2ull * d->N, d->map_max_load, d->map_headroom));
     if (rc) return rc;
     d->have_tree = true;
     d->baseline_id = d->current_id;
@@ -293,7 +419,11 @@ int do_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, bool make_base
     int rc = map_ensure(d);
     if (rc) return rc;
   }
-  const uint32_t B = d->current_id + 1u;
+  // bucket capacity grows in powers of two so a buffer's graph survives many checkpoints
+  uint32_t bcap = d->bcap ? d->bcap : 64u;
+  while (bcap < d->current_id + 1u) bcap <<= 1;
+  if (bcap > MAX_BUCKETS) bcap = MAX_BUCKETS;
+  d->bcap = bcap;
   B2D_CU(d->first_list.reserve(d->n));
   B2D_CU(d->shift_list.reserve(d->n));
   B2D_CU(d->tmp_first.reserve(d->n));
@@ -302,64 +432,91 @@ int do_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, bool make_base
   B2D_CU(d->region_off.reserve(d->n));
   B2D_CU(d->sprev.reserve(d->n));
   B2D_CU(d->skey.reserve(d->n));
-  B2D_CU(d->hist.reserve(B < 64 ? 64 : B));
-  B2D_CU(d->bucket_start.reserve(B < 64 ? 64 : B));
-  B2D_CU(d->partial.reserve((size_t)1184 * (B < 64 ? 64 : B)));
+  B2D_CU(d->hist.reserve(bcap));
+  B2D_CU(d->bucket_start.reserve(bcap));
+  B2D_CU(d->partial.reserve((size_t)1184 * bcap));
   B2D_CU(d->partial2.reserve(2 * SCAN_GRID));
   B2D_CU(d->diff.reserve(64 + 16ull * d->n + (uint64_t)d->n * d->chunk_size));
   B2D_CU(d->state.reserve(1));
   B2D_CU(d->state_h.reserve(1));
-  B2D_CU(cudaMemsetAsync(d->state.p, 0, sizeof(DevState), d->stream));
+  B2D_CU(d->round_h.reserve(1));
+  RoundState* r = d->round_h.p;
+  r->cur = d->current_id;
+  r->baseline_id = d->baseline_id;
+  r->baseline = baseline ? 1u : 0u;
+  r->buckets = d->current_id + 1u;
+  map_view(d, r->map);
+  return B2D_OK;
+}
+
+// everything a checkpoint's launches depend on; a different key means a different graph (the
+// digest map is not in it: kernels read its location from the RoundState)
+void graph_key(const b2d_dedup* d, const RoundState* rs_dev, std::vector<uint64_t>& k) {
+  k.assign({(uint64_t)d->data, d->data_len, d->chunk_size, (uint64_t)d->kind, (uint64_t)d->tree.p,
+            (uint64_t)d->lab.p, (uint64_t)d->leaflab.p, (uint64_t)d->push.p, (uint64_t)d->dupflag.p,
+            (uint64_t)d->first_list.p,
+            (uint64_t)d->shift_list.p, (uint64_t)d->tmp_first.p, (uint64_t)d->tmp_shift.p, (uint64_t)d->levels.p,
+            (uint64_t)d->region_off.p, (uint64_t)d->sprev.p, (uint64_t)d->skey.p, (uint64_t)d->hist.p,
+            (uint64_t)d->bucket_start.p, (uint64_t)d->partial.p, (uint64_t)d->partial2.p, (uint64_t)d->diff.p,
+            (uint64_t)d->state.p, (uint64_t)d->state_h.p, (uint64_t)d->round_h.p, (uint64_t)rs_dev, d->bcap,
+            (uint64_t)d->tune.allow_tma, (uint64_t)d->tune.stages, (uint64_t)d->tune.ctas_per_sm,
+            (uint64_t)d->sm_count});
+}
+
+// Device work of one checkpoint on `s`.  `rs_dev` is where the kernels read this checkpoint's
+// RoundState; with `upload` the host copy (pinned) is copied there first.  `managed`: a batch
+// clears the DevState, writes the RoundState and reads the DevState back for all its handles
+// at once (and may have hashed the leaves already: `skip_leaves`).
+int enqueue_checkpoint(b2d_dedup* d, cudaStream_t s, RoundState* rs_dev, bool upload, bool timing, bool skip_leaves,
+                       bool managed = false) {
   MapView m;
   map_view(d, m);
   DevState* ds = d->state.p;
-  const auto t1 = clk::now();
-  d->timers[0] = secs(t0, t1);
-  d->launches = 0;
-
-  B2D_CU(cudaEventRecord(d->ev[0], d->stream));
+  if (!managed) {
+    B2D_CU(cudaMemsetAsync(ds, 0, sizeof(DevState), s));
+    if (upload) B2D_CU(cudaMemcpyAsync(rs_dev, d->round_h.p, sizeof(RoundState), cudaMemcpyHostToDevice, s));
+  }
+  // inside a capture a plain event record only joins streams; External makes it a graph node
+  // that records the event on every replay
+  if (timing) B2D_CU(cudaEventRecordWithFlags(d->ev[0], s, cudaEventRecordExternal));
   // dedup_data_baseline (:13-259) / dedup_data (:261-509)
-  LeafArgs la{static_cast<const uint8_t*>(d_data), len, d->chunk_size, d->n, d->kind, baseline ? 1 : 0,
-              d->current_id, d->tree.p, d->leaflab.p, d->dupflag.p, m, &ds->status};
-  const int leaf_path = launch_leaves(la, d->sm_count, d->tune, d->stream);
-  if (leaf_path < 0) return B2D_ERR_CUDA;
-  d->leaf_tma = leaf_path == 1;
-  d->launches += 1;
-  B2D_CU(cudaEventRecord(d->ev[3], d->stream));
+  if (!skip_leaves) {
+    const LeafArgs la = leaf_args(d, rs_dev);
+    const int leaf_path = launch_leaves(la, d->sm_count, d->tune, s);
+    if (leaf_path < 0) return B2D_ERR_CUDA;
+    d->leaf_tma = leaf_path == 1;
+  }
+  if (timing) B2D_CU(cudaEventRecordWithFlags(d->ev[3], s, cudaEventRecordExternal));
   ForestArgs fa{d->tree.p, d->lab.p, d->leaflab.p, d->push.p, m, &ds->status, &ds->zero_exists, d->dupflag.p,
-                d->n, d->N, d->D, d->current_id, d->kind, baseline ? 1 : 0};
-  B2D_CU(launch_forest(fa, 1, d->stream));
-  if (baseline) {
-    B2D_CU(launch_zero_exists(m, &ds->zero_exists, d->stream));
-    d->launches += 1;
-  }
-  B2D_CU(launch_forest(fa, 2, d->stream));
-  if (baseline) {
-    B2D_CU(launch_baseline_inserts(fa, d->sm_count, d->stream));
-    d->launches += 1;
-  }
-  d->launches += 2 * forest_launch_count(d->D);
-  B2D_CU(cudaEventRecord(d->ev[1], d->stream));
+                d->n, d->N, d->D, 0, d->kind, 0, rs_dev};
+  B2D_CU(launch_forest(fa, 1, s));
+  B2D_CU(launch_zero_exists(&ds->zero_exists, rs_dev, s));
+  B2D_CU(launch_forest(fa, 2, s));
+  if (timing) B2D_CU(cudaEventRecordWithFlags(d->ev[1], s, cudaEventRecordExternal));
   // collect_diff (:511-710)
-  DiffArgs ga{static_cast<const uint8_t*>(d_data), len, d->chunk_size, d->n, d->N, d->D, d->current_id,
-              d->baseline_id, d->tree.p, d->push.p, m, &ds->status, &ds->meta, d->first_list.p,
-              d->shift_list.p, d->tmp_first.p, d->tmp_shift.p, d->levels.p, d->region_off.p, d->sprev.p, d->skey.p, d->hist.p, d->bucket_start.p,
-              d->partial.p, d->partial2.p, d->diff.p};
-  B2D_CU(launch_collect_diff(ga, d->sm_count, d->stream));
-  d->launches += 14;
-  B2D_CU(cudaEventRecord(d->ev[2], d->stream));
-  B2D_CU(cudaMemcpyAsync(d->state_h.p, d->state.p, sizeof(DevState), cudaMemcpyDeviceToHost, d->stream));
-  B2D_CU(cudaStreamSynchronize(d->stream));
+  DiffArgs ga{static_cast<const uint8_t*>(d->data), d->data_len, d->chunk_size, d->n, d->N, d->D, 0, 0,
+              d->tree.p, d->push.p, m, &ds->status, &ds->meta, d->first_list.p, d->shift_list.p, d->tmp_first.p,
+              d->tmp_shift.p, d->levels.p, d->region_off.p, d->sprev.p, d->skey.p, d->hist.p, d->bucket_start.p,
+              d->partial.p, d->partial2.p, d->diff.p, rs_dev};
+  B2D_CU(launch_collect_diff(ga, d->bcap, d->sm_count, s));
+  if (timing) B2D_CU(cudaEventRecordWithFlags(d->ev[2], s, cudaEventRecordExternal));
+  if (!managed) B2D_CU(cudaMemcpyAsync(d->state_h.p, d->state.p, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+  d->launches = (skip_leaves ? 0 : 1) + forest_launch_count(d->D, 1) + forest_launch_count(d->D, 2) + 1 + 14;
+  return B2D_OK;
+}
+
+int finish_checkpoint(b2d_dedup* d, bool advance, bool timing) {
   const DevState& st = *d->state_h.p;
-  float ms_dedup = 0, ms_gather = 0, ms_leaf = 0;
-  cudaEventElapsedTime(&ms_dedup, d->ev[0], d->ev[1]);
-  cudaEventElapsedTime(&ms_gather, d->ev[1], d->ev[2]);
-  cudaEventElapsedTime(&ms_leaf, d->ev[0], d->ev[3]);
-  d->phase[0] = ms_leaf * 1e-3;
-  d->phase[1] = (ms_dedup - ms_leaf) * 1e-3;
-  d->phase[2] = ms_gather * 1e-3;
-  d->timers[1] = ms_dedup * 1e-3;
-  d->timers[2] = ms_gather * 1e-3;
+  if (timing) {
+    const float ms_dedup = elapsed_ms(d->ev[0], d->ev[1]);
+    const float ms_gather = elapsed_ms(d->ev[1], d->ev[2]);
+    const float ms_leaf = elapsed_ms(d->ev[0], d->ev[3]);
+    d->phase[0] = ms_leaf * 1e-3;
+    d->phase[1] = (ms_dedup - ms_leaf) * 1e-3;
+    d->phase[2] = ms_gather * 1e-3;
+    d->timers[1] = ms_dedup * 1e-3;
+    d->timers[2] = ms_gather * 1e-3;
+  }
   d->timers[3] = 0;
   int rc = status_code(st.status);
   d->map_size_host = st.meta.map_size;
@@ -380,6 +537,42 @@ int do_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, bool make_base
   d->diff_valid = true;
   if (advance) d->current_id += 1;
   return B2D_OK;
+}
+
+int do_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, bool make_baseline, bool advance) {
+  using clk = std::chrono::high_resolution_clock;
+  const auto t0 = clk::now();
+  int rc = prepare_checkpoint(d, d_data, len, make_baseline);
+  if (rc) return rc;
+  RoundState* rs_dev = &d->state.p->round;
+  // the round state lives in DevState, which the enqueue clears first: upload after the clear
+  std::vector<uint64_t> key;
+  graph_key(d, rs_dev, key);
+  if (!d->graph_exec || key != d->graph_key) {
+    if (d->graph_exec) {
+      cudaGraphExecDestroy(d->graph_exec);
+      d->graph_exec = nullptr;
+    }
+    // captured on a private stream (the caller's may be the legacy default stream, which
+    // cannot be captured) and launched on the caller's
+    cudaGraph_t g = nullptr;
+    B2D_CU(cudaStreamBeginCapture(d->cap_stream, cudaStreamCaptureModeThreadLocal));
+    rc = enqueue_checkpoint(d, d->cap_stream, rs_dev, true, true, false);
+    const cudaError_t ce = cudaStreamEndCapture(d->cap_stream, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    B2D_CU(ce);
+    const cudaError_t ie = cudaGraphInstantiate(&d->graph_exec, g, 0);
+    cudaGraphDestroy(g);
+    B2D_CU(ie);
+    d->graph_key = key;
+  }
+  d->timers[0] = secs(t0, clk::now());
+  B2D_CU(cudaGraphLaunch(d->graph_exec, d->stream));
+  B2D_CU(cudaStreamSynchronize(d->stream));
+  return finish_checkpoint(d, advance, true);
 }
 
 int copy_diff(b2d_dedup* d, void* dst, uint64_t cap) {
@@ -625,6 +818,441 @@ int read_file(const std::string& path, std::vector<uint8_t>& out) {
   return got == (size_t)sz ? B2D_OK : B2D_ERR_IO;
 }
 
+// ------------------------------------------------------------------------------------------
+// Batched checkpoints: one checkpoint of each of many handles (buffers of any sizes, each
+// with its own device-resident tree and map) as ONE CUDA graph:
+//   upload (one copy: leaf work items, round states, state pointers)
+//   -> batch_init_kernel (clears every handle's DevState, writes its RoundState)
+//   -> one persistent leaf kernel per (unit, hash kind) group, fed by a tile work queue
+//   -> per handle: forest + diff assembly, spread over parallel graph branches
+//   -> batch_collect_kernel + one read-back of every handle's DevState.
+// Each handle's output is what its own b2d_checkpoint_device would produce.
+// ------------------------------------------------------------------------------------------
+static_assert(sizeof(DevState) % 4 == 0, "DevState is cleared word by word");
+
+__global__ void batch_init_kernel(DevState* const* states, const RoundState* rounds, uint32_t count,
+                                  unsigned int* queues, uint32_t ngroups, DevStatus* bst) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  for (uint32_t i = tid; i < count; i += gridDim.x * blockDim.x) {
+    uint32_t* w = reinterpret_cast<uint32_t*>(states[i]);
+    for (uint32_t j = 0; j < sizeof(DevState) / 4; j++) w[j] = 0u;
+    states[i]->round = rounds[i];
+  }
+  if (tid < ngroups) queues[tid] = 0u;
+  if (tid == 0) {
+    bst->error = 0u;
+    bst->detail = 0u;
+  }
+}
+
+__global__ void batch_collect_kernel(DevState* const* states, uint32_t count, DevState* out) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  for (uint32_t i = tid; i < count; i += gridDim.x * blockDim.x) out[i] = *states[i];
+}
+
+struct BatchCand {
+  int stages, ctas, tiles_per_pop, streams;
+};
+
+// Online coordinate-descent tuner.  Each incremental batch (same bytes every time) measures one
+// setting by its graph's device time: first the current setting, then, one knob at a time,
+// each other value of that knob, keeping a value whenever it is faster.  Knobs: graph branches
+// for the per-buffer work, tiles (of 256 chunks) per work-queue pop, and staging (ring depth x
+// CTAs per SM) of the hashing kernel.  1 + 2 + 2 + 1 = 6 measured batches.
+struct BatchTuner {
+  static constexpr int KNOBS = 3;
+  BatchCand base{0, 3, 4, 8};
+  double base_score = 0;
+  bool have_base = false, done = false;
+  int knob = 0;
+  size_t idx = 0;
+  BatchCand pending{0, 3, 4, 8};
+
+  static size_t nvalues(int k) { return k == 2 ? 2 : 3; }
+  static BatchCand with_value(BatchCand c, int k, size_t i) {
+    static const int streams[3] = {8, 32, 2}, tpp[3] = {4, 1, 16};
+    static const int stages[2] = {0, 3}, ctas[2] = {3, 2};
+    if (k == 0) c.streams = streams[i];
+    else if (k == 1) c.tiles_per_pop = tpp[i];
+    else {
+      c.stages = stages[i];
+      c.ctas = ctas[i];
+    }
+    return c;
+  }
+  static bool same(const BatchCand& a, const BatchCand& b) {
+    return a.stages == b.stages && a.ctas == b.ctas && a.tiles_per_pop == b.tiles_per_pop && a.streams == b.streams;
+  }
+  void reset(const BatchCand& start) {
+    *this = BatchTuner();
+    base = pending = start;
+  }
+  BatchCand next() {
+    if (!have_base || done) return pending = base;
+    while (knob < KNOBS) {
+      while (idx < nvalues(knob)) {
+        const BatchCand c = with_value(base, knob, idx);
+        if (!same(c, base)) return pending = c;
+        idx++;
+      }
+      knob++;
+      idx = 0;
+    }
+    done = true;
+    return pending = base;
+  }
+  void report(double score) {
+    if (done) return;
+    if (!have_base) {
+      have_base = true;
+      base_score = score;
+      return;
+    }
+    if (score > base_score) {
+      base = pending;
+      base_score = score;
+    }
+    idx++;
+    next();   // settles `done` once the last knob is exhausted
+  }
+};
+
+struct BatchLayout {
+  size_t items = 0, rounds = 0, states = 0, queues = 0, bstatus = 0, total = 0;
+};
+
+}  // namespace
+
+struct b2d_batch {
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t own_stream = nullptr, stream = nullptr, cap = nullptr;
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> side_ev;
+  cudaEvent_t fork_ev = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  DevBuf<uint8_t> blob;
+  PinnedBuf<uint8_t> blob_h;
+  DevBuf<DevState> coll;
+  PinnedBuf<DevState> coll_h;
+  BatchLayout lay;
+  // instantiated graphs by batch composition, least recently used evicted beyond graph_cap
+  struct GraphEntry {
+    std::vector<uint64_t> key;
+    uint64_t hash = 0;
+    cudaGraphExec_t exec = nullptr;
+    uint32_t launches = 0;
+    uint64_t last_use = 0;
+  };
+  std::vector<GraphEntry> graphs;
+  size_t graph_cap = 16;
+  uint64_t use_clock = 0;
+  // the batch in flight (launched, not yet finished)
+  bool inflight = false;
+  std::vector<b2d_dedup*> fl_handles;
+  uint64_t fl_bytes = 0;
+  bool fl_scoring = false, fl_any_baseline = false;
+  std::chrono::high_resolution_clock::time_point fl_t0;
+  // tuning: current values, and the online tuner
+  BatchCand cur{0, 3, 4, 8};
+  bool autotune = false;
+  BatchTuner tuner;
+  // last batch
+  double dev_s = 0, host_s = 0;
+  uint32_t launches = 0;
+  uint32_t leaf_groups = 0;
+
+  ~b2d_batch() {
+    for (auto& g : graphs)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+    for (auto e : side_ev)
+      if (e) cudaEventDestroy(e);
+    for (auto s : side)
+      if (s) cudaStreamDestroy(s);
+    if (fork_ev) cudaEventDestroy(fork_ev);
+    for (auto e : ev)
+      if (e) cudaEventDestroy(e);
+    if (own_stream) cudaStreamDestroy(own_stream);
+    if (cap) cudaStreamDestroy(cap);
+  }
+};
+
+namespace {
+
+int ensure_side_streams(b2d_batch* b, int n) {
+  while ((int)b->side.size() < n) {
+    cudaStream_t s = nullptr;
+    cudaEvent_t e = nullptr;
+    B2D_CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    b->side.push_back(s);
+    B2D_CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    b->side_ev.push_back(e);
+  }
+  return B2D_OK;
+}
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+uint64_t key_hash(const std::vector<uint64_t>& k) {
+  uint64_t h = 0x9E3779B97F4A7C15ull ^ k.size();
+  for (uint64_t v : k) {
+    h ^= v + 0x9E3779B97F4A7C15ull + (h << 6) + (h >> 2);
+  }
+  return h;
+}
+
+// Host preparation, graph lookup or capture, and launch of one batch; the device work is left
+// running and batch_finish collects it.
+int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, const uint64_t* lens,
+                 const int* make_baseline, uint32_t count, int* rcs) {
+  using clk = std::chrono::high_resolution_clock;
+  const auto t0 = clk::now();
+  if (b->inflight) return B2D_ERR_ARG;   // one batch in flight per batch object
+  if (count == 0) return B2D_OK;
+  for (uint32_t i = 0; i < count; i++) {
+    if (!hs[i]) return B2D_ERR_ARG;
+    for (uint32_t j = 0; j < i; j++)
+      if (hs[j] == hs[i]) return B2D_ERR_ARG;   // one checkpoint per handle per batch
+  }
+  // tuning for this batch
+  const bool scoring = b->autotune && !b->tuner.done;
+  const BatchCand cand = scoring ? b->tuner.next() : b->cur;
+  int rc = ensure_side_streams(b, cand.streams);
+  if (rc) return rc;
+
+  // host preparation of every handle, with its stream work on the batch stream
+  bool any_baseline = false;
+  uint64_t bytes = 0;
+  for (uint32_t i = 0; i < count; i++) {
+    b2d_dedup* d = hs[i];
+    cudaStream_t keep = d->stream;
+    d->stream = b->stream;
+    const bool mb = make_baseline && make_baseline[i];
+    any_baseline = any_baseline || mb || d->current_id == 0;
+    rc = prepare_checkpoint(d, data[i], lens[i], mb);
+    d->stream = keep;
+    if (rc) {
+      if (rcs) rcs[i] = rc;
+      return rc;
+    }
+    bytes += lens[i];
+  }
+
+  // leaf work items: handles whose leaves the persistent kernel can hash, grouped by
+  // (staging unit, hash kind); the rest hash their own leaves in their branch
+  struct Group {
+    int U, kind;
+    uint32_t beg, end, tiles;
+  };
+  std::vector<Group> groups;
+  std::vector<int> item_of(count, -1);
+  std::vector<std::vector<BatchLeafItem>> by_group;
+  for (uint32_t i = 0; i < count; i++) {
+    b2d_dedup* d = hs[i];
+    if (!d->tune.allow_tma) continue;
+    BatchLeafItem it;
+    std::memset(&it, 0, sizeof(it));
+    const int U = batch_leaf_item(leaf_args(d, &d->state.p->round), it);
+    if (U == 0) continue;
+    size_t g = 0;
+    while (g < groups.size() && !(groups[g].U == U && groups[g].kind == d->kind)) g++;
+    if (g == groups.size()) {
+      groups.push_back(Group{U, d->kind, 0, 0, 0});
+      by_group.emplace_back();
+    }
+    if (by_group[g].size() >= BATCH_MAX_ITEMS) continue;
+    it.tile_begin = groups[g].tiles;
+    groups[g].tiles += it.ntiles;
+    item_of[i] = (int)g;
+    by_group[g].push_back(it);
+  }
+  std::vector<BatchLeafItem> items;
+  for (size_t g = 0; g < groups.size(); g++) {
+    groups[g].beg = (uint32_t)items.size();
+    items.insert(items.end(), by_group[g].begin(), by_group[g].end());
+    groups[g].end = (uint32_t)items.size();
+  }
+
+  // blob layout and contents
+  BatchLayout L;
+  L.items = 0;
+  L.rounds = align_up(sizeof(BatchLeafItem) * items.size(), 64);
+  L.states = align_up(L.rounds + sizeof(RoundState) * count, 64);
+  L.queues = align_up(L.states + sizeof(DevState*) * count, 64);
+  L.bstatus = align_up(L.queues + sizeof(unsigned int) * (groups.size() + 1), 64);
+  L.total = align_up(L.bstatus + sizeof(DevStatus), 256);
+  B2D_CU(b->blob.reserve(L.total));
+  B2D_CU(b->blob_h.reserve(L.total));
+  B2D_CU(b->coll.reserve(count));
+  B2D_CU(b->coll_h.reserve(count));
+  uint8_t* H = b->blob_h.p;
+  if (!items.empty()) std::memcpy(H + L.items, items.data(), sizeof(BatchLeafItem) * items.size());
+  for (uint32_t i = 0; i < count; i++) {
+    std::memcpy(H + L.rounds + sizeof(RoundState) * i, hs[i]->round_h.p, sizeof(RoundState));
+    DevState* p = hs[i]->state.p;
+    std::memcpy(H + L.states + sizeof(DevState*) * i, &p, sizeof(p));
+  }
+  uint8_t* B = b->blob.p;
+  auto* d_items = reinterpret_cast<BatchLeafItem*>(B + L.items);
+  auto* d_rounds = reinterpret_cast<RoundState*>(B + L.rounds);
+  auto* d_states = reinterpret_cast<DevState* const*>(B + L.states);
+  auto* d_queues = reinterpret_cast<unsigned int*>(B + L.queues);
+  auto* d_bst = reinterpret_cast<DevStatus*>(B + L.bstatus);
+
+  // graph key: every handle's launch parameters, the grouping and the tuning
+  std::vector<uint64_t> key, k1;
+  for (uint32_t i = 0; i < count; i++) {
+    graph_key(hs[i], &hs[i]->state.p->round, k1);
+    key.insert(key.end(), k1.begin(), k1.end());
+    key.push_back((uint64_t)(int64_t)item_of[i]);
+  }
+  for (auto& g : groups) key.insert(key.end(), {(uint64_t)g.U, (uint64_t)g.kind, g.beg, g.end, g.tiles});
+  key.insert(key.end(), {(uint64_t)B, (uint64_t)H, L.total, (uint64_t)b->coll.p, (uint64_t)b->coll_h.p, (uint64_t)cand.stages,
+                         (uint64_t)cand.ctas, (uint64_t)cand.tiles_per_pop, (uint64_t)cand.streams});
+
+  const uint64_t kh = key_hash(key);
+  b2d_batch::GraphEntry* ge = nullptr;
+  for (auto& g : b->graphs)
+    if (g.hash == kh && g.key == key) ge = &g;
+  if (!ge) {
+    if (b->graphs.size() >= b->graph_cap) {
+      size_t lru = 0;
+      for (size_t i = 1; i < b->graphs.size(); i++)
+        if (b->graphs[i].last_use < b->graphs[lru].last_use) lru = i;
+      cudaGraphExecDestroy(b->graphs[lru].exec);
+      b->graphs.erase(b->graphs.begin() + (long)lru);
+    }
+    // branch assignment: largest handles first, each to the least loaded branch
+    std::vector<uint32_t> order(count);
+    for (uint32_t i = 0; i < count; i++) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return lens[x] > lens[y]; });
+    const int nb = std::min<int>(cand.streams, (int)count);
+    std::vector<uint64_t> load(nb, 0);
+    std::vector<std::vector<uint32_t>> branch(nb);
+    for (uint32_t i : order) {
+      int best = 0;
+      for (int j = 1; j < nb; j++)
+        if (load[j] < load[best]) best = j;
+      load[best] += lens[i] + (1ull << 20);   // fixed per-checkpoint cost ~ 1 MiB of data
+      branch[best].push_back(i);
+    }
+    cudaGraph_t g = nullptr;
+    B2D_CU(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+    int erc = B2D_OK;
+    auto cap_err = [&](cudaError_t e) {
+      if (e != cudaSuccess && erc == B2D_OK) erc = cuda_status(e);
+    };
+    cap_err(cudaMemcpyAsync(B, H, L.total, cudaMemcpyHostToDevice, b->cap));
+    batch_init_kernel<<<(count + 255) / 256, 256, 0, b->cap>>>(d_states, d_rounds, count, d_queues,
+                                                               (uint32_t)groups.size(), d_bst);
+    cap_err(cudaGetLastError());
+    uint32_t launches = 1;
+    LeafTuning lt;
+    lt.allow_tma = 1;
+    lt.stages = cand.stages;
+    lt.ctas_per_sm = cand.ctas;
+    for (size_t gi = 0; gi < groups.size() && erc == B2D_OK; gi++) {
+      const Group& gr = groups[gi];
+      cap_err(launch_leaves_batch(d_items + gr.beg, gr.end - gr.beg, gr.tiles, gr.U, gr.kind, d_queues + gi, d_bst,
+                                  b->sm_count, lt, (uint32_t)cand.tiles_per_pop, b->cap));
+      launches++;
+    }
+    cap_err(cudaEventRecord(b->fork_ev, b->cap));
+    for (int j = 0; j < nb && erc == B2D_OK; j++) {
+      cudaStream_t s = b->side[j];
+      cap_err(cudaStreamWaitEvent(s, b->fork_ev, 0));
+      for (uint32_t i : branch[j]) {
+        if (erc != B2D_OK) break;
+        b2d_dedup* d = hs[i];
+        const int r = enqueue_checkpoint(d, s, &d->state.p->round, false, false, item_of[i] >= 0, true);
+        if (r != B2D_OK) erc = r;
+        launches += d->launches;
+      }
+      cap_err(cudaEventRecord(b->side_ev[j], s));
+      cap_err(cudaStreamWaitEvent(b->cap, b->side_ev[j], 0));
+    }
+    batch_collect_kernel<<<(count + 127) / 128, 128, 0, b->cap>>>(d_states, count, b->coll.p);
+    cap_err(cudaGetLastError());
+    cap_err(cudaMemcpyAsync(b->coll_h.p, b->coll.p, sizeof(DevState) * count, cudaMemcpyDeviceToHost, b->cap));
+    cap_err(cudaMemcpyAsync(H + L.bstatus, d_bst, sizeof(DevStatus), cudaMemcpyDeviceToHost, b->cap));
+    launches += 1;
+    const cudaError_t ce = cudaStreamEndCapture(b->cap, &g);
+    if (erc != B2D_OK) {
+      if (g) cudaGraphDestroy(g);
+      return erc;
+    }
+    B2D_CU(ce);
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ie = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    B2D_CU(ie);
+    const cudaError_t ue = cudaGraphUpload(exec, b->stream);
+    if (ue != cudaSuccess) {
+      cudaGraphExecDestroy(exec);
+      return cuda_status(ue);
+    }
+    b->graphs.emplace_back();
+    ge = &b->graphs.back();
+    ge->key = key;
+    ge->hash = kh;
+    ge->exec = exec;
+    ge->launches = launches;
+  }
+  ge->last_use = ++b->use_clock;
+  b->launches = ge->launches;
+  b->leaf_groups = (uint32_t)groups.size();
+  b->lay = L;
+  B2D_CU(cudaEventRecord(b->ev[0], b->stream));
+  B2D_CU(cudaGraphLaunch(ge->exec, b->stream));
+  B2D_CU(cudaEventRecord(b->ev[1], b->stream));
+  b->inflight = true;
+  b->fl_handles.assign(hs, hs + count);
+  b->fl_bytes = bytes;
+  b->fl_scoring = scoring;
+  b->fl_any_baseline = any_baseline;
+  b->fl_t0 = t0;
+  return B2D_OK;
+}
+
+// Waits for the batch in flight and completes every handle's checkpoint.
+int batch_finish(b2d_batch* b, int* rcs) {
+  using clk = std::chrono::high_resolution_clock;
+  if (!b->inflight) return B2D_ERR_ARG;
+  b->inflight = false;
+  B2D_CU(cudaEventSynchronize(b->ev[1]));
+  b->dev_s = elapsed_ms(b->ev[0], b->ev[1]) * 1e-3;
+  const uint32_t count = (uint32_t)b->fl_handles.size();
+  b2d_dedup* const* hs = b->fl_handles.data();
+
+  // the persistent leaf kernel's own status (a wait that ran out) fails every handle
+  DevStatus bst;
+  std::memcpy(&bst, b->blob_h.p + b->lay.bstatus, sizeof(bst));
+  int first_rc = status_code(bst);
+  for (uint32_t i = 0; i < count; i++) {
+    b2d_dedup* d = hs[i];
+    *d->state_h.p = b->coll_h.p[i];
+    cudaStream_t keep = d->stream;
+    d->stream = b->stream;
+    int r = finish_checkpoint(d, true, false);
+    d->stream = keep;
+    if (r == B2D_OK && first_rc != B2D_OK) {
+      r = first_rc;
+      d->diff_valid = false;
+    }
+    d->phase[0] = d->phase[1] = d->phase[2] = 0;
+    if (rcs) rcs[i] = r;
+    if (r != B2D_OK && first_rc == B2D_OK) first_rc = r;
+  }
+  b->host_s = secs(b->fl_t0, clk::now());
+  // baselines cost more than incremental checkpoints: only incremental batches are compared
+  if (b->fl_scoring && !b->fl_any_baseline && first_rc == B2D_OK) {
+    b->tuner.report(b->dev_s > 0 ? (double)b->fl_bytes / b->dev_s : 0.0);
+    if (b->tuner.done) b->cur = b->tuner.base;
+  }
+  b->fl_handles.clear();
+  return first_rc;
+}
+
 }  // namespace
 
 #define B2D_GUARD(body)                    \
@@ -648,6 +1276,7 @@ int b2d_create(uint32_t chunk_size, int hash_kind, b2d_dedup** out) {
     cudaError_t e = cudaGetDevice(&d->device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&d->sm_count, cudaDevAttrMultiProcessorCount, d->device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&d->own_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&d->cap_stream, cudaStreamNonBlocking);
     for (auto& ev : d->ev)
       if (e == cudaSuccess) e = cudaEventCreate(&ev);
     if (e != cudaSuccess) {
@@ -783,6 +1412,7 @@ int b2d_set_param(b2d_dedup* d, const char* name, int64_t value) {
   else if (k == "leaf_stages" && value >= 0 && value <= 16) d->tune.stages = (int)value;
   else if (k == "leaf_ctas_per_sm" && value >= 0 && value <= 8) d->tune.ctas_per_sm = (int)value;
   else if (k == "map_max_load_pct" && value >= 10 && value <= 90) d->map_max_load = value / 100.0;
+  else if (k == "map_headroom_pct" && value >= 100 && value <= 1000) d->map_headroom = value / 100.0;
   else return B2D_ERR_ARG;
   return B2D_OK;
 }
@@ -857,6 +1487,162 @@ int b2d_hash_chunks(int kind, const void* d_data, uint64_t len, uint32_t cs, voi
                                                       static_cast<Digest*>(d_out));
   B2D_CU(cudaGetLastError());
   B2D_CU(cudaStreamSynchronize(s));
+  return B2D_OK;
+}
+
+int b2d_map_stats(b2d_dedup* d, double out[5]) {
+  if (!d || !out) return B2D_ERR_ARG;
+  out[0] = (double)d->map_cap;
+  out[1] = (double)d->map_size_host;
+  out[2] = (double)d->map_grows;
+  out[3] = d->map_grow_s;
+  out[4] = d->map_alloc_s;
+  return B2D_OK;
+}
+
+int b2d_memory(b2d_dedup* d, uint64_t* bytes) {
+  if (!d || !bytes) return B2D_ERR_ARG;
+  *bytes = handle_bytes(d);
+  return B2D_OK;
+}
+
+int b2d_estimate_memory(uint64_t len, uint32_t chunk_size, int map_max_load_pct, uint64_t* bytes) {
+  if (!bytes || chunk_size == 0 || len == 0) return B2D_ERR_ARG;
+  if (map_max_load_pct <= 0) map_max_load_pct = 75;
+  if (map_max_load_pct < 10 || map_max_load_pct > 90) return B2D_ERR_ARG;
+  // the allocations prepare_checkpoint makes for a buffer of `len` bytes (checkpoint side)
+  const uint64_t n = (len + chunk_size - 1) / chunk_size, N = 2 * n - 1;
+  const uint64_t cap = map_capacity(2 * N, map_max_load_pct / 100.0, 1.25);
+  uint64_t b = N * sizeof(Digest) + N + (n + 16) + ((N + 15) / 16 * 16 + 16) + n;   // tree, labels, flags
+  b += (cap + 1) * sizeof(MapSlot) + 8;                                              // map
+  b += 8 * 4 * n + 68 * 4;                                                           // lists and keys
+  b += (uint64_t)64 * 4 * 2 + (uint64_t)1184 * 64 * 4 + 2 * SCAN_GRID * 4;           // buckets, partials
+  b += 64 + 16 * n + n * chunk_size;                                                 // diff
+  b += sizeof(DevState);
+  *bytes = b;
+  return B2D_OK;
+}
+
+int b2d_batch_create(b2d_batch** out) {
+  B2D_GUARD({
+    if (!out) return B2D_ERR_ARG;
+    *out = nullptr;
+    b2d_batch* b = new b2d_batch();
+    cudaError_t e = cudaGetDevice(&b->device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, b->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming);
+    for (auto& ev : b->ev)
+      if (e == cudaSuccess) e = cudaEventCreate(&ev);
+    if (e != cudaSuccess) {
+      delete b;
+      return cuda_status(e);
+    }
+    b->stream = b->own_stream;
+    *out = b;
+    return B2D_OK;
+  })
+}
+
+int b2d_batch_destroy(b2d_batch* b) {
+  if (!b) return B2D_ERR_ARG;
+  if (b->inflight) batch_finish(b, nullptr);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  delete b;
+  return B2D_OK;
+}
+
+int b2d_batch_set_stream(b2d_batch* b, void* s) {
+  if (!b) return B2D_ERR_ARG;
+  b->stream = s ? static_cast<cudaStream_t>(s) : b->own_stream;
+  return B2D_OK;
+}
+
+int b2d_batch_set_param(b2d_batch* b, const char* name, int64_t value) {
+  if (!b || !name) return B2D_ERR_ARG;
+  const std::string k(name);
+  if (k == "leaf_stages" && value >= 0 && value <= 16) b->cur.stages = (int)value;
+  else if (k == "leaf_ctas_per_sm" && value >= 0 && value <= 8) b->cur.ctas = (int)value;
+  else if (k == "tiles_per_pop" && value >= 1 && value <= 1024) b->cur.tiles_per_pop = (int)value;
+  else if (k == "streams" && value >= 1 && value <= 64) b->cur.streams = (int)value;
+  else if (k == "graph_cache" && value >= 1 && value <= 4096) b->graph_cap = (size_t)value;
+  else if (k == "autotune" && (value == 0 || value == 1)) {
+    b->autotune = value != 0;
+    b->tuner.reset(b->cur);
+  } else return B2D_ERR_ARG;
+  return B2D_OK;
+}
+
+int b2d_batch_get_param(b2d_batch* b, const char* name, int64_t* value) {
+  if (!b || !name || !value) return B2D_ERR_ARG;
+  const std::string k(name);
+  if (k == "leaf_stages") *value = b->cur.stages;
+  else if (k == "leaf_ctas_per_sm") *value = b->cur.ctas;
+  else if (k == "tiles_per_pop") *value = b->cur.tiles_per_pop;
+  else if (k == "streams") *value = b->cur.streams;
+  else if (k == "autotune") *value = b->autotune ? 1 : 0;
+  else if (k == "tuned") *value = b->tuner.done ? 1 : 0;
+  else if (k == "graph_cache") *value = (int64_t)b->graph_cap;
+  else if (k == "graphs") *value = (int64_t)b->graphs.size();
+  else return B2D_ERR_ARG;
+  return B2D_OK;
+}
+
+int b2d_batch_checkpoint(b2d_batch* b, b2d_dedup* const* handles, const void* const* d_data, const uint64_t* lens,
+                         const int* make_baseline, uint32_t count, int* rcs) {
+  B2D_GUARD({
+    if (!b || (count && (!handles || !d_data || !lens))) return B2D_ERR_ARG;
+    int rc = batch_launch(b, handles, d_data, lens, make_baseline, count, rcs);
+    if (rc != B2D_OK || count == 0) return rc;
+    return batch_finish(b, rcs);
+  })
+}
+
+int b2d_batch_launch(b2d_batch* b, b2d_dedup* const* handles, const void* const* d_data, const uint64_t* lens,
+                     const int* make_baseline, uint32_t count, int* rcs) {
+  B2D_GUARD({
+    if (!b || !count || !handles || !d_data || !lens) return B2D_ERR_ARG;
+    return batch_launch(b, handles, d_data, lens, make_baseline, count, rcs);
+  })
+}
+
+int b2d_batch_query(b2d_batch* b, int* done) {
+  if (!b || !done) return B2D_ERR_ARG;
+  if (!b->inflight) {
+    *done = -1;
+    return B2D_OK;
+  }
+  const cudaError_t e = cudaEventQuery(b->ev[1]);
+  if (e == cudaErrorNotReady) {
+    *done = 0;
+    return B2D_OK;
+  }
+  *done = 1;
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    return cuda_status(e);
+  }
+  return B2D_OK;
+}
+
+int b2d_batch_wait(b2d_batch* b, int* rcs) {
+  B2D_GUARD({
+    if (!b) return B2D_ERR_ARG;
+    return batch_finish(b, rcs);
+  })
+}
+
+int b2d_batch_times(b2d_batch* b, double out[2]) {
+  if (!b || !out) return B2D_ERR_ARG;
+  out[0] = b->dev_s;
+  out[1] = b->host_s;
+  return B2D_OK;
+}
+
+int b2d_batch_launch_count(b2d_batch* b, uint32_t* out) {
+  if (!b || !out) return B2D_ERR_ARG;
+  *out = b->launches;
   return B2D_OK;
 }
 

@@ -1,5 +1,7 @@
 // Kernel argument blocks and launcher declarations shared by the dedup translation units.
 #pragma once
+#include <cuda.h>
+
 #include "common.cuh"
 #include "map.cuh"
 
@@ -9,6 +11,17 @@ constexpr uint32_t TMA_CONSUMER_WARPS = 8;   // 256 chunks per TMA tile
 constexpr uint32_t FOREST_BAND_LEVELS = 12;  // levels fused per forest band launch (4096-leaf subtrees)
 constexpr uint32_t SCAN_GRID = 296;          // fixed grid of the reduce-then-scan passes (2 x 148 SMs)
 constexpr uint32_t MAX_BUCKETS = 8192;       // source-checkpoint buckets handled per shift partition
+
+// Values that change from one checkpoint to the next.  Kernels read them from device memory
+// (not from launch parameters), so one captured launch sequence -- a CUDA graph -- serves every
+// checkpoint of a buffer.
+struct RoundState {
+  uint32_t cur;          // current_id
+  uint32_t baseline_id;  // ref_id written into the header
+  uint32_t baseline;     // 1: baseline checkpoint
+  uint32_t buckets;      // cur + 1: source-checkpoint buckets of the shift entries
+  MapView map;           // the digest map (moves when it grows; graphs read it here)
+};
 
 struct LeafArgs {
   const uint8_t* data;
@@ -23,6 +36,7 @@ struct LeafArgs {
   uint8_t* dupflag;   // per chunk: leaf shares a new digest with another leaf (see leaf.cu)
   MapView map;
   DevStatus* st;
+  const RoundState* rs;
 };
 
 struct ForestArgs {
@@ -38,6 +52,7 @@ struct ForestArgs {
   uint32_t cur;
   int kind;
   int baseline;
+  const RoundState* rs;
 };
 
 // Per-checkpoint sizes, computed on the device so no host round trip is needed mid-checkpoint.
@@ -74,7 +89,31 @@ struct DiffArgs {
   uint32_t* partial;      // SCAN_GRID * max(2, cur+1) scratch
   uint32_t* partial2;     // SCAN_GRID * 2 scratch
   uint8_t* diff;          // device diff buffer
+  const RoundState* rs;
 };
+
+// launch parameters carry the buffer geometry; the per-checkpoint values come from *rs
+__device__ __forceinline__ LeafArgs with_round(const LeafArgs& p) {
+  LeafArgs a = p;
+  a.cur = p.rs->cur;
+  a.baseline = (int)p.rs->baseline;
+  a.map = p.rs->map;
+  return a;
+}
+__device__ __forceinline__ ForestArgs with_round(const ForestArgs& p) {
+  ForestArgs a = p;
+  a.cur = p.rs->cur;
+  a.baseline = (int)p.rs->baseline;
+  a.map = p.rs->map;
+  return a;
+}
+__device__ __forceinline__ DiffArgs with_round(const DiffArgs& p) {
+  DiffArgs a = p;
+  a.cur = p.rs->cur;
+  a.baseline_id = p.rs->baseline_id;
+  a.map = p.rs->map;
+  return a;
+}
 
 // Tunables of the staged leaf kernel (0 = default).  Chosen per workload by the autotuner.
 struct LeafTuning {
@@ -83,10 +122,27 @@ struct LeafTuning {
   int ctas_per_sm = 0;   // resident CTAs per SM (default 3)
 };
 int launch_leaves(const LeafArgs& a, int sm_count, const LeafTuning& tune, cudaStream_t stream);
+
+// one buffer of a batched hashing launch (the tensor map must stay 64-byte aligned)
+constexpr uint32_t BATCH_MAX_ITEMS = 1024;
+struct __align__(64) BatchLeafItem {
+  CUtensorMap map;
+  LeafArgs args;
+  uint32_t nfull;        // whole chunks (TMA rows)
+  uint32_t S;            // segments per chunk
+  uint32_t tile_begin;   // first global tile of this buffer
+  uint32_t ntiles;
+};
+// Fills `item` for one buffer; returns the segment width U (0: the buffer cannot be staged).
+int batch_leaf_item(const LeafArgs& a, BatchLeafItem& item);
+// One persistent launch over all items (same U and hash kind).  `queue` is a zeroed counter.
+cudaError_t launch_leaves_batch(const BatchLeafItem* d_items, uint32_t nitems, uint32_t total_tiles, int U, int kind,
+                                unsigned int* queue, DevStatus* st, int sm_count, const LeafTuning& tune,
+                                uint32_t tiles_per_pop, cudaStream_t stream);
 cudaError_t launch_forest(const ForestArgs& a, int phase, cudaStream_t stream);
-int forest_launch_count(uint32_t D);
-cudaError_t launch_zero_exists(const MapView& m, int* flag, cudaStream_t stream);
-cudaError_t launch_baseline_inserts(const ForestArgs& a, int sm_count, cudaStream_t stream);
-cudaError_t launch_collect_diff(const DiffArgs& a, int sm_count, cudaStream_t stream);
+int forest_launch_count(uint32_t D, int phase);
+cudaError_t launch_zero_exists(int* flag, const RoundState* rs, cudaStream_t stream);
+// bcap: bucket capacity the scratch was sized for (>= rs->buckets of every checkpoint run)
+cudaError_t launch_collect_diff(const DiffArgs& a, uint32_t bcap, int sm_count, cudaStream_t stream);
 
 }  // namespace b2d

@@ -72,8 +72,16 @@ __device__ __noinline__ uint8_t shift_pair(const ForestArgs& a, uint32_t x) {
   return DONE;
 }
 
-__device__ __noinline__ void hash_baseline_parent(const ForestArgs& a, uint32_t x) {
-  a.tree[x] = hash_pair(a.kind, a.tree[2u * x + 1u], a.tree[2u * x + 2u]);   // inserted by baseline_insert_kernel
+// baseline "Insert entries" (:218-224) for a parent that is not a first occurrence (those were
+// hashed and inserted by phase 1 with a lower priority, so re-inserting them changes nothing):
+// hash, insert with priority 64 + height
+__device__ __noinline__ void baseline_parent(const ForestArgs& a, uint32_t x) {
+  const Digest d = hash_pair(a.kind, a.tree[2u * x + 1u], a.tree[2u * x + 2u]);
+  a.tree[x] = d;
+  const uint32_t height = a.D - node_level(x);
+  const unsigned long long v = ((unsigned long long)(64u + height) << 32) | x;
+  const MapRef ref = map_insert(a.map, d, v, a.cur, a.st);
+  if (ref.found && !ref.inserted) map_merge_current(a.map, ref.slot, v, a.cur);
 }
 
 template <int PHASE>
@@ -96,7 +104,7 @@ __device__ __forceinline__ uint8_t forest_node(const ForestArgs& a, uint32_t x, 
     } else {
       out = ll;   // FIXED, FIRST or DONE pairs keep the label
     }
-    if (a.baseline) hash_baseline_parent(a, x);
+    if (a.baseline && out != FIRST_OCUR) baseline_parent(a, x);
     return out;
   }
 }
@@ -165,110 +173,137 @@ __device__ __forceinline__ uint32_t pair_and(uint32_t m, int w) {
   return r;
 }
 
-// Phase-1 band: 12 levels above inputs at level `in`.  The first-occurrence labels are folded
-// as bit masks (a parent is a first occurrence iff both children are); the parents found are
-// recorded in a per-CTA bit set, and only then hashed and inserted level by level with all
-// threads of the CTA, so a run of new chunks costs one hash per node spread over the CTA
-// instead of a serial chain per thread.
-constexpr uint32_t FF_WORDS = 128;   // 4095 bits: heights 1..12 of a 4096-input band
+// Phase-1 band: 10 levels above the inputs at level `in` (1024 inputs per CTA of 256 threads:
+// 2 levels in registers, 5 by warp shuffles, 3 through shared memory).  A parent is a first
+// occurrence iff both children are; its digest is computed where its label is, from the
+// children's digests held in registers (shuffled between lanes), so a run of new chunks costs
+// one hash per node with no memory round trip between levels.  The parents found are recorded
+// in a per-CTA bit set and inserted into the map at the end, spread evenly over the threads.
+constexpr uint32_t FF_LEVELS = 10;
+constexpr uint32_t FF_WORDS = 32;          // 1023 bits: band heights 1..10
 __device__ __forceinline__ uint32_t ff_base(uint32_t k) {   // first bit of band height k
-  return 4096u - (8192u >> k);
+  return 1024u - (2048u >> k);
 }
-__global__ void __launch_bounds__(FAST_THREADS) forest_first_kernel(ForestArgs a, uint32_t in) {
+__device__ __forceinline__ void ff_set(uint32_t* ff, uint32_t k, uint32_t i) {
+  const uint32_t bit = ff_base(k) + i;
+  atomicOr(&ff[bit >> 5], 1u << (bit & 31u));
+}
+__device__ __forceinline__ Digest shfl_down_digest(const Digest& d, uint32_t delta) {
+  Digest r;
+#pragma unroll
+  for (int k = 0; k < 4; k++) r.w[k] = __shfl_down_sync(0xffffffffu, d.w[k], delta);
+  return r;
+}
+
+__global__ void __launch_bounds__(FAST_THREADS) forest_first_kernel(ForestArgs a0, uint32_t in) {
+  const ForestArgs a = with_round(a0);
   __shared__ uint32_t ff[FF_WORDS];
-  __shared__ uint32_t wbits[FAST_THREADS / 32];
+  __shared__ uint32_t wbit[FAST_THREADS / 32];
+  __shared__ Digest wdig[FAST_THREADS / 32];
+  __shared__ uint32_t wpre[FF_WORDS + 1];
   const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
   if (t < FF_WORDS) ff[t] = 0;
   __syncthreads();
-  const uint64_t root = ((1ull << (in - FAST_LEVELS)) - 1ull) + blockIdx.x;
-  const uint64_t x0 = (root << FAST_LEVELS) + ((1ull << FAST_LEVELS) - 1ull) + 16ull * t;
-  const uint64_t p0 = (x0 - 1ull) >> 1;   // first height-1 node of this thread
-  uint32_t m0 = 0;        // first-occurrence inputs
-  uint32_t m1 = 0;        // first-occurrence height-1 nodes (leaf or inner)
-  uint32_t inner1 = 0xffu;
-  if (in == a.D && (a.n & (a.n - 1u)) == 0) {
-    const uint4 w = *reinterpret_cast<const uint4*>(a.leaflab + (x0 - (a.n - 1u)));
-    const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      // exact per-byte zero test (FIRST = 0): no borrow crosses bytes
-      const uint32_t z = ~(((ws[k] & 0x7f7f7f7fu) + 0x7f7f7f7fu) | ws[k] | 0x7f7f7f7fu);
-      m0 |= ((z >> 7) & 1u | (z >> 14) & 2u | (z >> 21) & 4u | (z >> 28) & 8u) << (4 * k);
-    }
+  const uint64_t root = ((1ull << (in - FF_LEVELS)) - 1ull) + blockIdx.x;
+  const uint64_t x0 = (root << FF_LEVELS) + ((1ull << FF_LEVELS) - 1ull) + 4ull * t;
+  const uint64_t p0 = (x0 - 1ull) >> 1;
+  uint32_t m0 = 0;   // first-occurrence inputs
+  const bool aligned = in == a.D && (a.n & (a.n - 1u)) == 0;
+  if (aligned) {
+    // power-of-two leaf count, leaf band: inputs are chunks 4t.. of this CTA's 1024
+    const uint32_t w = *reinterpret_cast<const uint32_t*>(a.leaflab + (x0 - (a.n - 1u)));
+    const uint32_t z = ~(((w & 0x7f7f7f7fu) + 0x7f7f7f7fu) | w | 0x7f7f7f7fu);   // exact: byte == FIRST (0)
+    m0 = ((z >> 7) & 1u) | ((z >> 14) & 2u) | ((z >> 21) & 4u) | ((z >> 28) & 8u);
     if (m0) {   // lowest-index relabel of the first occurrences flagged by the leaf stage
-      for (int j = 0; j < 16; j++)
+#pragma unroll
+      for (int j = 0; j < 4; j++)
         if ((m0 >> j) & 1u)
           if (leaf_view<1>(a, (uint32_t)(x0 + j), FIRST_OCUR) != FIRST_OCUR) m0 &= ~(1u << j);
     }
-    m1 = pair_and(m0, 8);
   } else {
 #pragma unroll
-    for (int j = 0; j < 16; j++) m0 |= (uint32_t)(input_label<1>(a, x0 + j) == FIRST_OCUR) << j;
-    const uint32_t both = pair_and(m0, 8);
+    for (int j = 0; j < 4; j++) m0 |= (uint32_t)(input_label<1>(a, x0 + j) == FIRST_OCUR) << j;
+  }
+  // band height 1: nodes p0, p0 + 1
+  Digest d1[2];
+  uint32_t m1 = 0;
 #pragma unroll
-    for (int j = 0; j < 8; j++) {
-      const uint64_t p = p0 + j;
-      uint32_t bit;
-      if (p >= a.N) { bit = 0; inner1 &= ~(1u << j); }
-      else if (p >= (uint64_t)a.n - 1u) { bit = forest_leaf<1>(a, (uint32_t)p) == FIRST_OCUR; inner1 &= ~(1u << j); }
-      else bit = (both >> j) & 1u;
-      m1 |= bit << j;
+  for (int j = 0; j < 2; j++) {
+    const uint64_t p = p0 + j;
+    d1[j].w[0] = d1[j].w[1] = d1[j].w[2] = d1[j].w[3] = 0u;
+    if (!aligned && p >= a.N) continue;
+    if (!aligned && p >= (uint64_t)a.n - 1u) {   // a leaf on level D-1 (chunk count not a power of two)
+      if (forest_leaf<1>(a, (uint32_t)p) == FIRST_OCUR) {
+        d1[j] = a.tree[p];
+        m1 |= 1u << j;
+      }
+      continue;
+    }
+    if (((m0 >> (2 * j)) & 3u) == 3u) {
+      d1[j] = hash_pair(a.kind, a.tree[x0 + 2 * j], a.tree[x0 + 2 * j + 1]);
+      a.tree[p] = d1[j];
+      m1 |= 1u << j;
+      ff_set(ff, 1, 2u * t + j);
     }
   }
-  const uint32_t m2 = pair_and(m1, 4), m3 = pair_and(m2, 2), m4 = pair_and(m3, 1);
-  // record parents to hash (inner nodes only): heights 1..4 of this thread
-  if (m1 & inner1) atomicOr(&ff[(ff_base(1) + 8u * t) >> 5], (m1 & inner1) << ((8u * t) & 31u));
-  if (m2) atomicOr(&ff[(ff_base(2) + 4u * t) >> 5], m2 << ((4u * t) & 31u));
-  if (m3) atomicOr(&ff[(ff_base(3) + 2u * t) >> 5], m3 << ((2u * t) & 31u));
-  if (m4) atomicOr(&ff[(ff_base(4) + t) >> 5], 1u << (t & 31u));
-  // warp: heights 5..9
-  uint32_t b = m4;
+  // band height 2: node (root << 8) + 255 + t
+  uint64_t y = (p0 - 1ull) >> 1;
+  uint32_t b = 0;
+  Digest dg;
+  dg.w[0] = dg.w[1] = dg.w[2] = dg.w[3] = 0u;
+  if (m1 == 3u) {
+    dg = hash_pair(a.kind, d1[0], d1[1]);
+    a.tree[y] = dg;
+    b = 1;
+    ff_set(ff, 2, t);
+  }
+  // band heights 3..7: warp shuffles
+  if (__any_sync(0xffffffffu, b)) {
 #pragma unroll
-  for (int s = 0; s < 5; s++) {
-    const uint32_t rb = __shfl_down_sync(0xffffffffu, b, 1u << s);
-    if ((lane & ((2u << s) - 1u)) == 0) {
-      b &= rb;
-      if (b) {
-        const uint32_t idx = t >> (s + 1);
-        atomicOr(&ff[(ff_base(5 + s) + idx) >> 5], 1u << ((ff_base(5 + s) + idx) & 31u));
+    for (int s = 0; s < 5; s++) {
+      const uint32_t rb = __shfl_down_sync(0xffffffffu, b, 1u << s);
+      const Digest rd = shfl_down_digest(dg, 1u << s);
+      if ((lane & ((2u << s) - 1u)) == 0) {
+        y = (y - 1ull) >> 1;
+        b &= rb;
+        if (b) {
+          dg = hash_pair(a.kind, dg, rd);
+          a.tree[y] = dg;
+          ff_set(ff, 3 + s, t >> (s + 1));
+        }
       }
     }
+  } else {
+    b = 0;
   }
-  if (lane == 0) wbits[warp] = b;
+  if (lane == 0) {
+    wbit[warp] = b;
+    wdig[warp] = dg;
+  }
   __syncthreads();
+  // band heights 8..10: the 8 warp results
   if (warp == 0) {
-    b = lane < FAST_THREADS / 32 ? wbits[lane] : 0u;
+    b = lane < FAST_THREADS / 32 ? wbit[lane] : 0u;
+    if (lane < FAST_THREADS / 32) dg = wdig[lane];
+    y = (root << 3) + 7ull + lane;
 #pragma unroll
     for (int s = 0; s < 3; s++) {
       const uint32_t rb = __shfl_down_sync(0xffffffffu, b, 1u << s);
+      const Digest rd = shfl_down_digest(dg, 1u << s);
       if ((lane & ((2u << s) - 1u)) == 0 && lane < FAST_THREADS / 32) {
+        y = (y - 1ull) >> 1;
         b &= rb;
         if (b) {
-          const uint32_t idx = lane >> (s + 1);
-          atomicOr(&ff[(ff_base(10 + s) + idx) >> 5], 1u << ((ff_base(10 + s) + idx) & 31u));
+          dg = hash_pair(a.kind, dg, rd);
+          a.tree[y] = dg;
+          ff_set(ff, 8 + s, lane >> (s + 1));
         }
       }
     }
     if (lane == 0) band_output<1>(a, root, b ? FIRST_OCUR : DONE);
   }
   __syncthreads();
-  if (!__syncthreads_or(t < FF_WORDS && ff[t] != 0)) return;
-  // hash the recorded parents one height at a time (a parent needs its children's digests);
-  // the map inserts wait until every digest is known, then run spread evenly over the CTA
-  for (uint32_t k = 1; k <= FAST_LEVELS; k++) {
-    const uint32_t cnt = 4096u >> k, base = ff_base(k);
-    const uint64_t first = (root << (FAST_LEVELS - k)) + (1ull << (FAST_LEVELS - k)) - 1ull;
-    for (uint32_t i = t; i < cnt; i += FAST_THREADS) {
-      const uint32_t bit = base + i;
-      if ((ff[bit >> 5] >> (bit & 31u)) & 1u) {
-        const uint32_t x = (uint32_t)(first + i);
-        a.tree[x] = hash_pair(a.kind, a.tree[2u * x + 1u], a.tree[2u * x + 2u]);
-      }
-    }
-    __syncthreads();
-  }
   // inserts: rank the set bits (prefix of per-word counts), thread t takes ranks t, t+256, ...
-  __shared__ uint32_t wpre[FF_WORDS + 1];
   if (t < FF_WORDS) wpre[t + 1] = __popc(ff[t]);
   if (t == 0) wpre[0] = 0;
   __syncthreads();
@@ -286,8 +321,8 @@ __global__ void __launch_bounds__(FAST_THREADS) forest_first_kernel(ForestArgs a
     while (skip--) word &= word - 1u;   // drop the lower set bits
     const uint32_t bit = lo * 32u + (__ffs(word) - 1u);
     uint32_t k = 1;                     // band height of this bit
-    while (k < FAST_LEVELS && bit >= ff_base(k + 1)) k++;
-    const uint64_t first = (root << (FAST_LEVELS - k)) + (1ull << (FAST_LEVELS - k)) - 1ull;
+    while (k < FF_LEVELS && bit >= ff_base(k + 1)) k++;
+    const uint64_t first = (root << (FF_LEVELS - k)) + (1ull << (FF_LEVELS - k)) - 1ull;
     const uint32_t x = (uint32_t)(first + (bit - ff_base(k)));
     insert_first_parent(a, x, a.tree[x]);
   }
@@ -295,7 +330,8 @@ __global__ void __launch_bounds__(FAST_THREADS) forest_first_kernel(ForestArgs a
 
 // Fast band: inputs at level `in`, outputs at level in - 12.
 template <int PHASE>
-__global__ void __launch_bounds__(FAST_THREADS) forest_fast_kernel(ForestArgs a, uint32_t in) {
+__global__ void __launch_bounds__(FAST_THREADS) forest_fast_kernel(ForestArgs a0, uint32_t in) {
+  const ForestArgs a = with_round(a0);
   __shared__ uint8_t wlab[FAST_THREADS / 32];
   const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
   const uint64_t root = ((1ull << (in - FAST_LEVELS)) - 1ull) + blockIdx.x;
@@ -376,7 +412,8 @@ __global__ void __launch_bounds__(FAST_THREADS) forest_fast_kernel(ForestArgs a,
 // General band: levels [top, bot] (top <= bot <= D), level by level through shared memory.
 // Nodes at level `bot` are leaves or combine children at level bot+1 read from `lab`.
 template <int PHASE>
-__global__ void __launch_bounds__(FOREST_THREADS) forest_band_kernel(ForestArgs a, uint32_t top, uint32_t bot) {
+__global__ void __launch_bounds__(FOREST_THREADS) forest_band_kernel(ForestArgs a0, uint32_t top, uint32_t bot) {
+  const ForestArgs a = with_round(a0);
   __shared__ uint8_t buf[2][1u << (FOREST_BAND_LEVELS - 1)];
   const uint32_t H = bot - top;
   const uint64_t root = ((1ull << top) - 1ull) + blockIdx.x;
@@ -404,16 +441,19 @@ __global__ void __launch_bounds__(FOREST_THREADS) forest_band_kernel(ForestArgs 
   }
 }
 
+static uint32_t band_levels(int phase) { return phase == 1 ? FF_LEVELS : FAST_LEVELS; }
+
 cudaError_t launch_forest(const ForestArgs& a, int phase, cudaStream_t stream) {
   if (a.N <= 1) return cudaSuccess;   // one chunk: no inner nodes; the reference never pushes a region
+  const uint32_t L = band_levels(phase);
   uint32_t in = a.D;                  // labels at level `in` are known (leaves, or a band's output)
-  while (in >= FAST_LEVELS) {
-    const uint32_t ctas = 1u << (in - FAST_LEVELS);
+  while (in >= L) {
+    const uint32_t ctas = 1u << (in - L);
     if (phase == 1) forest_first_kernel<<<ctas, FAST_THREADS, 0, stream>>>(a, in);
     else forest_fast_kernel<2><<<ctas, FAST_THREADS, 0, stream>>>(a, in);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    in -= FAST_LEVELS;
+    in -= L;
   }
   if (in == 0) return cudaSuccess;    // the root was a fast band output
   // remaining levels [0, bot]: bot = D when no fast band ran (start from the leaves), else in-1
@@ -431,11 +471,12 @@ cudaError_t launch_forest(const ForestArgs& a, int phase, cudaStream_t stream) {
   return cudaSuccess;
 }
 
-int forest_launch_count(uint32_t D) {
+int forest_launch_count(uint32_t D, int phase) {
   if (D == 0) return 0;
   int c = 0;
   uint32_t in = D;
-  while (in >= FAST_LEVELS) { c++; in -= FAST_LEVELS; }
+  const uint32_t L = band_levels(phase);
+  while (in >= L) { c++; in -= L; }
   if (in == 0) return c;
   int bot = (in == D) ? (int)D : (int)in - 1;
   while (bot >= 0) {
@@ -447,30 +488,19 @@ int forest_launch_count(uint32_t D) {
   return c;
 }
 
-__global__ void zero_exists_kernel(MapView m, int* flag) {
+__global__ void zero_exists_kernel(int* flag, const RoundState* rs) {
+  if (!rs->baseline) return;   // only the baseline tests the stale zero digest
   Digest z;
   z.w[0] = z.w[1] = z.w[2] = z.w[3] = 0u;
+  const MapView m = rs->map;
   *flag = map_find(m, z) <= m.cap ? 1 : 0;
 }
 
-cudaError_t launch_zero_exists(const MapView& m, int* flag, cudaStream_t stream) {
-  zero_exists_kernel<<<1, 1, 0, stream>>>(m, flag);
+cudaError_t launch_zero_exists(int* flag, const RoundState* rs, cudaStream_t stream) {
+  zero_exists_kernel<<<1, 1, 0, stream>>>(flag, rs);
   return cudaGetLastError();
 }
 
-// baseline "Insert entries" (:218-224): every inner node, priority 64 + height
-__global__ void baseline_insert_kernel(ForestArgs a) {
-  for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x + 1u < a.n; x += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t height = a.D - node_level((uint32_t)x);
-    const unsigned long long v = ((unsigned long long)(64u + height) << 32) | x;
-    const MapRef ref = map_insert(a.map, a.tree[x], v, a.cur, a.st);
-    if (ref.found && !ref.inserted) map_merge_current(a.map, ref.slot, v, a.cur);
-  }
-}
 
-cudaError_t launch_baseline_inserts(const ForestArgs& a, int sm_count, cudaStream_t stream) {
-  baseline_insert_kernel<<<(unsigned)sm_count * 8u, 256, 0, stream>>>(a);
-  return cudaGetLastError();
-}
 
 }  // namespace b2d

@@ -42,7 +42,8 @@ __device__ __forceinline__ void count16(uint4 v, uint32_t& cf, uint32_t& cs) {
   }
 }
 
-__global__ void __launch_bounds__(COMPACT_THREADS) compact_count_kernel(DiffArgs a) {
+__global__ void __launch_bounds__(COMPACT_THREADS) compact_count_kernel(DiffArgs a0) {
+  const DiffArgs a = with_round(a0);
   __shared__ uint32_t sh[COMPACT_THREADS / 32 + 1];
   const uint64_t groups = ((uint64_t)a.N + 15u) / 16u;
   uint64_t beg, end;
@@ -60,7 +61,8 @@ __global__ void __launch_bounds__(COMPACT_THREADS) compact_count_kernel(DiffArgs
   }
 }
 
-__global__ void __launch_bounds__(1024) compact_scan_kernel(DiffArgs a, uint32_t g) {
+__global__ void __launch_bounds__(1024) compact_scan_kernel(DiffArgs a0, uint32_t g) {
+  const DiffArgs a = with_round(a0);
   __shared__ uint32_t sh[33];
   uint32_t tf, ts;
   const uint32_t i = threadIdx.x;
@@ -81,7 +83,8 @@ __global__ void __launch_bounds__(1024) compact_scan_kernel(DiffArgs a, uint32_t
 // COMPACT_GROUPS consecutive 16-node groups of a tile, so one block scan covers
 // COMPACT_THREADS * COMPACT_GROUPS * 16 nodes and the loads of a thread are independent.
 constexpr uint32_t COMPACT_GROUPS = 4;   // tile of 32768 nodes keeps both packed 16-bit counts exact
-__global__ void __launch_bounds__(COMPACT_THREADS) compact_write_kernel(DiffArgs a) {
+__global__ void __launch_bounds__(COMPACT_THREADS) compact_write_kernel(DiffArgs a0) {
+  const DiffArgs a = with_round(a0);
   __shared__ uint32_t sh[COMPACT_THREADS / 32 + 1];
   const uint64_t groups = ((uint64_t)a.N + 15u) / 16u;
   uint64_t beg, end;
@@ -150,7 +153,8 @@ __device__ __forceinline__ uint32_t warp_lower_bound(const uint32_t* v, uint32_t
 
 // level runs of the node-order lists: levels[L] = start of level L in tmp_first,
 // levels[34 + L] in tmp_shift (L = 0..D+1); one warp per search
-__global__ void compact_levels_kernel(DiffArgs a) {
+__global__ void compact_levels_kernel(DiffArgs a0) {
+  const DiffArgs a = with_round(a0);
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t L = gw >> 1;
   if (L > a.D + 1u) return;
@@ -165,7 +169,8 @@ __global__ void compact_levels_kernel(DiffArgs a) {
 }
 
 // canonical position of node-order entry i at level L: entries of deeper levels first
-__global__ void compact_permute_kernel(DiffArgs a) {
+__global__ void compact_permute_kernel(DiffArgs a0) {
+  const DiffArgs a = with_round(a0);
   const uint32_t F = a.meta->F, S = a.meta->S;
   const uint64_t tot = (uint64_t)F + S;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < tot; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -183,7 +188,8 @@ __global__ void compact_permute_kernel(DiffArgs a) {
 }
 
 // ---------------------------------------------------------------- region sizes and offsets
-__global__ void __launch_bounds__(COMPACT_THREADS) region_count_kernel(DiffArgs a) {
+__global__ void __launch_bounds__(COMPACT_THREADS) region_count_kernel(DiffArgs a0) {
+  const DiffArgs a = with_round(a0);
   __shared__ uint32_t sh[COMPACT_THREADS / 32 + 1];
   uint64_t beg, end;
   cta_range(a.meta->F, blockIdx.x, gridDim.x, beg, end);
@@ -201,7 +207,8 @@ __global__ void __launch_bounds__(COMPACT_THREADS) region_count_kernel(DiffArgs 
   if (threadIdx.x == 0) a.partial2[blockIdx.x] = t;
 }
 
-__global__ void __launch_bounds__(1024) region_scan_kernel(DiffArgs a, uint32_t g) {
+__global__ void __launch_bounds__(1024) region_scan_kernel(DiffArgs a0, uint32_t g) {
+  const DiffArgs a = with_round(a0);
   __shared__ uint32_t sh[33];
   uint32_t tot;
   const uint32_t i = threadIdx.x;
@@ -211,7 +218,8 @@ __global__ void __launch_bounds__(1024) region_scan_kernel(DiffArgs a, uint32_t 
   if (i == 0) a.meta->T = tot;
 }
 
-__global__ void __launch_bounds__(COMPACT_THREADS) region_write_kernel(DiffArgs a) {
+__global__ void __launch_bounds__(COMPACT_THREADS) region_write_kernel(DiffArgs a0) {
+  const DiffArgs a = with_round(a0);
   __shared__ uint32_t sh[COMPACT_THREADS / 32 + 1];
   uint64_t beg, end;
   cta_range(a.meta->F, blockIdx.x, gridDim.x, beg, end);
@@ -228,7 +236,9 @@ __global__ void __launch_bounds__(COMPACT_THREADS) region_write_kernel(DiffArgs 
 
 // ---------------------------------------------------------------- shifted duplicates
 // source NodeID of each entry (:572-580, :672-674) and per-range histograms by checkpoint
-__global__ void __launch_bounds__(128) shift_prev_kernel(DiffArgs a, uint32_t B) {
+__global__ void __launch_bounds__(128) shift_prev_kernel(DiffArgs a0, uint32_t bcap) {
+  const DiffArgs a = with_round(a0);
+  const uint32_t B = a0.rs->buckets <= bcap ? a0.rs->buckets : bcap;
   extern __shared__ uint32_t hs[];
   uint64_t beg, end;
   cta_range(a.meta->S, blockIdx.x, gridDim.x, beg, end);
@@ -261,7 +271,9 @@ __global__ void __launch_bounds__(128) shift_prev_kernel(DiffArgs a, uint32_t B)
 }
 
 // one CTA: bucket starts, repeat table, per-range scatter bases, header, byte layout
-__global__ void __launch_bounds__(1024) layout_kernel(DiffArgs a, uint32_t B, uint32_t g) {
+__global__ void __launch_bounds__(1024) layout_kernel(DiffArgs a0, uint32_t bcap, uint32_t g) {
+  const DiffArgs a = with_round(a0);
+  const uint32_t B = a0.rs->buckets <= bcap ? a0.rs->buckets : bcap;
   __shared__ uint32_t sh[33];
   __shared__ uint32_t carry_start, carry_rows;
   if (threadIdx.x == 0) { carry_start = 0; carry_rows = 0; }
@@ -346,7 +358,9 @@ __global__ void __launch_bounds__(1024) layout_kernel(DiffArgs a, uint32_t B, ui
 }
 
 // stable scatter of shift entries: one warp walks its range in order
-__global__ void __launch_bounds__(32) shift_write_kernel(DiffArgs a, uint32_t B) {
+__global__ void __launch_bounds__(32) shift_write_kernel(DiffArgs a0, uint32_t bcap) {
+  const DiffArgs a = with_round(a0);
+  const uint32_t B = a0.rs->buckets <= bcap ? a0.rs->buckets : bcap;
   extern __shared__ uint32_t run[];
   uint64_t beg, end;
   cta_range(a.meta->S, blockIdx.x, gridDim.x, beg, end);
@@ -389,7 +403,8 @@ __device__ __forceinline__ uint32_t find_region(const uint32_t* off, uint32_t F,
 // once and then walks forward; LPC lanes copy one chunk with 16-byte vectors (chunk size a
 // multiple of 16, both sides 16-byte aligned); the short last chunk is zero-padded (:643-645).
 template <uint32_t LPC>
-__global__ void __launch_bounds__(256) gather_vec_kernel(DiffArgs a) {
+__global__ void __launch_bounds__(256) gather_vec_kernel(DiffArgs a0) {
+  const DiffArgs a = with_round(a0);
   const DevMeta m = *a.meta;
   uint8_t* dst_base = a.diff + m.data_off;
   uint32_t* first_meta = reinterpret_cast<uint32_t*>(a.diff + m.first_off);
@@ -405,6 +420,36 @@ __global__ void __launch_bounds__(256) gather_vec_kernel(DiffArgs a) {
   if (k0 >= k1) return;
   const uint32_t units = a.cs / 16u;
   uint32_t r = find_region(a.region_off, m.F, k0);
+  if (units == LPC) {
+    // one 16-byte unit per lane per chunk: GATHER_UNROLL chunk groups per iteration, loads
+    // first then stores, so each lane keeps several loads in flight (large diffs, baselines)
+    constexpr uint32_t U = 4;
+    const uint32_t sub = lane % LPC;
+    for (; k0 + (uint64_t)CPW * U <= k1; k0 += (uint64_t)CPW * U) {
+      uint4 val[U];
+      uint4* dst[U];
+      bool full[U];
+      uint32_t rr = r;
+#pragma unroll
+      for (uint32_t u = 0; u < U; u++) {
+        const uint64_t kk = k0 + (uint64_t)u * CPW + lane / LPC;
+        while (rr + 1u < m.F && a.region_off[rr + 1u] <= kk) rr++;
+        const uint64_t chunk = (uint64_t)(leftmost_leaf(a.first_list[rr], a.N) - (a.n - 1u)) + (kk - a.region_off[rr]);
+        full[u] = chunk < a.n - 1u;   // the last chunk (maybe short) goes through the general path
+        dst[u] = reinterpret_cast<uint4*>(dst_base + kk * a.cs) + sub;
+        if (full[u]) val[u] = __ldg(reinterpret_cast<const uint4*>(a.data + chunk * a.cs) + sub);
+      }
+      bool all_full = true;
+#pragma unroll
+      for (uint32_t u = 0; u < U; u++) {
+        if (full[u]) *dst[u] = val[u];
+        all_full = all_full && full[u];
+      }
+      const uint32_t r_next = __reduce_max_sync(0xffffffffu, rr);
+      if (!__all_sync(0xffffffffu, all_full)) break;   // the general loop redoes this group from r
+      r = r_next;
+    }
+  }
   for (uint64_t k = k0; k < k1; k += CPW) {
     const uint64_t kk = k + lane / LPC;
     const uint32_t sub = lane % LPC;
@@ -444,7 +489,8 @@ __global__ void __launch_bounds__(256) gather_vec_kernel(DiffArgs a) {
 }
 
 // any chunk size / alignment: one thread per chunk, byte copies
-__global__ void __launch_bounds__(256) gather_bytes_kernel(DiffArgs a) {
+__global__ void __launch_bounds__(256) gather_bytes_kernel(DiffArgs a0) {
+  const DiffArgs a = with_round(a0);
   const DevMeta m = *a.meta;
   uint8_t* dst_base = a.diff + m.data_off;
   uint8_t* first_meta = a.diff + m.first_off;
@@ -467,9 +513,9 @@ __global__ void __launch_bounds__(256) gather_bytes_kernel(DiffArgs a) {
   }
 }
 
-cudaError_t launch_collect_diff(const DiffArgs& a, int sm_count, cudaStream_t stream) {
+cudaError_t launch_collect_diff(const DiffArgs& a, uint32_t bcap, int sm_count, cudaStream_t stream) {
   const uint32_t g = SCAN_GRID;
-  const uint32_t B = a.cur + 1u;
+  const uint32_t B = bcap;   // capacity; each kernel reads the checkpoint's bucket count from rs
   if (B > MAX_BUCKETS) return cudaErrorInvalidValue;
   compact_count_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);
   compact_scan_kernel<<<1, 1024, 0, stream>>>(a, g);

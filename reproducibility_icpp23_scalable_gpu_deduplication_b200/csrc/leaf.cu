@@ -63,7 +63,8 @@ __device__ __forceinline__ Digest prior_digest(const LeafArgs& a, uint64_t chunk
   return a.baseline ? z : a.tree[a.n - 1u + chunk];
 }
 
-__global__ void leaf_generic_kernel(LeafArgs a, uint32_t c_begin, uint32_t c_end) {
+__global__ void leaf_generic_kernel(LeafArgs a0, uint32_t c_begin, uint32_t c_end) {
+  const LeafArgs a = with_round(a0);
   for (uint64_t c = (uint64_t)c_begin + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < c_end;
        c += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t off = c * a.cs;
@@ -112,6 +113,12 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   *abort_flag = 1;
   return false;
 }
+// a tensor map read from global memory (written there by a copy before this launch)
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(map))
+               : "memory");
+}
+
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1,
                                             int c2) {
   asm volatile(
@@ -130,12 +137,46 @@ __device__ __forceinline__ uint32_t swz(uint32_t o) {
   else return o;
 }
 
+// fold the U-byte segment of row `row` of a staged tile into a lane's running digest state
+template <int U, int KIND>
+__device__ __forceinline__ void hash_segment(const uint8_t* stage, uint32_t row, Murmur3& mm, uint32_t md[4]) {
+  const uint32_t base = row * U;
+  if constexpr (KIND == HASH_MD5) {
+#pragma unroll
+    for (uint32_t blk = 0; blk < U / 64u; blk++) {
+      uint32_t m[16];
+#pragma unroll
+      for (uint32_t j = 0; j < 4; j++) {
+        const uint4 v = *reinterpret_cast<const uint4*>(stage + swz<U>(base + blk * 64u + 16u * j));
+        m[4 * j + 0] = v.x; m[4 * j + 1] = v.y; m[4 * j + 2] = v.z; m[4 * j + 3] = v.w;
+      }
+      md5_compress(md, m);
+    }
+  } else {
+#pragma unroll
+    for (uint32_t j = 0; j < U / 16u; j++) {
+      const uint4 v = *reinterpret_cast<const uint4*>(stage + swz<U>(base + 16u * j));
+      mm.block_words(v.x, v.y, v.z, v.w);
+    }
+  }
+}
+template <int KIND>
+__device__ __forceinline__ Digest finish_segments(Murmur3& mm, uint32_t md[4], uint32_t cs) {
+  if constexpr (KIND == HASH_MD5) {
+    md5_pad_block64(md, cs);
+    return md5_digest(md);
+  } else {
+    return mm.finish(cs);
+  }
+}
+
 // Tile = R = 32 * TMA_CONSUMER_WARPS chunks; stage = one U-byte segment of each chunk of a
 // tile (R x U bytes); a chunk of cs bytes takes S = cs / U stages.
 template <int U, int KIND>
 __global__ void __launch_bounds__((TMA_CONSUMER_WARPS + 1) * 32)
-    leaf_tma_kernel(const __grid_constant__ CUtensorMap tmap, LeafArgs a, uint32_t nfull, uint32_t S,
+    leaf_tma_kernel(const __grid_constant__ CUtensorMap tmap, LeafArgs a0, uint32_t nfull, uint32_t S,
                     uint32_t stages) {
+  const LeafArgs a = with_round(a0);
   constexpr uint32_t R = 32u * TMA_CONSUMER_WARPS;
   constexpr uint32_t STAGE_BYTES = R * U;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -205,39 +246,128 @@ __global__ void __launch_bounds__((TMA_CONSUMER_WARPS + 1) * 32)
       const uint32_t s = k % stages, ph = (k / stages) & 1u;
       if (!mbar_wait_bounded(&full[s], ph, a.st, &abort_flag)) return;
       const uint8_t* stage = smem + (size_t)s * STAGE_BYTES;
-      if (valid) {
-        const uint32_t base = row * U;
-        if constexpr (KIND == HASH_MD5) {
-#pragma unroll
-          for (uint32_t blk = 0; blk < U / 64u; blk++) {
-            uint32_t m[16];
-#pragma unroll
-            for (uint32_t j = 0; j < 4; j++) {
-              const uint4 v = *reinterpret_cast<const uint4*>(stage + swz<U>(base + blk * 64u + 16u * j));
-              m[4 * j + 0] = v.x; m[4 * j + 1] = v.y; m[4 * j + 2] = v.z; m[4 * j + 3] = v.w;
-            }
-            md5_compress(md, m);
-          }
-        } else {
-#pragma unroll
-          for (uint32_t j = 0; j < U / 16u; j++) {
-            const uint4 v = *reinterpret_cast<const uint4*>(stage + swz<U>(base + 16u * j));
-            mm.block_words(v.x, v.y, v.z, v.w);
-          }
-        }
-      }
+      if (valid) hash_segment<U, KIND>(stage, row, mm, md);
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
     }
-    if (valid) {
-      Digest d;
-      if constexpr (KIND == HASH_MD5) {
-        md5_pad_block64(md, a.cs);
-        d = md5_digest(md);
-      } else {
-        d = mm.finish(a.cs);
+    if (valid) leaf_finish(a, chunk, finish_segments<KIND>(mm, md, a.cs), old);
+  }
+}
+
+// Batched form: one persistent launch hashes the chunks of many buffers.  The producer lane
+// pulls work from a global queue of (buffer, tile) items -- `tiles_per_pop` tiles at a time --
+// and passes each stage's owner to the consumers through shared memory next to the ring; a
+// sentinel stage ends the consumers.  Every buffer has its own tensor map, state and round.
+template <int U, int KIND>
+__global__ void __launch_bounds__((TMA_CONSUMER_WARPS + 1) * 32)
+    leaf_tma_batch_kernel(const BatchLeafItem* items, uint32_t nitems, uint32_t total_tiles, uint32_t tiles_per_pop,
+                          unsigned int* queue, uint32_t stages, DevStatus* st) {
+  constexpr uint32_t R = 32u * TMA_CONSUMER_WARPS;
+  constexpr uint32_t STAGE_BYTES = R * U;
+  constexpr uint32_t NO_ITEM = 0xffffffffu;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023u) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)stages * STAGE_BYTES);
+  uint64_t* empty = full + stages;
+  __shared__ uint32_t tbeg[BATCH_MAX_ITEMS + 1];
+  __shared__ uint32_t slot_item[16], slot_tile[16], slot_seg[16];
+  __shared__ int abort_flag;
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  for (uint32_t i = threadIdx.x; i < nitems; i += blockDim.x) tbeg[i] = items[i].tile_begin;
+  if (threadIdx.x == 0) {
+    tbeg[nitems] = total_tiles;
+    abort_flag = 0;
+    for (uint32_t s = 0; s < stages; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], TMA_CONSUMER_WARPS);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+
+  if (warp == TMA_CONSUMER_WARPS) {
+    if (lane == 0) {
+      uint32_t k = 0, last = NO_ITEM;
+      bool ok = true;
+      while (ok) {
+        const uint32_t base = atomicAdd(queue, tiles_per_pop);
+        if (base >= total_tiles) break;
+        const uint32_t stop = base + tiles_per_pop < total_tiles ? base + tiles_per_pop : total_tiles;
+        for (uint32_t tg = base; tg < stop && ok; tg++) {
+          uint32_t lo = 0, hi = nitems;   // item with tbeg[i] <= tg < tbeg[i+1]
+          while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (tbeg[mid] <= tg) lo = mid; else hi = mid;
+          }
+          const uint32_t tile = tg - tbeg[lo];
+          const uint32_t S = items[lo].S;
+          if (lo != last) {
+            tensormap_acquire(&items[lo].map);
+            last = lo;
+          }
+          for (uint32_t g = 0; g < S; g++, k++) {
+            const uint32_t s = k % stages, ph = (k / stages) & 1u;
+            if (k >= stages && !mbar_wait_bounded(&empty[s], ph ^ 1u, st, &abort_flag)) { ok = false; break; }
+            slot_item[s] = lo;
+            slot_tile[s] = tile;
+            slot_seg[s] = g;
+            mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
+            tma_load_3d(smem + (size_t)s * STAGE_BYTES, &items[lo].map, &full[s], 0, (int)g, (int)(tile * R));
+          }
+        }
       }
-      leaf_finish(a, chunk, d, old);
+      const uint32_t issued = k;
+      // wait for this CTA's copies still in flight (before the sentinel reuses a stage's barrier)
+      const uint32_t first = issued > stages ? issued - stages : 0;
+      for (uint32_t q = first; q < issued; q++)
+        mbar_wait_bounded(&full[q % stages], (q / stages) & 1u, st, &abort_flag);
+      if (ok) {   // sentinel: a stage with no data whose owner says "done"
+        const uint32_t s = k % stages, ph = (k / stages) & 1u;
+        if (k < stages || mbar_wait_bounded(&empty[s], ph ^ 1u, st, &abort_flag)) {
+          slot_item[s] = NO_ITEM;
+          mbar_arrive(&full[s]);
+        }
+      }
+      // short last chunks (len not a multiple of cs), one buffer per CTA in turn
+      for (uint32_t i = blockIdx.x; i < nitems; i += gridDim.x) {
+        const LeafArgs a = with_round(items[i].args);
+        for (uint64_t c = items[i].nfull; c < a.n; c++) {
+          const uint64_t off = c * a.cs;
+          const uint64_t nb = (c == a.n - 1u) ? a.len - off : a.cs;
+          leaf_finish(a, (uint32_t)c, hash_bytes(a.kind, a.data + off, nb), prior_digest(a, c));
+        }
+      }
+    }
+    return;
+  }
+
+  const uint32_t row = warp * 32u + lane;
+  Murmur3 mm;
+  uint32_t md[4];
+  Digest old;
+  uint32_t chunk = 0;
+  bool valid = false;
+  for (uint32_t k = 0;; k++) {
+    const uint32_t s = k % stages, ph = (k / stages) & 1u;
+    if (!mbar_wait_bounded(&full[s], ph, st, &abort_flag)) return;
+    const uint32_t it = slot_item[s];
+    if (it == NO_ITEM) break;
+    const uint32_t tile = slot_tile[s], g = slot_seg[s];
+    const uint32_t S = items[it].S;
+    if (g == 0) {   // a new tile: this lane's chunk, its prior digest, fresh digest state
+      chunk = tile * R + row;
+      valid = chunk < items[it].nfull;
+      mm.init();
+      md5_init(md);
+      old.w[0] = old.w[1] = old.w[2] = old.w[3] = 0u;
+      if (valid) old = prior_digest(with_round(items[it].args), chunk);
+    }
+    if (valid) hash_segment<U, KIND>(smem + (size_t)s * STAGE_BYTES, row, mm, md);
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
+    if (g + 1 == S && valid) {
+      const LeafArgs a = with_round(items[it].args);
+      leaf_finish(a, chunk, finish_segments<KIND>(mm, md, a.cs), old);
     }
   }
 }
@@ -297,27 +427,83 @@ static cudaError_t launch_tma(const CUtensorMap& map, const LeafArgs& a, uint32_
   return cudaGetLastError();
 }
 
+static bool encode_map(const LeafArgs& a, int U, CUtensorMap& map) {
+  EncodeTiledFn enc = get_encode_fn();
+  if (!enc) return false;
+  const uint32_t nfull = (uint32_t)(a.len / a.cs);
+  const cuuint64_t S = a.cs / (uint32_t)U;
+  cuuint64_t dims[3] = {(cuuint64_t)U, S, (cuuint64_t)nfull};
+  cuuint64_t strides[2] = {(cuuint64_t)U, (cuuint64_t)a.cs};
+  cuuint32_t box[3] = {(cuuint32_t)U, 1u, 32u * TMA_CONSUMER_WARPS};
+  cuuint32_t estr[3] = {1u, 1u, 1u};
+  CUtensorMapSwizzle sw = U == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
+                        : U == 64  ? CU_TENSOR_MAP_SWIZZLE_64B
+                        : U == 32  ? CU_TENSOR_MAP_SWIZZLE_32B
+                                   : CU_TENSOR_MAP_SWIZZLE_NONE;
+  return enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<uint8_t*>(a.data), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+int batch_leaf_item(const LeafArgs& a, BatchLeafItem& item) {
+  const uint32_t nfull = (uint32_t)(a.len / a.cs);
+  const int U = choose_unit(a.cs, a.kind);
+  if (U == 0 || nfull == 0 || (reinterpret_cast<uintptr_t>(a.data) & 15u) != 0) return 0;
+  if (!encode_map(a, U, item.map)) return 0;
+  item.args = a;
+  item.nfull = nfull;
+  item.S = a.cs / (uint32_t)U;
+  item.ntiles = (nfull + 32u * TMA_CONSUMER_WARPS - 1) / (32u * TMA_CONSUMER_WARPS);
+  return U;
+}
+
+template <int U, int KIND>
+static cudaError_t launch_batch(const BatchLeafItem* d_items, uint32_t nitems, uint32_t total_tiles,
+                                unsigned int* queue, DevStatus* st, int sm_count, const LeafTuning& tune,
+                                uint32_t tiles_per_pop, cudaStream_t stream) {
+  constexpr uint32_t STAGE_BYTES = 32u * TMA_CONSUMER_WARPS * U;
+  uint32_t stages = tune.stages > 0 ? (uint32_t)tune.stages : (64u * 1024u) / STAGE_BYTES;
+  if (stages < 2) stages = 2;
+  if (stages > 16) stages = 16;
+  while (stages > 2 && (size_t)stages * STAGE_BYTES > 200u * 1024u) stages--;
+  const size_t smem = (size_t)stages * STAGE_BYTES + 2 * stages * sizeof(uint64_t) + 1024;
+  auto kern = leaf_tma_batch_kernel<U, KIND>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  uint32_t grid = (uint32_t)sm_count * (uint32_t)(tune.ctas_per_sm > 0 ? tune.ctas_per_sm : 3);
+  if (grid == 0) grid = 1;
+  kern<<<grid, (TMA_CONSUMER_WARPS + 1) * 32, smem, stream>>>(d_items, nitems, total_tiles,
+                                                              tiles_per_pop ? tiles_per_pop : 1u, queue, stages, st);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_leaves_batch(const BatchLeafItem* d_items, uint32_t nitems, uint32_t total_tiles, int U, int kind,
+                                unsigned int* queue, DevStatus* st, int sm_count, const LeafTuning& tune,
+                                uint32_t tiles_per_pop, cudaStream_t stream) {
+  if (nitems == 0 || nitems > BATCH_MAX_ITEMS) return cudaErrorInvalidValue;
+  if (kind == HASH_MD5) {
+    if (U == 128) return launch_batch<128, HASH_MD5>(d_items, nitems, total_tiles, queue, st, sm_count, tune, tiles_per_pop, stream);
+    if (U == 64) return launch_batch<64, HASH_MD5>(d_items, nitems, total_tiles, queue, st, sm_count, tune, tiles_per_pop, stream);
+    return cudaErrorInvalidValue;
+  }
+  switch (U) {
+    case 128: return launch_batch<128, HASH_MURMUR3>(d_items, nitems, total_tiles, queue, st, sm_count, tune, tiles_per_pop, stream);
+    case 64: return launch_batch<64, HASH_MURMUR3>(d_items, nitems, total_tiles, queue, st, sm_count, tune, tiles_per_pop, stream);
+    case 32: return launch_batch<32, HASH_MURMUR3>(d_items, nitems, total_tiles, queue, st, sm_count, tune, tiles_per_pop, stream);
+    case 16: return launch_batch<16, HASH_MURMUR3>(d_items, nitems, total_tiles, queue, st, sm_count, tune, tiles_per_pop, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 // Returns 1 if the staged TMA path was used, 0 for the generic path, negative on error.
 int launch_leaves(const LeafArgs& a, int sm_count, const LeafTuning& tune, cudaStream_t stream) {
   const uint32_t nfull = (uint32_t)(a.len / a.cs);
   const int U = choose_unit(a.cs, a.kind);
   const bool aligned = (reinterpret_cast<uintptr_t>(a.data) & 15u) == 0;
-  EncodeTiledFn enc = get_encode_fn();
-  if (tune.allow_tma && U > 0 && aligned && nfull > 0 && enc != nullptr) {
-    CUtensorMap map;
+  CUtensorMap map;
+  if (tune.allow_tma && U > 0 && aligned && nfull > 0) {
     const cuuint64_t S = a.cs / (uint32_t)U;
-    cuuint64_t dims[3] = {(cuuint64_t)U, S, (cuuint64_t)nfull};
-    cuuint64_t strides[2] = {(cuuint64_t)U, (cuuint64_t)a.cs};
-    cuuint32_t box[3] = {(cuuint32_t)U, 1u, 32u * TMA_CONSUMER_WARPS};
-    cuuint32_t estr[3] = {1u, 1u, 1u};
-    CUtensorMapSwizzle sw = U == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
-                          : U == 64  ? CU_TENSOR_MAP_SWIZZLE_64B
-                          : U == 32  ? CU_TENSOR_MAP_SWIZZLE_32B
-                                     : CU_TENSOR_MAP_SWIZZLE_NONE;
-    CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<uint8_t*>(a.data), dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r == CUDA_SUCCESS) {
+    if (encode_map(a, U, map)) {
       cudaError_t e;
       const uint32_t s32 = (uint32_t)S;
       if (a.kind == HASH_MD5) {

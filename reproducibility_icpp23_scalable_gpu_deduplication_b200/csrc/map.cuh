@@ -37,9 +37,9 @@ constexpr uint32_t MAP_TREE_PENDING = 0xffffffffu;
 
 struct MapView {
   MapSlot* slots;      // cap + 1 slots
-  uint64_t cap;        // power of two
-  uint64_t mask;
+  uint64_t cap;        // any positive count (homes are mapped onto [0, cap) by a multiply)
   unsigned long long* size;   // device counter of occupied slots
+  uint64_t pad;
 };
 
 struct MapRef {
@@ -58,12 +58,14 @@ __device__ __forceinline__ Key128 digest_key(const Digest& d) {
 __device__ __forceinline__ bool key_is_empty_pattern(const Key128& k) {
   return k.lo == MAP_EMPTY && k.hi == MAP_EMPTY;
 }
-__device__ __forceinline__ uint64_t map_home(const Key128& k, uint64_t mask) {
-  // digests are uniformly distributed; fold both halves so a table of any size mixes all bits
+__device__ __forceinline__ uint64_t map_home(const Key128& k, uint64_t cap) {
+  // digests are uniformly distributed; fold both halves, then scale the 64-bit value onto
+  // [0, cap) (high half of the product), which needs no power-of-two capacity
   unsigned long long h = k.lo ^ (k.hi * 0x9E3779B97F4A7C15ull);
   h ^= h >> 31;
-  return (uint64_t)h & mask;
+  return (uint64_t)__umul64hi(h, (unsigned long long)cap);
 }
+__device__ __forceinline__ uint64_t map_next(uint64_t i, uint64_t cap) { return i + 1 == cap ? 0 : i + 1; }
 
 // Find without concurrent inserters on the probed path (all lookups in this library happen
 // either in a later kernel than the inserts, or for keys whose probe path was complete
@@ -74,15 +76,23 @@ __device__ __forceinline__ uint64_t map_find(const MapView& m, const Digest& d) 
     const MapSlot& s = m.slots[m.cap];
     return s.pad ? m.cap : m.cap + 1;
   }
-  uint64_t i = map_home(k, m.mask);
-  for (uint64_t probe = 0; probe <= m.mask; probe++) {
+  uint64_t i = map_home(k, m.cap);
+  for (uint64_t probe = 0; probe < m.cap; probe++) {
     const MapSlot* s = &m.slots[i];
     const unsigned long long lo = s->key_lo, hi = s->key_hi;
     if (lo == k.lo && hi == k.hi) return i;
     if (lo == MAP_EMPTY && hi == MAP_EMPTY) return m.cap + 1;
-    i = (i + 1) & m.mask;
+    i = map_next(i, m.cap);
   }
   return m.cap + 1;
+}
+
+// occupied-slot counter: one atomic per group of lanes that insert together (a single counter
+// takes every insert of a launch, so per-lane atomics would serialise on it)
+__device__ __forceinline__ void count_insert(unsigned long long* size) {
+  const unsigned am = __activemask();
+  const unsigned lane = threadIdx.x & 31u;
+  if (lane == (unsigned)(__ffs(am) - 1)) atomicAdd(size, (unsigned long long)__popc(am));
 }
 
 __device__ __forceinline__ Key128 atomic_cas_key(MapSlot* s, Key128 cmp, Key128 val) {
@@ -105,15 +115,15 @@ __device__ __forceinline__ MapRef map_insert(const MapView& m, const Digest& d, 
     r.inserted = (old == 0u);
     if (r.inserted) {
       atomicExch(&s->tree, cur);
-      atomicAdd(m.size, 1ull);
+      atomicAdd(m.size, 1ull);   // one slot, rare: no aggregation needed
     }
     return r;
   }
   // a key with an all-ones half could be confused with a half-written slot: always CAS
   const bool cas_only = (k.lo == MAP_EMPTY) || (k.hi == MAP_EMPTY);
   const Key128 empty{MAP_EMPTY, MAP_EMPTY};
-  uint64_t i = map_home(k, m.mask);
-  for (uint64_t probe = 0; probe <= m.mask; probe++) {
+  uint64_t i = map_home(k, m.cap);
+  for (uint64_t probe = 0; probe < m.cap; probe++) {
     MapSlot* s = &m.slots[i];
     bool try_cas = true;
     if (!cas_only) {
@@ -132,7 +142,7 @@ __device__ __forceinline__ MapRef map_insert(const MapView& m, const Digest& d, 
       if (old.lo == MAP_EMPTY && old.hi == MAP_EMPTY) {
         r.prev = atomicMin(&s->val, val);
         atomicExch(&s->tree, cur);
-        atomicAdd(m.size, 1ull);
+        count_insert(m.size);
         r.slot = i; r.found = true; r.inserted = true;
         return r;
       }
@@ -141,7 +151,7 @@ __device__ __forceinline__ MapRef map_insert(const MapView& m, const Digest& d, 
         return r;
       }
     }
-    i = (i + 1) & m.mask;
+    i = map_next(i, m.cap);
   }
   set_error(st, DERR_MAP_FULL, 0);
   return r;

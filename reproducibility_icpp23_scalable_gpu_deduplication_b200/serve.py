@@ -1,0 +1,265 @@
+"""Served form: a request loop over many clients' checkpoint requests, with continuous batching.
+
+The reference has no server; its driver checkpoints one buffer per call
+(src/dedup_files.cpp:98-102 -> TreeDeduplicator::checkpoint, src/tree_approach.cpp:1705).  Here
+clients submit "checkpoint my device buffer now" requests as they arrive.  The loop
+
+* keeps each client's Merkle tree and digest map resident on the device between its requests
+  (one ``TreeDeduplicator`` handle per client), so every request after the first is an
+  incremental checkpoint against that client's own previous one;
+* admits a request when its client's state fits in the HBM budget (the handle's device bytes:
+  ``estimate_memory`` before its first checkpoint, ``memory()`` after), evicting the least
+  recently used idle clients when allowed (an evicted client's next request is a baseline);
+* launches every admitted request whose client is idle as one batch (``CheckpointBatch``) as
+  soon as a batch slot is free, while the batches already launched keep running on their own
+  streams: requests that arrive during a batch join the next one (continuous batching), and up
+  to ``max_inflight`` batches overlap on the device;
+* completes a batch when its device work is done and stamps each request's completion time.
+
+A client has at most one request in flight; its later requests wait in arrival order.  Each
+request's diff is exactly what its client's handle gives when it checkpoints the same buffers
+alone, one request at a time.
+
+``plain=True`` serves the same requests the drop-in way instead: one request at a time, in
+arrival order, each through ``TreeDeduplicator.checkpoint_device``.
+"""
+import collections
+import time
+
+from ._lib import HASH_MURMUR3
+from .batch import CheckpointBatch
+from .tree import TreeDeduplicator, estimate_memory
+
+__all__ = ["CheckpointServer", "Request"]
+
+
+class Request:
+    __slots__ = ("client", "buffer", "nbytes", "make_baseline", "arrival", "admitted", "launched", "done", "rc",
+                 "diff_len", "checksum", "ready", "seq")
+
+    def __init__(self, client, buffer, make_baseline, arrival, seq):
+        self.client, self.buffer, self.make_baseline, self.arrival, self.seq = client, buffer, make_baseline, arrival, seq
+        self.nbytes = buffer.numel() * buffer.element_size()
+        self.admitted = self.launched = self.done = None
+        self.rc = None
+        self.diff_len = None
+        self.checksum = None
+        self.ready = None
+
+    @property
+    def latency(self):
+        return None if self.done is None else self.done - self.arrival
+
+
+class _Client:
+    __slots__ = ("handle", "reserved", "last_use", "busy", "pending", "outstanding")
+
+    def __init__(self):
+        self.handle = None
+        self.reserved = 0
+        self.last_use = 0.0
+        self.busy = False                     # a request of this client is in a launched batch
+        self.pending = collections.deque()   # admitted, not launched
+        self.outstanding = 0                 # submitted, not completed
+
+
+class CheckpointServer:
+    def __init__(self, hbm_budget=150e9, chunk_size=128, hash_kind=HASH_MURMUR3, max_batch=64, max_inflight=2,
+                 evict=True, plain=False, checksum=False, clock=time.perf_counter, **batch_params):
+        import torch
+
+        self.budget = int(hbm_budget)
+        self.cs, self.kind = int(chunk_size), int(hash_kind)
+        self.max_batch, self.plain, self.evict, self.checksum = int(max_batch), plain, evict, checksum
+        self.clock = clock
+        self.clients = collections.defaultdict(_Client)
+        self.waiting = collections.deque()       # arrived, not admitted (arrival order)
+        self.resident = 0                        # bytes reserved by resident clients
+        self.peak_resident = 0
+        self.completed = []
+        self.batches = 0
+        self.seq = 0
+        params = {"graph_cache": 256}
+        params.update(batch_params)
+        self.slots = [] if plain else [
+            (CheckpointBatch(**params), torch.cuda.Stream(), []) for _ in range(max(1, int(max_inflight)))]
+
+    # -- client side
+    def submit(self, client, buffer, make_baseline=False, arrival=None):
+        """Queue one checkpoint of `buffer` (a CUDA tensor the client will not touch until the
+        request completes) for `client`.  Work queued on the current stream before this call is
+        ordered before the checkpoint."""
+        import torch
+
+        r = Request(client, buffer, bool(make_baseline), self.clock() if arrival is None else arrival, self.seq)
+        self.seq += 1
+        r.ready = torch.cuda.Event()
+        r.ready.record(torch.cuda.current_stream())
+        self.waiting.append(r)
+        self.clients[client].outstanding += 1
+        return r
+
+    def busy(self, client):
+        """True while a request of `client` is not completed (its buffer must stay unchanged)."""
+        c = self.clients.get(client)
+        return bool(c and c.outstanding)
+
+    def idle(self):
+        return (not self.waiting and not any(c.pending for c in self.clients.values())
+                and not any(reqs for _, _, reqs in self.slots))
+
+    def close(self):
+        for b, _, reqs in self.slots:
+            if reqs:
+                b.wait(check_status=False)
+            b.close()
+        for c in self.clients.values():
+            if c.handle is not None:
+                c.handle.close()
+                c.handle = None
+        self.clients.clear()
+
+    # -- loop
+    def step(self):
+        """One pass of the loop: complete finished batches, admit, launch.  Returns requests completed."""
+        if self.plain:
+            return self._step_plain()
+        done = self._complete()
+        self._admit()
+        self._launch()
+        return done
+
+    def drain(self, poll=0.0):
+        while not self.idle():
+            self.step()
+            if poll:
+                time.sleep(poll)
+
+    # -- internals
+    def _need(self, c, r):
+        if c.handle is not None:
+            return 0
+        return estimate_memory(r.nbytes, self.cs)
+
+    def _evict_for(self, need):
+        idle = [(c.last_use, cid) for cid, c in self.clients.items()
+                if c.handle is not None and not c.busy and not c.pending]
+        idle.sort()
+        for _, cid in idle:
+            if self.resident + need <= self.budget:
+                break
+            c = self.clients[cid]
+            c.handle.close()
+            c.handle = None
+            self.resident -= c.reserved
+            c.reserved = 0
+
+    def _admit(self):
+        keep = collections.deque()
+        blocked = set()
+        while self.waiting:
+            r = self.waiting.popleft()
+            c = self.clients[r.client]
+            if r.client in blocked:
+                keep.append(r)
+                continue
+            need = self._need(c, r)
+            if need and self.resident + need > self.budget and self.evict:
+                self._evict_for(need)
+            if need and self.resident + need > self.budget:
+                keep.append(r)          # waits for memory; later requests of this client wait behind it
+                blocked.add(r.client)
+                continue
+            if c.handle is None:
+                c.handle = TreeDeduplicator(self.cs, self.kind)
+                c.reserved = need
+                self.resident += need
+                self.peak_resident = max(self.peak_resident, self.resident)
+            r.admitted = self.clock()
+            c.pending.append(r)
+        self.waiting = keep
+
+    def _launch(self):
+        for slot in self.slots:
+            b, stream, reqs = slot
+            if reqs:
+                continue
+            heads = sorted((c.pending[0].seq, cid) for cid, c in self.clients.items() if c.pending and not c.busy)
+            if not heads:
+                return
+            batch = [self.clients[cid].pending.popleft() for _, cid in heads[:self.max_batch]]
+            for r in batch:
+                stream.wait_event(r.ready)
+                self.clients[r.client].busy = True
+            now = self.clock()
+            for r in batch:
+                r.launched = now
+            b.launch([self.clients[r.client].handle for r in batch], [r.buffer for r in batch],
+                     [r.make_baseline for r in batch], stream=stream)
+            reqs.extend(batch)
+            self.batches += 1
+
+    def _finish(self, r, rc):
+        c = self.clients[r.client]
+        r.rc = rc
+        if rc == 0:
+            r.diff_len = c.handle.diff_device()[1]
+            if self.checksum:
+                r.checksum = c.handle.diff_checksum()
+            used = c.handle.memory()
+            if used > c.reserved:              # maps grow: keep the reservation honest
+                self.resident += used - c.reserved
+                c.reserved = used
+                self.peak_resident = max(self.peak_resident, self.resident)
+        c.busy = False
+        c.outstanding -= 1
+        c.last_use = r.done
+        r.buffer = None
+        self.completed.append(r)
+
+    def _complete(self):
+        out = []
+        for b, _, reqs in self.slots:
+            if not reqs or not b.done():
+                continue
+            rcs = b.wait(check_status=False)
+            now = self.clock()
+            for r, rc in zip(reqs, rcs):
+                r.done = now
+                self._finish(r, rc)
+                out.append(r)
+            reqs.clear()
+        return out
+
+    def _step_plain(self):
+        self._admit()
+        nxt = None
+        for c in self.clients.values():
+            if c.pending and (nxt is None or c.pending[0].seq < nxt.seq):
+                nxt = c.pending[0]
+        if nxt is None:
+            return []
+        c = self.clients[nxt.client]
+        c.pending.popleft()
+        nxt.launched = self.clock()
+        nxt.ready.synchronize()
+        rc = 0
+        try:
+            c.handle.checkpoint_device(nxt.buffer, nxt.make_baseline)
+        except Exception as e:   # noqa: BLE001 - the status travels with the request
+            rc = getattr(e, "code", -8)
+        nxt.done = self.clock()
+        self._finish(nxt, rc)
+        self.batches += 1
+        return [nxt]
+
+
+def percentile(values, q):
+    """q-th percentile (0..100) by linear interpolation between order statistics."""
+    v = sorted(values)
+    if not v:
+        return None
+    k = (len(v) - 1) * q / 100.0
+    lo = int(k)
+    hi = min(lo + 1, len(v) - 1)
+    return v[lo] + (v[hi] - v[lo]) * (k - lo)

@@ -80,6 +80,15 @@ def words_torch(seed, streams, nwords, device):
     return _mix64_t(keys[:, None] + j[None, :] * _s64(GOLDEN))
 
 
+def words_torch_t(seed, streams, nwords):
+    """words_torch for streams already in a device int64 tensor (bit patterns of the uint64 ids)."""
+    import torch
+
+    keys = _mix64_t(_s64(seed) ^ _mix64_t(streams + _s64(C_STREAM)))
+    j = torch.arange(1, nwords + 1, dtype=torch.int64, device=streams.device)
+    return _mix64_t(keys[:, None] + j[None, :] * _s64(GOLDEN))
+
+
 def chunk_bytes_np(seed, streams, cs):
     w = words_np(seed, streams, (cs + 7) // 8)
     return w.view(np.uint8).reshape(len(streams), -1)[:, :cs]
@@ -268,6 +277,70 @@ def served_sizes(count=64, lo=4 << 20, hi=2 << 30, align=128, seed=SEED):
 def poisson_arrivals(rate_hz, count, seed=SEED):
     rng = plan_rng(seed, 5, 888888, 0)
     return np.cumsum(rng.exponential(1.0 / rate_hz, count))
+
+
+class DeviceSeries:
+    """A device buffer whose checkpoints are edited on the device: only a handful of scalars and run
+    bounds are drawn on the host, so a request loop can advance many clients in real time.
+
+    ckpt 0 is uniform random bytes; each later checkpoint rewrites a fraction of the whole chunks,
+    drawn uniform in `rate`, as runs of 1..`max_run` chunks with fresh bytes, and copies `shift`
+    of the chunks verbatim from other offsets (sources read before the edits).  Deterministic in
+    (seed, client, checkpoint).
+    """
+
+    def __init__(self, nbytes, chunk_size, client, seed=SEED, device="cuda", max_run=512, rate=(0.005, 0.20),
+                 shift=0.01):
+        self.nbytes, self.cs, self.client, self.seed = int(nbytes), int(chunk_size), int(client), seed
+        self.device, self.max_run, self.rate, self.shift = device, int(max_run), rate, shift
+        self.nfull = self.nbytes // self.cs
+        self.ckpt = -1
+        self.data = None
+
+    def next(self):
+        import torch
+
+        self.ckpt += 1
+        dev = self.device
+        if self.ckpt == 0:
+            self.data = torch.empty(self.nbytes, dtype=torch.uint8, device=dev)
+            step = 1 << 24
+            total_words = (self.nbytes + 7) // 8
+            for b in range((total_words + step - 1) // step):
+                w = words_torch(self.seed, [int(_stream_id(3, 0, self.client * 4096 + b))], step, dev)[0]
+                lo = b * step * 8
+                hi = min(self.nbytes, lo + step * 8)
+                self.data[lo:hi] = w.view(torch.uint8)[:hi - lo]
+            return self.data
+        n = self.nfull
+        if n == 0:
+            return self.data
+        view = self.data[:n * self.cs].view(n, self.cs)
+        rng = plan_rng(self.seed, 6, self.client, self.ckpt)
+        rate = rng.uniform(*self.rate)
+        nruns = max(1, round(rate * n / ((1 + self.max_run) / 2)))
+        lens = rng.integers(1, self.max_run + 1, nruns)
+        starts = rng.integers(0, n, nruns)
+        total = int(lens.sum())
+        L = torch.as_tensor(lens, device=dev)
+        S = torch.as_tensor(starts, device=dev)
+        idx = torch.repeat_interleave(S, L, output_size=total)
+        idx += torch.arange(total, device=dev) - torch.repeat_interleave(torch.cumsum(L, 0) - L, L, output_size=total)
+        idx.clamp_(max=n - 1)   # a run past the end rewrites the last chunk (same bytes every time)
+        m = round(self.shift * n) if n > 1 else 0
+        if m:
+            g = torch.Generator(device=dev)
+            g.manual_seed(int(rng.integers(1 << 62)))
+            dst = torch.randperm(n, generator=g, device=dev)[:m]
+            src = torch.randint(0, n - 1, (m,), generator=g, device=dev)
+            src += (src >= dst).to(src.dtype)
+            rows = view[src].clone()
+        streams = idx | ((2 << 56) | (self.ckpt << 40))
+        w = words_torch_t(self.seed + self.client, streams, (self.cs + 7) // 8)
+        view[idx] = w.view(torch.uint8).reshape(total, -1)[:, :self.cs]
+        if m:
+            view[dst] = rows
+        return self.data
 
 
 # ----------------------------------------------------------------------------- float32 / MD5

@@ -199,6 +199,32 @@ class TreeDeduplicator:
         check(lib().b2d_last_launch_count(self._h, ctypes.byref(v)), "b2d_last_launch_count")
         return v.value
 
+    def memory(self):
+        """Device bytes this handle holds."""
+        v = ctypes.c_uint64()
+        check(lib().b2d_memory(self._h, ctypes.byref(v)), "b2d_memory")
+        return v.value
+
+    def map_stats(self):
+        """(slots, entries, growths, seconds spent growing, of which allocating) of the digest map."""
+        a = (ctypes.c_double * 5)()
+        check(lib().b2d_map_stats(self._h, a), "b2d_map_stats")
+        return int(a[0]), int(a[1]), int(a[2]), a[3], a[4]
+
+    def diff_checksum(self, block=4096):
+        """MD5 (hex) of the Murmur3 digests of the device diff's `block`-byte blocks: a cheap identity
+        check of a large diff without copying it to the host."""
+        import hashlib
+
+        import torch
+
+        p, n = self.diff_device()
+        nblk = (n + block - 1) // block
+        out = torch.empty((nblk, 16), dtype=torch.uint8, device="cuda")
+        check(lib().b2d_hash_chunks(HASH_MURMUR3, ctypes.c_void_p(p), n, int(block), ctypes.c_void_p(out.data_ptr()),
+                                    _stream_handle()), "b2d_hash_chunks")
+        return hashlib.md5(out.cpu().numpy().tobytes() + n.to_bytes(8, "little")).hexdigest()
+
     def debug_tree(self, nodes):
         out = np.empty((nodes, 16), np.uint8)
         check(lib().b2d_debug_tree(self._h, ctypes.c_void_p(out.ctypes.data), nodes), "b2d_debug_tree")
@@ -208,6 +234,14 @@ class TreeDeduplicator:
         out = np.empty(leaves, np.uint8)
         check(lib().b2d_debug_labels(self._h, ctypes.c_void_p(out.ctypes.data), leaves), "b2d_debug_labels")
         return out
+
+
+def estimate_memory(nbytes, chunk_size, map_max_load_pct=0):
+    """Device bytes a handle will hold for checkpoints of an `nbytes` buffer."""
+    v = ctypes.c_uint64()
+    check(lib().b2d_estimate_memory(int(nbytes), int(chunk_size), int(map_max_load_pct), ctypes.byref(v)),
+          "b2d_estimate_memory")
+    return v.value
 
 
 def hash_chunks(data, chunk_size, hash_kind=HASH_MURMUR3):

@@ -1,0 +1,122 @@
+"""Served form: every request's diff is the same alone and in the mix.
+
+Clients' requests go through the continuous-batching loop (several batches in flight, requests
+joining whichever batch launches next) and, separately, through one handle per client that
+checkpoints the same buffers one at a time.  Diff checksums must be identical request by request.
+"""
+import pytest
+
+from reproducibility_icpp23_scalable_gpu_deduplication_b200 import TreeDeduplicator, synth
+from reproducibility_icpp23_scalable_gpu_deduplication_b200.serve import CheckpointServer, percentile
+from reproducibility_icpp23_scalable_gpu_deduplication_b200.tree import estimate_memory, parse_header
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [1 << 20, (3 << 20) + 77, 200, 5 << 20, 64 << 10, (2 << 20) + 4096]
+
+
+def drive(server, sizes, rounds, order_seed=1):
+    """Submit `rounds` requests per client in a shuffled interleaving, stepping the loop between."""
+    import numpy as np
+
+    series = [synth.DeviceSeries(n, 128, c, max_run=64) for c, n in enumerate(sizes)]
+    order = [c for c in range(len(sizes)) for _ in range(rounds)]
+    np.random.default_rng(order_seed).shuffle(order)
+    reqs = {}
+    count = [0] * len(sizes)
+    for i, c in enumerate(order):
+        while server.busy(c):
+            server.step()
+        buf = series[c].next()
+        reqs[(c, count[c])] = server.submit(c, buf)
+        count[c] += 1
+        if i % 3 == 2:          # requests arrive in small bursts: several join one batch
+            server.step()
+    server.drain()
+    return reqs
+
+
+def alone(sizes, rounds):
+    out = {}
+    for c, n in enumerate(sizes):
+        s = synth.DeviceSeries(n, 128, c, max_run=64)
+        h = TreeDeduplicator(128)
+        for k in range(rounds):
+            h.checkpoint_device(s.next(), k == 0)
+            out[(c, k)] = h.diff_checksum()
+        h.close()
+    return out
+
+
+def test_served_same_alone_and_in_mix(cuda):
+    rounds = 4
+    srv = CheckpointServer(hbm_budget=8e9, max_batch=4, max_inflight=2, checksum=True)
+    reqs = drive(srv, SIZES, rounds)
+    assert all(r.rc == 0 for r in reqs.values())
+    assert srv.batches < len(reqs)          # some requests shared a batch
+    lat = [r.latency for r in reqs.values()]
+    assert percentile(lat, 50) > 0 and percentile(lat, 99) >= percentile(lat, 50)
+    want = alone(SIZES, rounds)
+    for key, r in reqs.items():
+        assert r.checksum == want[key], key
+    srv.close()
+
+
+def test_served_plain_mode_same(cuda):
+    rounds = 3
+    srv = CheckpointServer(hbm_budget=8e9, plain=True, checksum=True)
+    reqs = drive(srv, SIZES, rounds, order_seed=2)
+    want = alone(SIZES, rounds)
+    for key, r in reqs.items():
+        assert r.rc == 0 and r.checksum == want[key], key
+    srv.close()
+
+
+def test_served_admission_budget(cuda):
+    """a budget that holds two clients' state: the loop never exceeds it, evicts idle clients,
+    and an evicted client's next request is a baseline"""
+    sizes = [2 << 20] * 4
+    budget = int(estimate_memory(2 << 20, 128) * 2.5)
+    srv = CheckpointServer(hbm_budget=budget, max_batch=4, max_inflight=2, checksum=True)
+    reqs = drive(srv, sizes, 3, order_seed=3)
+    assert all(r.rc == 0 for r in reqs.values())
+    assert srv.peak_resident <= budget
+    assert sum(1 for c in srv.clients.values() if c.handle is not None) <= 2
+    srv.close()
+
+
+def test_served_waits_without_eviction(cuda):
+    """without eviction, a client that does not fit waits until the budget allows it (here: never
+    while the others stay resident), and the loop reports it as not admitted"""
+    import torch
+
+    size = 1 << 20
+    budget = int(estimate_memory(size, 128) * 1.5)
+    srv = CheckpointServer(hbm_budget=budget, evict=False)
+    a = torch.zeros(size, dtype=torch.uint8, device="cuda")
+    b = torch.ones(size, dtype=torch.uint8, device="cuda")
+    r0 = srv.submit(0, a)
+    r1 = srv.submit(1, b)
+    for _ in range(50):
+        srv.step()
+        if r0.done is not None:
+            break
+    while r0.done is None:
+        srv.step()
+    srv.step()
+    assert r0.rc == 0 and r1.admitted is None and r1.done is None
+    srv.close()
+
+
+def test_served_diff_header(cuda):
+    """first request of a client is its baseline, later ones reference it"""
+    import numpy as np
+
+    srv = CheckpointServer(hbm_budget=8e9)
+    reqs = drive(srv, SIZES[:2], 2)
+    for c in range(2):
+        h = srv.clients[c].handle
+        hdr = parse_header(np.frombuffer(bytes(h.copy_diff()), np.uint8))
+        assert hdr["chkpt_id"] == 1 and hdr["ref_id"] == 0
+    assert all(r.rc == 0 for r in reqs.values())
+    srv.close()
