@@ -21,6 +21,7 @@ Multi-GPU (torchrun): every rank deduplicates its own buffer (independent replic
 reference's MPI driver); nothing crosses ranks but the barrier and the max-time reduction.
 """
 import argparse
+import collections
 import json
 import os
 import statistics
@@ -42,8 +43,10 @@ def parse():
     p.add_argument("--steps", type=int, default=16)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--chunk-size", type=int, default=128)
-    p.add_argument("--nbytes", type=int, default=4 << 30)
+    p.add_argument("--workload", default="plain_4g", choices=["plain_4g", "md5_f32_8g"],
+                   help="plain form: the 4 GiB Murmur3 series (default) or the 8 GiB float32 MD5 series")
+    p.add_argument("--chunk-size", type=int, default=None, help="default 128 (plain_4g) / 256 (md5_f32_8g)")
+    p.add_argument("--nbytes", type=int, default=None, help="default 4 GiB (plain_4g) / 8 GiB (md5_f32_8g)")
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--cpu-sample-bytes", type=int, default=512 << 20)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -55,11 +58,21 @@ def parse():
     p.add_argument("--buffers", type=int, default=256, help="batched form: number of buffers")
     p.add_argument("--max-buffer", type=int, default=512 << 20, help="batched form: largest buffer size")
     p.add_argument("--no-autotune", action="store_true")
+    p.add_argument("--no-graph", action="store_true", help="plain form: launch kernels one by one, no CUDA graph")
     p.add_argument("--clients", type=int, default=64, help="served form: clients")
     p.add_argument("--requests", type=int, default=1000, help="served form: requests in the stream")
     p.add_argument("--rate", type=float, default=200.0, help="served form: aggregate arrivals per second")
+    p.add_argument("--client-max-buffer", type=int, default=2 << 30, help="served form: largest client buffer")
+    p.add_argument("--map-reserve", type=float, default=20e9,
+                   help="served form: device bytes kept mapped for digest-map growth")
     p.add_argument("--hbm-budget", type=float, default=150e9, help="served form: device bytes for client state")
-    return p.parse_args()
+    a = p.parse_args()
+    md5 = a.workload == "md5_f32_8g"
+    if a.chunk_size is None:
+        a.chunk_size = 256 if md5 else 128
+    if a.nbytes is None:
+        a.nbytes = (8 << 30) if md5 else (4 << 30)
+    return a
 
 
 def measured_peak():
@@ -123,13 +136,21 @@ class ClockSampler:
                 "reasons": sorted(self.reasons - {"gpu_idle"}), "samples": len(self.samples)}
 
 
-def cpu_baseline_run(nbytes, cs, steps, threads):
+def workload_series(workload, nbytes, cs, device, seed):
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import synth
+
+    if workload == "md5_f32_8g":
+        return synth.FloatSeries(nbytes=nbytes, device=device, seed=seed)
+    return synth.plain_4g(nbytes=nbytes, chunk_size=cs, device=device, seed=seed)
+
+
+def cpu_baseline_run(nbytes, cs, steps, threads, workload="plain_4g"):
     """The oracle (sequential restatement of the reference) on the host, all threads hashing."""
     from oracle import oracle as O
     from reproducibility_icpp23_scalable_gpu_deduplication_b200 import synth
 
-    s = synth.plain_4g(nbytes=nbytes, chunk_size=cs)
-    o = O.OracleTreeDeduplicator(cs, O.HASH_MURMUR3, threads=threads)
+    s = workload_series(workload, nbytes, cs, None, synth.SEED)
+    o = O.OracleTreeDeduplicator(cs, O.HASH_MD5 if workload == "md5_f32_8g" else O.HASH_MURMUR3, threads=threads)
     o.checkpoint(s.next(), True)
     t = 0.0
     for _ in range(steps):
@@ -157,15 +178,15 @@ def run_reference(args, rank):
         return
     threads = os.cpu_count() or 1
     steps = max(1, args.steps)
-    gbps, t = cpu_baseline_run(args.cpu_sample_bytes, args.chunk_size, steps, threads)
-    sample = (f"{args.cpu_sample_bytes >> 20} MiB buffer with the 4 GiB workload's change pattern, chunk "
-              f"{args.chunk_size} B, {steps} incremental checkpoints after an untimed baseline")
+    gbps, t = cpu_baseline_run(args.cpu_sample_bytes, args.chunk_size, steps, threads, args.workload)
+    sample = (f"{args.cpu_sample_bytes >> 20} MiB buffer with the {args.workload} workload's change pattern, "
+              f"chunk {args.chunk_size} B, {steps} incremental checkpoints after an untimed baseline")
     line = {
         "impl": "reference", "metric": "tree-dedup ingest GB/s", "value": round(gbps, 4), "unit": "GB/s",
         "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "ms_per_step": round(1e3 * t / steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-        "config": {"workload": "plain_4g", "nbytes": args.nbytes, "chunk_size": args.chunk_size,
-                   "hash": "murmur3"},
+        "config": {"workload": args.workload, "nbytes": args.nbytes, "chunk_size": args.chunk_size,
+                   "hash": "md5" if args.workload == "md5_f32_8g" else "murmur3"},
         "cpu_baseline": {"value": round(gbps, 4), "unit": "GB/s", "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": round(gbps, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -307,22 +328,66 @@ def serve_stream(server_kw, sizes, clients, arrivals, dev, warm_rounds=2):
     torch.cuda.synchronize()
     srv.completed.clear()
     clock = srv.clock
-    t0 = clock()
-    reqs = []
+    # clients act independently: a client submits its next request once it is due and its
+    # previous one has completed (its buffer is free to edit); nobody waits for another client
+    due = [collections.deque() for _ in sizes]
     for c, a in zip(clients, arrivals):
-        t_arr = t0 + a
-        while clock() < t_arr:
-            srv.step()
-        while srv.busy(c):
-            srv.step()
-        reqs.append(srv.submit(int(c), series[c].next(), arrival=t_arr))
+        due[int(c)].append(float(a))
+    active = {c for c in range(len(sizes)) if due[c]}
+    reqs, submitted = [], []
+    t0 = clock()
+    while active:
+        now = clock() - t0
+        for c in sorted(active, key=lambda c: due[c][0]):
+            if due[c][0] <= now and not srv.busy(c):
+                a = due[c].popleft()
+                buf = series[c].next()
+                submitted.append(clock())
+                reqs.append(srv.submit(c, buf, arrival=t0 + a))
+                if not due[c]:
+                    active.discard(c)
+        srv.step()
     srv.drain()
     wall = max(r.done for r in reqs) - t0
     batches = srv.batches
+    service = [r.done - t for r, t in zip(reqs, submitted)]
     srv.close()
     del series
     torch.cuda.empty_cache()
-    return reqs, wall, batches
+    return reqs, wall, batches, service
+
+
+def serve_capacity(server_kw, sizes, waves, dev, warm_rounds=2):
+    """Saturation: every client's next buffer is edited and resident, then all clients submit at
+    once and the loop drains them; repeated `waves` times.  Returns (requests, busy seconds,
+    batches, service times)."""
+    import torch
+
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import synth
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200.serve import CheckpointServer
+
+    series = [synth.DeviceSeries(n, 128, c, device=dev) for c, n in enumerate(sizes)]
+    srv = CheckpointServer(**server_kw)
+    for _ in range(warm_rounds):
+        for c in range(len(sizes)):
+            srv.submit(c, series[c].next())
+        srv.drain()
+    reqs, service, busy = [], [], 0.0
+    b0 = srv.batches
+    for _ in range(waves):
+        bufs = [s.next() for s in series]
+        torch.cuda.synchronize()
+        t = srv.clock()
+        wave = [srv.submit(c, bufs[c], arrival=t) for c in range(len(sizes))]
+        srv.drain()
+        busy += max(r.done for r in wave) - t
+        reqs += wave
+        service += [r.done - t for r in wave]
+    batches = srv.batches - b0
+    srv.close()
+    del series, bufs
+    torch.cuda.empty_cache()
+    return reqs, busy, batches, service
 
 
 def run_served(args, rank, world, dev):
@@ -330,29 +395,30 @@ def run_served(args, rank, world, dev):
     from reproducibility_icpp23_scalable_gpu_deduplication_b200 import synth
     from reproducibility_icpp23_scalable_gpu_deduplication_b200.serve import percentile
 
-    sizes = synth.served_sizes(count=args.clients, hi=args.max_buffer if args.max_buffer != (512 << 20) else 2 << 30)
+    sizes = synth.served_sizes(count=args.clients, hi=args.client_max_buffer)
     rng = np.random.default_rng(synth.SEED + rank)
     n = args.requests
     clients = rng.integers(0, len(sizes), n)
     arrivals = synth.poisson_arrivals(args.rate, n, seed=synth.SEED + rank)
     budget = args.hbm_budget
-    kw = {"hbm_budget": budget, "max_batch": 64, "max_inflight": 2}
+    kw = {"hbm_budget": budget, "max_batch": 64, "max_inflight": 2, "map_reserve": args.map_reserve}
 
-    def summarize(reqs, wall, batches):
+    def summarize(reqs, wall, batches, service):
         lat = [1e3 * r.latency for r in reqs]
+        svc = [1e3 * v for v in service]
         byt = sum(r.nbytes for r in reqs)
         return {"value": round(byt / wall / GB, 2), "unit": "GB/s", "p50_ms": round(percentile(lat, 50), 3),
-                "p99_ms": round(percentile(lat, 99), 3), "max_ms": round(max(lat), 3), "requests": len(reqs),
-                "batches": batches, "failed": sum(1 for r in reqs if r.rc != 0), "wall_s": round(wall, 3)}
+                "p99_ms": round(percentile(lat, 99), 3), "max_ms": round(max(lat), 3),
+                "service_p50_ms": round(percentile(svc, 50), 3), "service_p99_ms": round(percentile(svc, 99), 3),
+                "requests": len(reqs), "batches": batches, "failed": sum(1 for r in reqs if r.rc != 0),
+                "wall_s": round(wall, 3)}
 
     with ClockSampler(int(dev.index or 0)) as clk:
         served = summarize(*serve_stream(kw, sizes, clients, arrivals, dev))
         plain = summarize(*serve_stream(dict(kw, plain=True), sizes, clients, arrivals, dev))
-        # capacity: the same clients with every request already waiting (arrival rate unbounded)
-        m = min(n, 4 * len(sizes))
-        burst = np.zeros(m)
-        cap_served = summarize(*serve_stream(kw, sizes, clients[:m], burst, dev))
-        cap_plain = summarize(*serve_stream(dict(kw, plain=True), sizes, clients[:m], burst, dev))
+        # capacity: all clients' requests waiting at once (unbounded arrival rate), 4 waves
+        cap_served = summarize(*serve_capacity(kw, sizes, 4, dev))
+        cap_plain = summarize(*serve_capacity(dict(kw, plain=True), sizes, 4, dev))
     line = {
         "metric": "tree-dedup served GB/s", "value": served["value"], "unit": "GB/s", "n_gpus": world,
         "steps": n, "warmup": 2, "ms_per_step": served["p50_ms"], "higher_is_better": True, "scaling": "weak",
@@ -361,11 +427,13 @@ def run_served(args, rank, world, dev):
                    "requests": n, "client_bytes_total": sum(sizes), "min_buffer": min(sizes),
                    "max_buffer": max(sizes), "chunk_size": 128, "hash": "murmur3", "hbm_budget": budget,
                    "change": "uniform [0.5%, 20%] in runs of 1-512 chunks + 1% shifted, edited on the device",
-                   "latency": "scheduled arrival -> diff ready on the device (includes the client's edit "
-                              "of its buffer queued at arrival)"},
+                   "latency": "scheduled arrival -> diff ready on the device (includes the client's wait "
+                              "for its own previous request and its device-side edit of its buffer); "
+                              "service_*: submission -> diff ready"},
         "latency_ms": {"p50": served["p50_ms"], "p99": served["p99_ms"], "max": served["max_ms"]},
         "served": served, "plain_same_stream": plain,
-        "capacity": {"served": cap_served, "plain": cap_plain,
+        "capacity": {"mode": "all 64 clients submit at once, buffers edited and resident; 4 waves",
+                     "served": cap_served, "plain": cap_plain,
                      "speedup_vs_plain": round(cap_served["value"] / cap_plain["value"], 3)},
         "e2e": None, "clocks": clk.summary(),
     }
@@ -402,7 +470,7 @@ def main():
     import torch
     import torch.distributed as dist
 
-    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import TreeDeduplicator, synth
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import HASH_MD5, HASH_MURMUR3, TreeDeduplicator, synth
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -414,12 +482,15 @@ def main():
     nbytes = args.nbytes
     n_chunks = (nbytes + cs - 1) // cs
 
-    series = synth.plain_4g(nbytes=nbytes, chunk_size=cs, device=dev, seed=synth.SEED + rank)
-    dd = TreeDeduplicator(cs)
+    md5 = args.workload == "md5_f32_8g"
+    series = workload_series(args.workload, nbytes, cs, dev, synth.SEED + rank)
+    dd = TreeDeduplicator(cs, HASH_MD5 if md5 else HASH_MURMUR3)
     if args.leaf_stages:
         dd.set_param("leaf_stages", args.leaf_stages)
     if args.leaf_ctas:
         dd.set_param("leaf_ctas_per_sm", args.leaf_ctas)
+    if args.no_graph:
+        dd.set_param("graph", 0)
     dd.checkpoint_device(series.next(), make_baseline=True)          # checkpoint 0: baseline
     for _ in range(args.warmup):
         dd.checkpoint_device(series.next())
@@ -491,7 +562,7 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic (seeded; reference datasets unavailable)",
-        "config": {"workload": "plain_4g", "nbytes": nbytes, "chunk_size": cs, "hash": "murmur3",
+        "config": {"workload": args.workload, "nbytes": nbytes, "chunk_size": cs, "hash": "md5" if md5 else "murmur3",
                    "checkpoints": 1 + args.warmup + args.steps, "l2": "inputs 4 GiB > L2, no flush",
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": round(e2e_value, 2) if e2e_value else None, "unit": "GB/s", "h2d_bytes_per_step": nbytes,
@@ -505,7 +576,7 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        gbps, _ = cpu_baseline_run(args.cpu_sample_bytes, cs, 2, threads)
+        gbps, _ = cpu_baseline_run(args.cpu_sample_bytes, cs, 2, threads, args.workload)
         line["cpu_baseline"] = {"value": round(gbps, 4), "unit": "GB/s", "cores": threads, "kind": "port",
                                 "sample": f"{args.cpu_sample_bytes >> 20} MiB buffer with this workload's change "
                                           f"pattern, 2 incremental checkpoints after a baseline"}

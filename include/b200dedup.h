@@ -69,8 +69,10 @@ int b2d_set_stream(b2d_dedup* d, void* cuda_stream);
  *   "leaf_ctas_per_sm"  resident hashing CTAs per SM, 1..8 (0 = default 3)
  *   "map_max_load_pct"  digest-map load limit, 10..90 (default 75): a checkpoint starts only
  *                       when the map's entries plus every node of the tree fit under it
- *   "map_headroom_pct"  size of a baseline's map over that minimum, 100..1000 (default 125);
- *                       more headroom = fewer growths (allocate + rehash) in a long series */
+ *   "map_headroom_pct"  size of a baseline's map over that minimum, 100..1000 (default 200);
+ *                       more headroom = fewer growths (allocate + rehash) in a long series
+ *   "graph"             1 = replay a checkpoint's launches as one CUDA graph (default), 0 = launch
+ *                       them one by one on the handle's stream */
 int b2d_set_param(b2d_dedup* d, const char* name, int64_t value);
 
 /* checkpoint(header_t&, uint8_t* data_ptr, size_t len, HostMirror& diff_h, bool make_baseline)
@@ -156,6 +158,12 @@ int b2d_debug_labels(b2d_dedup* d, void* dst, uint64_t leaves);
 int b2d_hash_chunks(int hash_kind, const void* d_data, uint64_t len, uint32_t chunk_size, void* d_out,
                     void* cuda_stream);
 
+/* Keep `bytes` of device memory mapped for digest maps on the current device (0 = release
+ * it).  Growing a map allocates a larger table; allocating memory the driver has not mapped
+ * yet costs tens of ms per GB, which a long-running caller (a checkpoint server with a memory
+ * budget) pays once here instead of inside a later checkpoint.  Maps are carved out of this
+ * memory while it lasts.  No reference counterpart. */
+int b2d_pool_reserve(uint64_t bytes);
 /* Device bytes a handle holds now (its tree, map, scratch and diff buffers), and the bytes a
  * handle will hold for checkpoints of a `len`-byte buffer (map_max_load_pct 0 = the default
  * 75), for admission against a memory budget.  No reference counterpart. */

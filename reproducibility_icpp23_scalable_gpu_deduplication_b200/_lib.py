@@ -48,6 +48,7 @@ SIGNATURES = [
     ("b2d_debug_tree", _int, [_vp, _vp, _u64]),
     ("b2d_debug_labels", _int, [_vp, _vp, _u64]),
     ("b2d_hash_chunks", _int, [_int, _vp, _u64, _u32, _vp, _vp]),
+    ("b2d_pool_reserve", _int, [_u64]),
     ("b2d_memory", _int, [_vp, ctypes.POINTER(_u64)]),
     ("b2d_map_stats", _int, [_vp, ctypes.POINTER(ctypes.c_double)]),
     ("b2d_estimate_memory", _int, [_u64, _u32, _int, ctypes.POINTER(_u64)]),

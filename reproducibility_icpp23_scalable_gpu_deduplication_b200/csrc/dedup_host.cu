@@ -132,6 +132,11 @@ struct DevState {
 
 using namespace b2d;
 
+// default size of a baseline's digest map over its minimum, and the factor a growing map
+// takes over its new minimum
+constexpr double MAP_HEADROOM = 2.0;
+constexpr double MAP_GROWTH = 2.0;
+
 struct b2d_dedup {
   // BaseDeduplicator state (include/deduplicator_interface.hpp:16-23)
   uint32_t chunk_size = 0;
@@ -151,7 +156,8 @@ struct b2d_dedup {
   bool have_tree = false;
   LeafTuning tune;
   double map_max_load = 0.75;
-  double map_headroom = 1.25;     // baseline table size over its minimum (entries + N at max load)
+  bool use_graph = true;          // replay each checkpoint's launches as one CUDA graph
+  double map_headroom = MAP_HEADROOM;   // baseline table size over its minimum (entries + N at max load)
 
   cudaStream_t own_stream = nullptr;
   cudaStream_t cap_stream = nullptr;   // graph capture only
@@ -202,6 +208,9 @@ namespace {
 // growth instead of returning it to the driver, and its frees are stream-ordered, so growing
 // a map neither waits for the whole device nor maps fresh pages each time.  Unused memory
 // goes back to the driver when a handle is destroyed.
+std::mutex g_pool_mu;
+std::vector<uint64_t> g_pool_keep;   // bytes each device's pool keeps mapped (b2d_pool_reserve)
+
 cudaMemPool_t map_pool(int device) {
   static std::mutex mu;
   static std::vector<cudaMemPool_t> pools;
@@ -231,7 +240,10 @@ b2d_dedup::~b2d_dedup() {
       cudaStream_t s = own_stream ? own_stream : stream;
       cudaFreeAsync(map_slots, s);
       cudaStreamSynchronize(s);
-      if (cudaMemPool_t p = map_pool(device)) cudaMemPoolTrimTo(p, 0);
+      if (cudaMemPool_t p = map_pool(device)) {
+        std::lock_guard<std::mutex> lock(g_pool_mu);
+        cudaMemPoolTrimTo(p, device < (int)g_pool_keep.size() ? g_pool_keep[device] : 0);
+      }
     }
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     for (auto& e : ev)
@@ -242,6 +254,16 @@ b2d_dedup::~b2d_dedup() {
 }
 
 namespace {
+
+// A timing event inside a stream capture must be an external record node (a plain record only
+// joins streams there); outside a capture it is an ordinary record.
+cudaError_t record_timing(cudaEvent_t ev, cudaStream_t s) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaError_t e = cudaStreamIsCapturing(s, &cs);
+  if (e != cudaSuccess) return e;
+  return cs == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(ev, s, cudaEventRecordExternal)
+                                             : cudaEventRecord(ev, s);
+}
 
 // events that were never recorded (a failed launch) read as 0 and leave no error behind for
 // the next call's launch checks
@@ -315,10 +337,10 @@ int map_reset(b2d_dedup* d, uint64_t cap) {
 // Capacity policy.  The reference rehashes when capacity < size + num_nodes
 // (src/tree_approach.cpp:1622-1623): room for every node of the next checkpoint to be new.
 // Here that room must fit under the load limit map_max_load (default 0.75), so no checkpoint
-// can push the table past it: a new table holds its entries plus N at that load, with
-// map_headroom (default 25%) extra at a baseline and 50% when it grows.  Growing allocates and
-// rehashes, so a series whose digests keep changing grows less often with more headroom.
-// Capacities are multiples of 1024, not powers of two.
+// can push the table past it: a new table holds its entries plus N at that load, times
+// map_headroom (default 2) at a baseline and MAP_GROWTH when it grows.  Growing allocates and
+// rehashes (allocation dominates: tens of ms per GB), so a series whose digests keep changing
+// grows less often with more headroom.  Capacities are multiples of 1024, not powers of two.
 uint64_t map_capacity(uint64_t need, double max_load, double headroom) {
   const uint64_t c = (uint64_t)((double)need * headroom / max_load) + 1;
   return (c + 1023) / 1024 * 1024;
@@ -327,7 +349,7 @@ uint64_t map_capacity(uint64_t need, double max_load, double headroom) {
 int map_ensure(b2d_dedup* d) {
   const uint64_t need = d->map_size_host + d->N;
   if (d->map_slots && (double)need <= d->map_max_load * (double)d->map_cap) return B2D_OK;
-  const uint64_t cap = map_capacity(need, d->map_max_load, 1.5);
+  const uint64_t cap = map_capacity(need, d->map_max_load, MAP_GROWTH);
   if (!d->map_slots || d->map_size_host == 0) return map_reset(d, cap);
   const auto t0 = std::chrono::high_resolution_clock::now();
   MapSlot* fresh = nullptr;
@@ -476,9 +498,7 @@ int enqueue_checkpoint(b2d_dedup* d, cudaStream_t s, RoundState* rs_dev, bool up
     B2D_CU(cudaMemsetAsync(ds, 0, sizeof(DevState), s));
     if (upload) B2D_CU(cudaMemcpyAsync(rs_dev, d->round_h.p, sizeof(RoundState), cudaMemcpyHostToDevice, s));
   }
-  // inside a capture a plain event record only joins streams; External makes it a graph node
-  // that records the event on every replay
-  if (timing) B2D_CU(cudaEventRecordWithFlags(d->ev[0], s, cudaEventRecordExternal));
+  if (timing) B2D_CU(record_timing(d->ev[0], s));
   // dedup_data_baseline (:13-259) / dedup_data (:261-509)
   if (!skip_leaves) {
     const LeafArgs la = leaf_args(d, rs_dev);
@@ -486,20 +506,20 @@ int enqueue_checkpoint(b2d_dedup* d, cudaStream_t s, RoundState* rs_dev, bool up
     if (leaf_path < 0) return B2D_ERR_CUDA;
     d->leaf_tma = leaf_path == 1;
   }
-  if (timing) B2D_CU(cudaEventRecordWithFlags(d->ev[3], s, cudaEventRecordExternal));
+  if (timing) B2D_CU(record_timing(d->ev[3], s));
   ForestArgs fa{d->tree.p, d->lab.p, d->leaflab.p, d->push.p, m, &ds->status, &ds->zero_exists, d->dupflag.p,
                 d->n, d->N, d->D, 0, d->kind, 0, rs_dev};
   B2D_CU(launch_forest(fa, 1, s));
   B2D_CU(launch_zero_exists(&ds->zero_exists, rs_dev, s));
   B2D_CU(launch_forest(fa, 2, s));
-  if (timing) B2D_CU(cudaEventRecordWithFlags(d->ev[1], s, cudaEventRecordExternal));
+  if (timing) B2D_CU(record_timing(d->ev[1], s));
   // collect_diff (:511-710)
   DiffArgs ga{static_cast<const uint8_t*>(d->data), d->data_len, d->chunk_size, d->n, d->N, d->D, 0, 0,
               d->tree.p, d->push.p, m, &ds->status, &ds->meta, d->first_list.p, d->shift_list.p, d->tmp_first.p,
               d->tmp_shift.p, d->levels.p, d->region_off.p, d->sprev.p, d->skey.p, d->hist.p, d->bucket_start.p,
               d->partial.p, d->partial2.p, d->diff.p, rs_dev};
   B2D_CU(launch_collect_diff(ga, d->bcap, d->sm_count, s));
-  if (timing) B2D_CU(cudaEventRecordWithFlags(d->ev[2], s, cudaEventRecordExternal));
+  if (timing) B2D_CU(record_timing(d->ev[2], s));
   if (!managed) B2D_CU(cudaMemcpyAsync(d->state_h.p, d->state.p, sizeof(DevState), cudaMemcpyDeviceToHost, s));
   d->launches = (skip_leaves ? 0 : 1) + forest_launch_count(d->D, 1) + forest_launch_count(d->D, 2) + 1 + 14;
   return B2D_OK;
@@ -545,6 +565,13 @@ int do_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, bool make_base
   int rc = prepare_checkpoint(d, d_data, len, make_baseline);
   if (rc) return rc;
   RoundState* rs_dev = &d->state.p->round;
+  if (!d->use_graph) {
+    d->timers[0] = secs(t0, clk::now());
+    rc = enqueue_checkpoint(d, d->stream, rs_dev, true, true, false);
+    if (rc) return rc;
+    B2D_CU(cudaStreamSynchronize(d->stream));
+    return finish_checkpoint(d, advance, true);
+  }
   // the round state lives in DevState, which the enqueue clears first: upload after the clear
   std::vector<uint64_t> key;
   graph_key(d, rs_dev, key);
@@ -1413,6 +1440,7 @@ int b2d_set_param(b2d_dedup* d, const char* name, int64_t value) {
   else if (k == "leaf_ctas_per_sm" && value >= 0 && value <= 8) d->tune.ctas_per_sm = (int)value;
   else if (k == "map_max_load_pct" && value >= 10 && value <= 90) d->map_max_load = value / 100.0;
   else if (k == "map_headroom_pct" && value >= 100 && value <= 1000) d->map_headroom = value / 100.0;
+  else if (k == "graph" && (value == 0 || value == 1)) d->use_graph = value != 0;
   else return B2D_ERR_ARG;
   return B2D_OK;
 }
@@ -1500,6 +1528,36 @@ int b2d_map_stats(b2d_dedup* d, double out[5]) {
   return B2D_OK;
 }
 
+int b2d_pool_reserve(uint64_t bytes) {
+  B2D_GUARD({
+    int dev = 0;
+    B2D_CU(cudaGetDevice(&dev));
+    cudaMemPool_t pool = map_pool(dev);
+    if (!pool) return B2D_ERR_CUDA;
+    {
+      std::lock_guard<std::mutex> lock(g_pool_mu);
+      if ((int)g_pool_keep.size() <= dev) g_pool_keep.resize(dev + 1, 0);
+      g_pool_keep[dev] = bytes;
+    }
+    if (bytes == 0) {
+      B2D_CU(cudaMemPoolTrimTo(pool, 0));
+      return B2D_OK;
+    }
+    // map the memory once: allocate it as one block and hand it back to the pool, which keeps
+    // it (release threshold: never) and carves later map allocations out of it
+    cudaStream_t s = nullptr;
+    B2D_CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    void* p = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, pool, s);
+    if (e == cudaSuccess) e = cudaFreeAsync(p, s);
+    const cudaError_t e2 = cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    B2D_CU(e);
+    B2D_CU(e2);
+    return B2D_OK;
+  })
+}
+
 int b2d_memory(b2d_dedup* d, uint64_t* bytes) {
   if (!d || !bytes) return B2D_ERR_ARG;
   *bytes = handle_bytes(d);
@@ -1512,7 +1570,7 @@ int b2d_estimate_memory(uint64_t len, uint32_t chunk_size, int map_max_load_pct,
   if (map_max_load_pct < 10 || map_max_load_pct > 90) return B2D_ERR_ARG;
   // the allocations prepare_checkpoint makes for a buffer of `len` bytes (checkpoint side)
   const uint64_t n = (len + chunk_size - 1) / chunk_size, N = 2 * n - 1;
-  const uint64_t cap = map_capacity(2 * N, map_max_load_pct / 100.0, 1.25);
+  const uint64_t cap = map_capacity(2 * N, map_max_load_pct / 100.0, MAP_HEADROOM);
   uint64_t b = N * sizeof(Digest) + N + (n + 16) + ((N + 15) / 16 * 16 + 16) + n;   // tree, labels, flags
   b += (cap + 1) * sizeof(MapSlot) + 8;                                              // map
   b += 8 * 4 * n + 68 * 4;                                                           // lists and keys

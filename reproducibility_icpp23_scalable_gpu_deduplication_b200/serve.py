@@ -28,7 +28,7 @@ import time
 
 from ._lib import HASH_MURMUR3
 from .batch import CheckpointBatch
-from .tree import TreeDeduplicator, estimate_memory
+from .tree import TreeDeduplicator, estimate_memory, reserve_map_memory
 
 __all__ = ["CheckpointServer", "Request"]
 
@@ -65,7 +65,10 @@ class _Client:
 
 class CheckpointServer:
     def __init__(self, hbm_budget=150e9, chunk_size=128, hash_kind=HASH_MURMUR3, max_batch=64, max_inflight=2,
-                 evict=True, plain=False, checksum=False, clock=time.perf_counter, **batch_params):
+                 evict=True, plain=False, checksum=False, clock=time.perf_counter, map_reserve=0, **batch_params):
+        """`map_reserve`: bytes of device memory mapped up front for digest-map growth
+        (``reserve_map_memory``), so a client whose map grows does not pay for fresh driver
+        allocations inside its request; released by ``close``."""
         import torch
 
         self.budget = int(hbm_budget)
@@ -81,6 +84,9 @@ class CheckpointServer:
         self.seq = 0
         params = {"graph_cache": 256}
         params.update(batch_params)
+        self.map_reserve = int(map_reserve)
+        if self.map_reserve:
+            reserve_map_memory(self.map_reserve)
         self.slots = [] if plain else [
             (CheckpointBatch(**params), torch.cuda.Stream(), []) for _ in range(max(1, int(max_inflight)))]
 
@@ -118,6 +124,9 @@ class CheckpointServer:
                 c.handle.close()
                 c.handle = None
         self.clients.clear()
+        if self.map_reserve:
+            reserve_map_memory(0)
+            self.map_reserve = 0
 
     # -- loop
     def step(self):

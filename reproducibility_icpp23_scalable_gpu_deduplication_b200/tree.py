@@ -236,6 +236,11 @@ class TreeDeduplicator:
         return out
 
 
+def reserve_map_memory(nbytes):
+    """Keep `nbytes` of device memory mapped for digest maps (see b2d_pool_reserve)."""
+    check(lib().b2d_pool_reserve(int(nbytes)), "b2d_pool_reserve")
+
+
 def estimate_memory(nbytes, chunk_size, map_max_load_pct=0):
     """Device bytes a handle will hold for checkpoints of an `nbytes` buffer."""
     v = ctypes.c_uint64()
