@@ -43,8 +43,9 @@ def parse():
     p.add_argument("--steps", type=int, default=16)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--workload", default="plain_4g", choices=["plain_4g", "md5_f32_8g"],
-                   help="plain form: the 4 GiB Murmur3 series (default) or the 8 GiB float32 MD5 series")
+    p.add_argument("--workload", default="plain_4g", choices=["plain_4g", "md5_f32_8g", "plain_64m"],
+                   help="plain form: the 4 GiB Murmur3 series (default), the 8 GiB float32 MD5 series, or "
+                        "the 64 MiB CPU-runnable series (5% rewritten, 2% shifted, 1% zeroed per checkpoint)")
     p.add_argument("--chunk-size", type=int, default=None, help="default 128 (plain_4g) / 256 (md5_f32_8g)")
     p.add_argument("--nbytes", type=int, default=None, help="default 4 GiB (plain_4g) / 8 GiB (md5_f32_8g)")
     p.add_argument("--e2e-steps", type=int, default=2)
@@ -58,7 +59,10 @@ def parse():
     p.add_argument("--buffers", type=int, default=256, help="batched form: number of buffers")
     p.add_argument("--max-buffer", type=int, default=512 << 20, help="batched form: largest buffer size")
     p.add_argument("--no-autotune", action="store_true")
-    p.add_argument("--no-graph", action="store_true", help="plain form: launch kernels one by one, no CUDA graph")
+    p.add_argument("--no-plain", action="store_true", help="batched form: skip the one-at-a-time pass")
+    p.add_argument("--graph", type=int, default=None, choices=[0, 1, 2],
+                   help="plain form: 0 launch kernels one by one, 1 replay a CUDA graph, 2 graph without "
+                        "phase-timing events (default: the library's)")
     p.add_argument("--clients", type=int, default=64, help="served form: clients")
     p.add_argument("--requests", type=int, default=1000, help="served form: requests in the stream")
     p.add_argument("--rate", type=float, default=200.0, help="served form: aggregate arrivals per second")
@@ -71,7 +75,7 @@ def parse():
     if a.chunk_size is None:
         a.chunk_size = 256 if md5 else 128
     if a.nbytes is None:
-        a.nbytes = (8 << 30) if md5 else (4 << 30)
+        a.nbytes = (8 << 30) if md5 else ((64 << 20) if a.workload == "plain_64m" else (4 << 30))
     return a
 
 
@@ -141,6 +145,8 @@ def workload_series(workload, nbytes, cs, device, seed):
 
     if workload == "md5_f32_8g":
         return synth.FloatSeries(nbytes=nbytes, device=device, seed=seed)
+    if workload == "plain_64m":
+        return synth.plain_64m(nbytes=nbytes, chunk_size=cs, device=device, seed=seed)
     return synth.plain_4g(nbytes=nbytes, chunk_size=cs, device=device, seed=seed)
 
 
@@ -268,9 +274,9 @@ def run_batched(args, rank, world, dev):
         return batch.launch_count()
 
     with ClockSampler(int(dev.index or 0)) as clk:
-        t_plain, s_plain, l_plain = series_pass(plain_step)
+        t_plain, s_plain, l_plain = series_pass(plain_step) if not args.no_plain else ([float("nan")], None, 0)
         t_batch, s_batch, l_batch = series_pass(batch_step)
-    same = s_plain == s_batch
+    same = s_plain == s_batch or args.no_plain
     ms_b, ms_p = statistics.mean(t_batch), statistics.mean(t_plain)
     tt = torch.tensor([ms_b, ms_p], device=dev)
     if world > 1:
@@ -291,11 +297,11 @@ def run_batched(args, rank, world, dev):
                    "min_buffer": min(sizes), "max_buffer": max(sizes), "chunk_size": 128, "hash": "murmur3",
                    "checkpoints": ckpts, "change": "uniform [0.5%, 20%] in runs of 1-256 chunks + 1% shifted",
                    "l2": f"inputs {total / 2**30:.1f} GiB > L2, no flush", "tuned": tuned},
-        "plain_same_workload": {"value": round(plain, 2), "unit": "GB/s", "ms_per_step": round(ms_p, 4),
-                                "gpu_launches": l_plain},
-        "speedup_vs_plain": round(value / plain, 3),
-        "parity": ("identical" if same else "MISMATCH") + f": diff checksums of {len(sizes)} buffers x {ckpts} "
-                  "checkpoints, batched vs one at a time",
+        "plain_same_workload": None if args.no_plain else {
+            "value": round(plain, 2), "unit": "GB/s", "ms_per_step": round(ms_p, 4), "gpu_launches": l_plain},
+        "speedup_vs_plain": None if args.no_plain else round(value / plain, 3),
+        "parity": ("not compared (--no-plain)" if args.no_plain else ("identical" if same else "MISMATCH") +
+                   f": diff checksums of {len(sizes)} buffers x {ckpts} checkpoints, batched vs one at a time"),
         "e2e": None,
         "gpu_launches": l_batch,
         "roofline": {"bound": "hbm", "kernel": "whole batch (graph)", "achieved": round(alg / (ms_b * 1e-3) / GB, 1),
@@ -351,6 +357,15 @@ def serve_stream(server_kw, sizes, clients, arrivals, dev, warm_rounds=2):
     wall = max(r.done for r in reqs) - t0
     batches = srv.batches
     service = [r.done - t for r, t in zip(reqs, submitted)]
+    grows = sum(c.handle.map_stats()[2] for c in srv.clients.values() if c.handle is not None)
+    queue = sorted(1e3 * (r.launched - t) for r, t in zip(reqs, submitted))
+    execu = sorted(1e3 * (r.done - r.launched) for r in reqs)
+    print(json.dumps({"diag": "served_stream", "plain": bool(server_kw.get("plain")), "map_grows_total": grows,
+                      "queue_ms_p50_p99_max": [queue[len(queue) // 2], queue[int(0.99 * len(queue))], queue[-1]],
+                      "exec_ms_p50_p99_max": [execu[len(execu) // 2], execu[int(0.99 * len(execu))], execu[-1]],
+                      "slowest": sorted(((round(1e3 * (r.done - t), 1), r.client, r.nbytes >> 20)
+                                         for r, t in zip(reqs, submitted)), reverse=True)[:8]}),
+          file=sys.stderr, flush=True)
     srv.close()
     del series
     torch.cuda.empty_cache()
@@ -489,8 +504,8 @@ def main():
         dd.set_param("leaf_stages", args.leaf_stages)
     if args.leaf_ctas:
         dd.set_param("leaf_ctas_per_sm", args.leaf_ctas)
-    if args.no_graph:
-        dd.set_param("graph", 0)
+    if args.graph is not None:
+        dd.set_param("graph", args.graph)
     dd.checkpoint_device(series.next(), make_baseline=True)          # checkpoint 0: baseline
     for _ in range(args.warmup):
         dd.checkpoint_device(series.next())
@@ -503,10 +518,21 @@ def main():
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    # inputs smaller than 2x the 126 MB L2: flush L2 before each step (outside the timed spans)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev) if nbytes < (256 << 20) else None
+    step_ms = []
     with ClockSampler(local) as clk:
         start.record(stream)
         for b in bufs:
+            if flush is not None:
+                flush.fill_(1)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
             diff_bytes.append(dd.checkpoint_device(b))
+            if flush is not None:
+                e1.record(stream)
+                e1.synchronize()
+                step_ms.append(e0.elapsed_time(e1))
             ph, path = dd.phase_times()
             leaf_s.append(ph[0])
             forest_s.append(ph[1])
@@ -516,13 +542,14 @@ def main():
         torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    ms = start.elapsed_time(stop)
+    ms = start.elapsed_time(stop) if flush is None else sum(step_ms)
+    del flush
     t = torch.tensor([ms], device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_max = float(t.item())
     value = world * args.steps * nbytes / (ms_max * 1e-3) / GB
-    leaf_ms = 1e3 * statistics.mean(leaf_s)
+    leaf_ms = 1e3 * statistics.mean(leaf_s)   # 0 when the graph runs without timing events
     del bufs
 
     # end to end through the public API: host buffers in pinned memory, diff back to the host
@@ -549,7 +576,7 @@ def main():
 
     peak, peak_kind = measured_peak()
     alg_leaf = nbytes + 32 * n_chunks              # read the buffer, read + write a digest per chunk
-    achieved = alg_leaf / (leaf_ms * 1e-3) / GB
+    achieved = alg_leaf / (leaf_ms * 1e-3) / GB if leaf_ms > 0 else 0.0
     tb = leaf_traffic(cs)
     roofline = {"bound": "hbm", "kernel": f"leaf_tma_kernel (chunk {cs} B)" if path else "leaf_generic_kernel",
                 "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
@@ -563,7 +590,9 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic (seeded; reference datasets unavailable)",
         "config": {"workload": args.workload, "nbytes": nbytes, "chunk_size": cs, "hash": "md5" if md5 else "murmur3",
-                   "checkpoints": 1 + args.warmup + args.steps, "l2": "inputs 4 GiB > L2, no flush",
+                   "checkpoints": 1 + args.warmup + args.steps,
+                   "l2": (f"inputs {nbytes / 2**30:.2f} GiB > L2, no flush" if nbytes >= (256 << 20) else
+                          "L2 flushed (512 MiB write) before each step, outside the timed spans"),
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": round(e2e_value, 2) if e2e_value else None, "unit": "GB/s", "h2d_bytes_per_step": nbytes,
                 "d2h_bytes_per_step": int(statistics.mean(d2h)) if d2h else 0},

@@ -71,8 +71,9 @@ int b2d_set_stream(b2d_dedup* d, void* cuda_stream);
  *                       when the map's entries plus every node of the tree fit under it
  *   "map_headroom_pct"  size of a baseline's map over that minimum, 100..1000 (default 200);
  *                       more headroom = fewer growths (allocate + rehash) in a long series
- *   "graph"             1 = replay a checkpoint's launches as one CUDA graph (default), 0 = launch
- *                       them one by one on the handle's stream */
+ *   "graph"             0 = launch a checkpoint's kernels one by one on the handle's stream
+ *                       (default; measured faster), 1 = replay them as one CUDA graph, 2 = graph
+ *                       without the phase-timing events (b2d_phase_times then reads 0) */
 int b2d_set_param(b2d_dedup* d, const char* name, int64_t value);
 
 /* checkpoint(header_t&, uint8_t* data_ptr, size_t len, HostMirror& diff_h, bool make_baseline)
@@ -170,7 +171,7 @@ int b2d_pool_reserve(uint64_t bytes);
 int b2d_memory(b2d_dedup* d, uint64_t* bytes);
 /* Digest map statistics: out[0] slots, out[1] entries after the last checkpoint, out[2] times
  * the map has grown (rehashed into a larger table), out[3] host seconds spent growing it,
- * out[4] of which allocating the larger tables. */
+ * out[4] host seconds spent in the allocation calls of all its tables (baselines included). */
 int b2d_map_stats(b2d_dedup* d, double out[5]);
 int b2d_estimate_memory(uint64_t len, uint32_t chunk_size, int map_max_load_pct, uint64_t* bytes);
 

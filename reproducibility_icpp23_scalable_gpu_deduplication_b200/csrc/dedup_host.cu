@@ -156,7 +156,10 @@ struct b2d_dedup {
   bool have_tree = false;
   LeafTuning tune;
   double map_max_load = 0.75;
-  bool use_graph = true;          // replay each checkpoint's launches as one CUDA graph
+  // replay each checkpoint's launches as one CUDA graph (off by default: on the 4 GiB series
+  // the graph launch measured 0.15-0.2 ms slower per checkpoint than the 22 stream launches)
+  bool use_graph = false;
+  bool graph_timing = true;       // phase timing events inside the graph
   double map_headroom = MAP_HEADROOM;   // baseline table size over its minimum (entries + N at max load)
 
   cudaStream_t own_stream = nullptr;
@@ -171,7 +174,7 @@ struct b2d_dedup {
   MapSlot* map_slots = nullptr;   // map_cap + 1 slots, from the library's map pool
   uint64_t map_cap = 0;
   double map_grow_s = 0;          // host seconds spent growing the map (all checkpoints)
-  double map_alloc_s = 0;         // of which in allocating the larger table
+  double map_alloc_s = 0;         // host seconds in the map allocation calls (all tables)
   uint32_t map_grows = 0;
   uint64_t map_size_host = 0;     // occupied slots after the last checkpoint
   DevBuf<unsigned long long> map_size;
@@ -310,7 +313,9 @@ int map_view(b2d_dedup* d, MapView& m) {
 int map_alloc(b2d_dedup* d, uint64_t cap, MapSlot** out) {
   cudaMemPool_t pool = map_pool(d->device);
   if (!pool) return B2D_ERR_CUDA;
+  const auto t0 = std::chrono::high_resolution_clock::now();
   B2D_CU(cudaMallocFromPoolAsync(reinterpret_cast<void**>(out), sizeof(MapSlot) * (cap + 1), pool, d->stream));
+  d->map_alloc_s += secs(t0, std::chrono::high_resolution_clock::now());
   B2D_CU(cudaMemsetAsync(*out, 0xff, sizeof(MapSlot) * (cap + 1), d->stream));
   map_special_init_kernel<<<1, 1, 0, d->stream>>>(*out + cap);
   return cuda_status(cudaGetLastError());
@@ -355,7 +360,6 @@ int map_ensure(b2d_dedup* d) {
   MapSlot* fresh = nullptr;
   int rc = map_alloc(d, cap, &fresh);
   if (rc) return rc;
-  d->map_alloc_s += secs(t0, std::chrono::high_resolution_clock::now());
   DevBuf<unsigned long long> cnt;
   B2D_CU(cnt.reserve(1));
   B2D_CU(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long), d->stream));
@@ -481,7 +485,7 @@ void graph_key(const b2d_dedup* d, const RoundState* rs_dev, std::vector<uint64_
             (uint64_t)d->region_off.p, (uint64_t)d->sprev.p, (uint64_t)d->skey.p, (uint64_t)d->hist.p,
             (uint64_t)d->bucket_start.p, (uint64_t)d->partial.p, (uint64_t)d->partial2.p, (uint64_t)d->diff.p,
             (uint64_t)d->state.p, (uint64_t)d->state_h.p, (uint64_t)d->round_h.p, (uint64_t)rs_dev, d->bcap,
-            (uint64_t)d->tune.allow_tma, (uint64_t)d->tune.stages, (uint64_t)d->tune.ctas_per_sm,
+            (uint64_t)d->tune.allow_tma, (uint64_t)d->tune.stages, (uint64_t)d->tune.ctas_per_sm, (uint64_t)d->graph_timing,
             (uint64_t)d->sm_count});
 }
 
@@ -584,7 +588,7 @@ int do_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, bool make_base
     // cannot be captured) and launched on the caller's
     cudaGraph_t g = nullptr;
     B2D_CU(cudaStreamBeginCapture(d->cap_stream, cudaStreamCaptureModeThreadLocal));
-    rc = enqueue_checkpoint(d, d->cap_stream, rs_dev, true, true, false);
+    rc = enqueue_checkpoint(d, d->cap_stream, rs_dev, true, d->graph_timing, false);
     const cudaError_t ce = cudaStreamEndCapture(d->cap_stream, &g);
     if (rc) {
       if (g) cudaGraphDestroy(g);
@@ -599,7 +603,7 @@ int do_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, bool make_base
   d->timers[0] = secs(t0, clk::now());
   B2D_CU(cudaGraphLaunch(d->graph_exec, d->stream));
   B2D_CU(cudaStreamSynchronize(d->stream));
-  return finish_checkpoint(d, advance, true);
+  return finish_checkpoint(d, advance, d->graph_timing);
 }
 
 int copy_diff(b2d_dedup* d, void* dst, uint64_t cap) {
@@ -1440,7 +1444,10 @@ int b2d_set_param(b2d_dedup* d, const char* name, int64_t value) {
   else if (k == "leaf_ctas_per_sm" && value >= 0 && value <= 8) d->tune.ctas_per_sm = (int)value;
   else if (k == "map_max_load_pct" && value >= 10 && value <= 90) d->map_max_load = value / 100.0;
   else if (k == "map_headroom_pct" && value >= 100 && value <= 1000) d->map_headroom = value / 100.0;
-  else if (k == "graph" && (value == 0 || value == 1)) d->use_graph = value != 0;
+  else if (k == "graph" && value >= 0 && value <= 2) {
+    d->use_graph = value != 0;
+    d->graph_timing = value != 2;
+  }
   else return B2D_ERR_ARG;
   return B2D_OK;
 }

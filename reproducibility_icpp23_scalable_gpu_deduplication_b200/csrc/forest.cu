@@ -224,6 +224,12 @@ __global__ void __launch_bounds__(FAST_THREADS) forest_first_kernel(ForestArgs a
 #pragma unroll
     for (int j = 0; j < 4; j++) m0 |= (uint32_t)(input_label<1>(a, x0 + j) == FIRST_OCUR) << j;
   }
+  // no first occurrence among the inputs: nothing to hash or insert, the band root is DONE
+  // (unless level D-1 holds leaves, which the first band of a non-power-of-two tree reads below)
+  if ((aligned || in < a.D) && !__syncthreads_or(m0 != 0u)) {
+    if (t == 0) band_output<1>(a, root, DONE);
+    return;
+  }
   // band height 1: nodes p0, p0 + 1
   Digest d1[2];
   uint32_t m1 = 0;
@@ -304,11 +310,17 @@ __global__ void __launch_bounds__(FAST_THREADS) forest_first_kernel(ForestArgs a
   }
   __syncthreads();
   // inserts: rank the set bits (prefix of per-word counts), thread t takes ranks t, t+256, ...
-  if (t < FF_WORDS) wpre[t + 1] = __popc(ff[t]);
-  if (t == 0) wpre[0] = 0;
-  __syncthreads();
-  if (t == 0)
-    for (uint32_t w = 1; w <= FF_WORDS; w++) wpre[w] += wpre[w - 1];
+  static_assert(FF_WORDS == 32, "one word per lane of warp 0");
+  if (warp == 0) {
+    uint32_t c = __popc(ff[lane]);
+#pragma unroll
+    for (uint32_t o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xffffffffu, c, o);
+      if (lane >= o) c += v;
+    }
+    wpre[lane + 1] = c;
+    if (lane == 0) wpre[0] = 0;
+  }
   __syncthreads();
   const uint32_t total = wpre[FF_WORDS];
   for (uint32_t r = t; r < total; r += FAST_THREADS) {
@@ -362,6 +374,12 @@ __global__ void __launch_bounds__(FAST_THREADS) forest_fast_kernel(ForestArgs a0
       if (PHASE == 2) fast = fast && v[j] == FIXED_DUPL;
       else fast = fast && v[j] != FIRST_OCUR && v[j] != NONE_LABEL;
     }
+  }
+  // every input of the band unchanged (phase 2: all FIXED; phase 1: no first occurrence): the
+  // whole subtree folds to one label without further work
+  if (!__syncthreads_or(!fast)) {
+    if (t == 0) band_output<PHASE>(a, root, PHASE == 2 ? FIXED_DUPL : DONE);
+    return;
   }
   uint8_t lab;
   if (fast) {

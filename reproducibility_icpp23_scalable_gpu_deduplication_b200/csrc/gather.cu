@@ -513,25 +513,33 @@ __global__ void __launch_bounds__(256) gather_bytes_kernel(DiffArgs a0) {
   }
 }
 
+static uint32_t grid_for(uint64_t units, uint64_t per_cta, uint32_t cap) {
+  const uint64_t g = (units + per_cta - 1) / per_cta;
+  return g < 1 ? 1u : (g > cap ? cap : (uint32_t)g);
+}
+
 cudaError_t launch_collect_diff(const DiffArgs& a, uint32_t bcap, int sm_count, cudaStream_t stream) {
-  const uint32_t g = SCAN_GRID;
+  // grids follow the buffer size (host-known bounds: F, S <= n), so a small buffer is not
+  // charged for hundreds of idle CTAs per launch; large buffers get the full grids
+  const uint32_t g = grid_for(((uint64_t)a.N + 15u) / 16u, 512, SCAN_GRID);   // ~1 16-node load per thread
+  const uint32_t gs = grid_for(a.n, 2048, SHIFT_GRID);
   const uint32_t B = bcap;   // capacity; each kernel reads the checkpoint's bucket count from rs
   if (B > MAX_BUCKETS) return cudaErrorInvalidValue;
   compact_count_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);
   compact_scan_kernel<<<1, 1024, 0, stream>>>(a, g);
   compact_write_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);
   compact_levels_kernel<<<(2u * (a.D + 2u) * 32u + 255u) / 256u, 256, 0, stream>>>(a);
-  compact_permute_kernel<<<(uint32_t)sm_count * 2u, 256, 0, stream>>>(a);
+  compact_permute_kernel<<<grid_for(a.n, 2048, (uint32_t)sm_count * 2u), 256, 0, stream>>>(a);
   region_count_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);
   region_scan_kernel<<<1, 1024, 0, stream>>>(a, g);
   region_write_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);
   cudaError_t e = cudaMemsetAsync(a.hist, 0, sizeof(uint32_t) * B, stream);
   if (e != cudaSuccess) return e;
   const size_t hsm = sizeof(uint32_t) * B;   // <= 32 KB for MAX_BUCKETS
-  shift_prev_kernel<<<SHIFT_GRID, 128, hsm, stream>>>(a, B);
-  layout_kernel<<<1, 1024, 0, stream>>>(a, B, SHIFT_GRID);
-  shift_write_kernel<<<SHIFT_GRID, 32, hsm, stream>>>(a, B);
-  const uint32_t gblocks = (uint32_t)sm_count * 4u;
+  shift_prev_kernel<<<gs, 128, hsm, stream>>>(a, B);
+  layout_kernel<<<1, 1024, 0, stream>>>(a, B, gs);
+  shift_write_kernel<<<gs, 32, hsm, stream>>>(a, B);
+  const uint32_t gblocks = grid_for((uint64_t)a.n * a.cs, 32768, (uint32_t)sm_count * 4u);
   const bool vec = (a.cs % 16u == 0) && ((reinterpret_cast<uintptr_t>(a.data) & 15u) == 0) &&
                    ((reinterpret_cast<uintptr_t>(a.diff) & 15u) == 0);
   if (vec) {

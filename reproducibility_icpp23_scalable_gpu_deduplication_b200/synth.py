@@ -335,9 +335,13 @@ class DeviceSeries:
             src = torch.randint(0, n - 1, (m,), generator=g, device=dev)
             src += (src >= dst).to(src.dtype)
             rows = view[src].clone()
-        streams = idx | ((2 << 56) | (self.ckpt << 40))
-        w = words_torch_t(self.seed + self.client, streams, (self.cs + 7) // 8)
-        view[idx] = w.view(torch.uint8).reshape(total, -1)[:, :self.cs]
+        # fresh bytes in slices, so the temporaries stay small and are reused from the allocator
+        tag = (2 << 56) | (self.ckpt << 40)
+        step = 1 << 16
+        for lo in range(0, total, step):
+            part = idx[lo:lo + step]
+            w = words_torch_t(self.seed + self.client, part | tag, (self.cs + 7) // 8)
+            view[part] = w.view(torch.uint8).reshape(part.numel(), -1)[:, :self.cs]
         if m:
             view[dst] = rows
         return self.data
