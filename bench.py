@@ -59,6 +59,7 @@ def parse():
     p.add_argument("--buffers", type=int, default=256, help="batched form: number of buffers")
     p.add_argument("--max-buffer", type=int, default=512 << 20, help="batched form: largest buffer size")
     p.add_argument("--no-autotune", action="store_true")
+    p.add_argument("--no-restart", action="store_true", help="plain form: skip the restart measurement")
     p.add_argument("--no-plain", action="store_true", help="batched form: skip the one-at-a-time pass")
     p.add_argument("--graph", type=int, default=None, choices=[0, 1, 2],
                    help="plain form: 0 launch kernels one by one, 1 replay a CUDA graph, 2 graph without "
@@ -317,7 +318,7 @@ def run_batched(args, rank, world, dev):
         sys.exit(3)
 
 
-def serve_stream(server_kw, sizes, clients, arrivals, dev, warm_rounds=2):
+def serve_stream(server_kw, sizes, clients, arrivals, dev, warm_rounds=2, reserve=0):
     """Drive one CheckpointServer through a request stream; returns (requests, wall seconds)."""
     import torch
 
@@ -331,6 +332,9 @@ def serve_stream(server_kw, sizes, clients, arrivals, dev, warm_rounds=2):
         for c in range(len(sizes)):
             srv.submit(c, series[c].next())
         srv.drain()
+    if reserve:
+        srv.reserve_growth(reserve)     # clients resident: keep memory mapped for map growth
+    srv.enable_host_copy({c: n for c, n in enumerate(sizes)})   # a request ends with its diff on the host
     torch.cuda.synchronize()
     srv.completed.clear()
     clock = srv.clock
@@ -416,7 +420,7 @@ def run_served(args, rank, world, dev):
     clients = rng.integers(0, len(sizes), n)
     arrivals = synth.poisson_arrivals(args.rate, n, seed=synth.SEED + rank)
     budget = args.hbm_budget
-    kw = {"hbm_budget": budget, "max_batch": 64, "max_inflight": 2, "map_reserve": args.map_reserve}
+    kw = {"hbm_budget": budget, "max_batch": 64, "max_inflight": 2}
 
     def summarize(reqs, wall, batches, service):
         lat = [1e3 * r.latency for r in reqs]
@@ -429,8 +433,9 @@ def run_served(args, rank, world, dev):
                 "wall_s": round(wall, 3)}
 
     with ClockSampler(int(dev.index or 0)) as clk:
-        served = summarize(*serve_stream(kw, sizes, clients, arrivals, dev))
-        plain = summarize(*serve_stream(dict(kw, plain=True), sizes, clients, arrivals, dev))
+        served = summarize(*serve_stream(kw, sizes, clients, arrivals, dev, reserve=args.map_reserve))
+        plain = summarize(*serve_stream(dict(kw, plain=True), sizes, clients, arrivals, dev,
+                                        reserve=args.map_reserve))
         # capacity: all clients' requests waiting at once (unbounded arrival rate), 4 waves
         cap_served = summarize(*serve_capacity(kw, sizes, 4, dev))
         cap_plain = summarize(*serve_capacity(dict(kw, plain=True), sizes, 4, dev))
@@ -440,11 +445,11 @@ def run_served(args, rank, world, dev):
         "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded; reference datasets unavailable)",
         "config": {"workload": f"served_{len(sizes)}_clients", "clients": len(sizes), "rate_hz": args.rate,
                    "requests": n, "client_bytes_total": sum(sizes), "min_buffer": min(sizes),
-                   "max_buffer": max(sizes), "chunk_size": 128, "hash": "murmur3", "hbm_budget": budget,
+                   "max_buffer": max(sizes), "chunk_size": 128, "hash": "murmur3", "hbm_budget": budget, "map_growth_reserve": args.map_reserve,
                    "change": "uniform [0.5%, 20%] in runs of 1-512 chunks + 1% shifted, edited on the device",
-                   "latency": "scheduled arrival -> diff ready on the device (includes the client's wait "
+                   "latency": "scheduled arrival -> diff in pinned host memory (includes the client's wait "
                               "for its own previous request and its device-side edit of its buffer); "
-                              "service_*: submission -> diff ready"},
+                              "service_*: submission -> diff on the host; capacity: diffs stay on the device"},
         "latency_ms": {"p50": served["p50_ms"], "p99": served["p99_ms"], "max": served["max_ms"]},
         "served": served, "plain_same_stream": plain,
         "capacity": {"mode": "all 64 clients submit at once, buffers edited and resident; 4 waves",
@@ -573,6 +578,35 @@ def main():
     if world > 1:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_value = world * len(e2e_bufs) * nbytes / (float(te.item()) * 1e-3) / GB if e2e_bufs else None
+    del e2e_bufs
+
+    # restart: rebuild the last checkpoint of a fresh 4-checkpoint series from its diffs held in
+    # pinned host memory (host -> device copies and scatter inside the timed span)
+    restart = None
+    if not args.no_restart:
+        rs = workload_series(args.workload, nbytes, cs, dev, synth.SEED + rank + 17)
+        rd = TreeDeduplicator(cs, HASH_MD5 if md5 else HASH_MURMUR3)
+        diffs = []
+        for k in range(4):
+            x = rs.next()
+            rd.checkpoint_device(x, k == 0)
+            pin = torch.empty(rd.diff_device()[1], dtype=torch.uint8).pin_memory()
+            diffs.append(rd.copy_diff(pin.numpy()))
+        out = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        rd.restart(out, diffs, 3)
+        torch.cuda.synchronize()
+        r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        r0.record(stream)
+        rd.restart(out, diffs, 3)
+        r1.record(stream)
+        torch.cuda.synchronize()
+        r_ms = r0.elapsed_time(r1)
+        restart = {"value": round(nbytes / (r_ms * 1e-3) / GB, 2), "unit": "GB/s", "ms": round(r_ms, 3),
+                   "diffs": 4, "h2d_bytes": int(sum(d.nbytes for d in diffs)),
+                   "identical": bool(torch.equal(out, x.view(torch.uint8).reshape(-1)[:nbytes]))}
+        rd.close()
+        del rs, diffs, out, x
+        torch.cuda.empty_cache()
 
     peak, peak_kind = measured_peak()
     alg_leaf = nbytes + 32 * n_chunks              # read the buffer, read + write a digest per chunk
@@ -597,6 +631,7 @@ def main():
         "e2e": {"value": round(e2e_value, 2) if e2e_value else None, "unit": "GB/s", "h2d_bytes_per_step": nbytes,
                 "d2h_bytes_per_step": int(statistics.mean(d2h)) if d2h else 0},
         "gpu_launches": launches,
+        "restart": restart,
         "roofline": roofline,
         "clocks": clk.summary(),
         "diff_bytes_per_step": int(statistics.mean(diff_bytes)),

@@ -87,6 +87,11 @@ int b2d_checkpoint_device(b2d_dedup* d, const void* d_data, uint64_t len, int ma
 int b2d_diff_device(b2d_dedup* d, const void** d_diff, uint64_t* diff_len);
 /* Copy the last diff to host memory `dst` of `cap` bytes (timers[3] of the reference). */
 int b2d_copy_diff(b2d_dedup* d, void* dst, uint64_t cap);
+/* The same copy enqueued on `cuda_stream` (NULL = the handle's stream) without waiting: `dst`
+ * (pinned host memory for an asynchronous copy) holds the diff once that stream reaches this
+ * point.  For callers that overlap the copy-back with other checkpoints.  No reference
+ * counterpart. */
+int b2d_copy_diff_async(b2d_dedup* d, void* dst, uint64_t cap, void* cuda_stream);
 
 /* checkpoint(uint8_t* data_ptr, size_t len, HostMirror& diff_h, bool make_baseline)
  * -- src/tree_approach.cpp:1740-1748.  *diff points at pinned host memory owned by the handle,
@@ -193,8 +198,10 @@ int b2d_batch_set_stream(b2d_batch* b, void* cuda_stream);
  * "tiles_per_pop" (work-queue granule, tiles of 256 chunks), "streams" (graph branches for the
  * per-handle work), "autotune" (1: coordinate descent over those knobs, one setting per
  * incremental batch -- six batches -- measured by device time; "tuned" reads 1 once it has
- * settled and the knobs then read the chosen values), "graph_cache" (instantiated graphs kept,
- * one per batch composition, default 16).  Output never depends on them. */
+ * settled and the knobs then read the chosen values), "graph" (2 = launch a composition directly
+ * the first time and as a captured graph from its second batch on, default; 1 = always a graph;
+ * 0 = never), "graph_cache" (instantiated graphs kept, one per batch composition, default 16).
+ * Output never depends on them. */
 int b2d_batch_set_param(b2d_batch* b, const char* name, int64_t value);
 int b2d_batch_get_param(b2d_batch* b, const char* name, int64_t* value);
 int b2d_batch_checkpoint(b2d_batch* b, b2d_dedup* const* handles, const void* const* d_data, const uint64_t* lens,

@@ -785,10 +785,18 @@ int do_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* di
     // stage the diff (plus its repeat-table running counts) in pinned memory, then one copy
     const uint32_t delta = (uint32_t)((16u - (hh.data_off & 15u)) & 15u);
     const uint64_t ncum = (uint64_t)hh.chkpt_id + 1;
-    B2D_CU(cudaStreamSynchronize(d->stream));   // the staging buffer is reused per diff
-    uint8_t* stage = d->r_stage.p;
+    // pinned (page-locked) diffs are copied straight to the device; others go through the
+    // handle's pinned staging buffer, reused per diff
+    cudaPointerAttributes pa;
+    const bool pinned = cudaPointerGetAttributes(&pa, diffs[idx]) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    if (!pinned) (void)cudaGetLastError();
+    if (!pinned) B2D_CU(cudaStreamSynchronize(d->stream));
     const auto c0 = clk::now();
-    memcpy(stage + delta, diffs[idx], sizes[idx]);
+    const uint8_t* src = diffs[idx];
+    if (!pinned) {
+      memcpy(d->r_stage.p + delta, diffs[idx], sizes[idx]);
+      src = d->r_stage.p + delta;
+    }
     std::vector<unsigned long long> cum(ncum, 0ull);
     bool bad_row = false;
     for (uint32_t i = 0; i < hh.P; i++) {
@@ -798,7 +806,7 @@ int do_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* di
       if (ck < ncum) cum[ck] = cnt; else bad_row = true;
     }
     for (uint64_t t = 1; t < ncum; t++) cum[t] += cum[t - 1];
-    B2D_CU(cudaMemcpyAsync(d->r_diff.p, stage, sizes[idx] + delta, cudaMemcpyHostToDevice, d->stream));
+    B2D_CU(cudaMemcpyAsync(d->r_diff.p + delta, src, sizes[idx], cudaMemcpyHostToDevice, d->stream));
     B2D_CU(cudaMemcpyAsync(d->r_cum.p, cum.data(), sizeof(unsigned long long) * ncum, cudaMemcpyHostToDevice,
                            d->stream));
     if (idx == (int)id) {
@@ -977,6 +985,8 @@ struct b2d_batch {
   };
   std::vector<GraphEntry> graphs;
   size_t graph_cap = 16;
+  int graph_mode = 2;                // 0 direct launches, 1 always a graph, 2 graph from the 2nd sighting
+  std::vector<uint64_t> seen;        // compositions launched directly once
   uint64_t use_clock = 0;
   // the batch in flight (launched, not yet finished)
   bool inflight = false;
@@ -1145,14 +1155,10 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
   b2d_batch::GraphEntry* ge = nullptr;
   for (auto& g : b->graphs)
     if (g.hash == kh && g.key == key) ge = &g;
-  if (!ge) {
-    if (b->graphs.size() >= b->graph_cap) {
-      size_t lru = 0;
-      for (size_t i = 1; i < b->graphs.size(); i++)
-        if (b->graphs[i].last_use < b->graphs[lru].last_use) lru = i;
-      cudaGraphExecDestroy(b->graphs[lru].exec);
-      b->graphs.erase(b->graphs.begin() + (long)lru);
-    }
+
+  // Everything the batch does, enqueued on `main` (the capture stream or the batch stream) and
+  // the side streams: blob upload, init, hashing launches, per-handle branches, collection.
+  auto enqueue_batch = [&](cudaStream_t main, uint32_t& launches) -> int {
     // branch assignment: largest handles first, each to the least loaded branch
     std::vector<uint32_t> order(count);
     for (uint32_t i = 0; i < count; i++) order[i] = i;
@@ -1167,17 +1173,15 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
       load[best] += lens[i] + (1ull << 20);   // fixed per-checkpoint cost ~ 1 MiB of data
       branch[best].push_back(i);
     }
-    cudaGraph_t g = nullptr;
-    B2D_CU(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
     int erc = B2D_OK;
     auto cap_err = [&](cudaError_t e) {
       if (e != cudaSuccess && erc == B2D_OK) erc = cuda_status(e);
     };
-    cap_err(cudaMemcpyAsync(B, H, L.total, cudaMemcpyHostToDevice, b->cap));
-    batch_init_kernel<<<(count + 255) / 256, 256, 0, b->cap>>>(d_states, d_rounds, count, d_queues,
-                                                               (uint32_t)groups.size(), d_bst);
+    cap_err(cudaMemcpyAsync(B, H, L.total, cudaMemcpyHostToDevice, main));
+    batch_init_kernel<<<(count + 255) / 256, 256, 0, main>>>(d_states, d_rounds, count, d_queues,
+                                                             (uint32_t)groups.size(), d_bst);
     cap_err(cudaGetLastError());
-    uint32_t launches = 1;
+    launches = 1;
     LeafTuning lt;
     lt.allow_tma = 1;
     lt.stages = cand.stages;
@@ -1185,10 +1189,10 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
     for (size_t gi = 0; gi < groups.size() && erc == B2D_OK; gi++) {
       const Group& gr = groups[gi];
       cap_err(launch_leaves_batch(d_items + gr.beg, gr.end - gr.beg, gr.tiles, gr.U, gr.kind, d_queues + gi, d_bst,
-                                  b->sm_count, lt, (uint32_t)cand.tiles_per_pop, b->cap));
+                                  b->sm_count, lt, (uint32_t)cand.tiles_per_pop, main));
       launches++;
     }
-    cap_err(cudaEventRecord(b->fork_ev, b->cap));
+    cap_err(cudaEventRecord(b->fork_ev, main));
     for (int j = 0; j < nb && erc == B2D_OK; j++) {
       cudaStream_t s = b->side[j];
       cap_err(cudaStreamWaitEvent(s, b->fork_ev, 0));
@@ -1200,42 +1204,81 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
         launches += d->launches;
       }
       cap_err(cudaEventRecord(b->side_ev[j], s));
-      cap_err(cudaStreamWaitEvent(b->cap, b->side_ev[j], 0));
+      cap_err(cudaStreamWaitEvent(main, b->side_ev[j], 0));
     }
-    batch_collect_kernel<<<(count + 127) / 128, 128, 0, b->cap>>>(d_states, count, b->coll.p);
+    batch_collect_kernel<<<(count + 127) / 128, 128, 0, main>>>(d_states, count, b->coll.p);
     cap_err(cudaGetLastError());
-    cap_err(cudaMemcpyAsync(b->coll_h.p, b->coll.p, sizeof(DevState) * count, cudaMemcpyDeviceToHost, b->cap));
-    cap_err(cudaMemcpyAsync(H + L.bstatus, d_bst, sizeof(DevStatus), cudaMemcpyDeviceToHost, b->cap));
+    cap_err(cudaMemcpyAsync(b->coll_h.p, b->coll.p, sizeof(DevState) * count, cudaMemcpyDeviceToHost, main));
+    cap_err(cudaMemcpyAsync(H + L.bstatus, d_bst, sizeof(DevStatus), cudaMemcpyDeviceToHost, main));
     launches += 1;
-    const cudaError_t ce = cudaStreamEndCapture(b->cap, &g);
-    if (erc != B2D_OK) {
-      if (g) cudaGraphDestroy(g);
-      return erc;
+    return erc;
+  };
+
+  // graph_mode 1: always replay a graph; 2: capture one the second time a composition comes
+  // (a stream of ever-new compositions, like a request loop's, would pay a capture each time)
+  // (the tuner compares graph replays: a direct launch's device time includes host enqueueing)
+  bool use_graph = ge != nullptr || b->graph_mode == 1 || (scoring && b->graph_mode != 0);
+  if (!use_graph && b->graph_mode == 2) {
+    if (std::find(b->seen.begin(), b->seen.end(), kh) != b->seen.end()) {
+      use_graph = true;
+    } else {
+      if (b->seen.size() >= 4 * b->graph_cap) b->seen.erase(b->seen.begin());
+      b->seen.push_back(kh);
     }
-    B2D_CU(ce);
-    cudaGraphExec_t exec = nullptr;
-    const cudaError_t ie = cudaGraphInstantiate(&exec, g, 0);
-    cudaGraphDestroy(g);
-    B2D_CU(ie);
-    const cudaError_t ue = cudaGraphUpload(exec, b->stream);
-    if (ue != cudaSuccess) {
-      cudaGraphExecDestroy(exec);
-      return cuda_status(ue);
-    }
-    b->graphs.emplace_back();
-    ge = &b->graphs.back();
-    ge->key = key;
-    ge->hash = kh;
-    ge->exec = exec;
-    ge->launches = launches;
   }
-  ge->last_use = ++b->use_clock;
-  b->launches = ge->launches;
   b->leaf_groups = (uint32_t)groups.size();
   b->lay = L;
-  B2D_CU(cudaEventRecord(b->ev[0], b->stream));
-  B2D_CU(cudaGraphLaunch(ge->exec, b->stream));
-  B2D_CU(cudaEventRecord(b->ev[1], b->stream));
+  if (!use_graph) {
+    uint32_t launches = 0;
+    B2D_CU(cudaEventRecord(b->ev[0], b->stream));
+    const int erc = enqueue_batch(b->stream, launches);
+    if (erc != B2D_OK) {
+      cudaStreamSynchronize(b->stream);
+      return erc;
+    }
+    B2D_CU(cudaEventRecord(b->ev[1], b->stream));
+    b->launches = launches;
+  } else {
+    if (!ge) {
+      if (b->graphs.size() >= b->graph_cap) {
+        size_t lru = 0;
+        for (size_t i = 1; i < b->graphs.size(); i++)
+          if (b->graphs[i].last_use < b->graphs[lru].last_use) lru = i;
+        cudaGraphExecDestroy(b->graphs[lru].exec);
+        b->graphs.erase(b->graphs.begin() + (long)lru);
+      }
+      cudaGraph_t g = nullptr;
+      uint32_t launches = 0;
+      B2D_CU(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+      const int erc = enqueue_batch(b->cap, launches);
+      const cudaError_t ce = cudaStreamEndCapture(b->cap, &g);
+      if (erc != B2D_OK) {
+        if (g) cudaGraphDestroy(g);
+        return erc;
+      }
+      B2D_CU(ce);
+      cudaGraphExec_t exec = nullptr;
+      const cudaError_t ie = cudaGraphInstantiate(&exec, g, 0);
+      cudaGraphDestroy(g);
+      B2D_CU(ie);
+      const cudaError_t ue = cudaGraphUpload(exec, b->stream);
+      if (ue != cudaSuccess) {
+        cudaGraphExecDestroy(exec);
+        return cuda_status(ue);
+      }
+      b->graphs.emplace_back();
+      ge = &b->graphs.back();
+      ge->key = key;
+      ge->hash = kh;
+      ge->exec = exec;
+      ge->launches = launches;
+    }
+    ge->last_use = ++b->use_clock;
+    b->launches = ge->launches;
+    B2D_CU(cudaEventRecord(b->ev[0], b->stream));
+    B2D_CU(cudaGraphLaunch(ge->exec, b->stream));
+    B2D_CU(cudaEventRecord(b->ev[1], b->stream));
+  }
   b->inflight = true;
   b->fl_handles.assign(hs, hs + count);
   b->fl_bytes = bytes;
@@ -1355,6 +1398,13 @@ int b2d_copy_diff(b2d_dedup* d, void* dst, uint64_t cap) {
     if (!d || !dst) return B2D_ERR_ARG;
     return copy_diff(d, dst, cap);
   })
+}
+
+int b2d_copy_diff_async(b2d_dedup* d, void* dst, uint64_t cap, void* stream) {
+  if (!d || !dst || !d->diff_valid || cap < d->diff_len) return B2D_ERR_ARG;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : d->stream;
+  B2D_CU(cudaMemcpyAsync(dst, d->diff.p + d->diff_delta, d->diff_len, cudaMemcpyDeviceToHost, s));
+  return B2D_OK;
 }
 
 int b2d_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, int make_baseline, const uint8_t** diff,
@@ -1632,6 +1682,7 @@ int b2d_batch_set_param(b2d_batch* b, const char* name, int64_t value) {
   else if (k == "tiles_per_pop" && value >= 1 && value <= 1024) b->cur.tiles_per_pop = (int)value;
   else if (k == "streams" && value >= 1 && value <= 64) b->cur.streams = (int)value;
   else if (k == "graph_cache" && value >= 1 && value <= 4096) b->graph_cap = (size_t)value;
+  else if (k == "graph" && value >= 0 && value <= 2) b->graph_mode = (int)value;
   else if (k == "autotune" && (value == 0 || value == 1)) {
     b->autotune = value != 0;
     b->tuner.reset(b->cur);
@@ -1650,6 +1701,7 @@ int b2d_batch_get_param(b2d_batch* b, const char* name, int64_t* value) {
   else if (k == "tuned") *value = b->tuner.done ? 1 : 0;
   else if (k == "graph_cache") *value = (int64_t)b->graph_cap;
   else if (k == "graphs") *value = (int64_t)b->graphs.size();
+  else if (k == "graph") *value = b->graph_mode;
   else return B2D_ERR_ARG;
   return B2D_OK;
 }

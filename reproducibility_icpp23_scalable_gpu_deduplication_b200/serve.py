@@ -14,7 +14,9 @@ clients submit "checkpoint my device buffer now" requests as they arrive.  The l
   soon as a batch slot is free, while the batches already launched keep running on their own
   streams: requests that arrive during a batch join the next one (continuous batching), and up
   to ``max_inflight`` batches overlap on the device;
-* completes a batch when its device work is done and stamps each request's completion time.
+* completes a batch when its device work is done and stamps each request's completion time; with
+  ``enable_host_copy`` a request completes once its diff has been copied back to pinned host
+  memory (the copies of a batch run on its slot's stream while later batches compute).
 
 A client has at most one request in flight; its later requests wait in arrival order.  Each
 request's diff is exactly what its client's handle gives when it checkpoints the same buffers
@@ -35,7 +37,7 @@ __all__ = ["CheckpointServer", "Request"]
 
 class Request:
     __slots__ = ("client", "buffer", "nbytes", "make_baseline", "arrival", "admitted", "launched", "done", "rc",
-                 "diff_len", "checksum", "ready", "seq")
+                 "diff_len", "checksum", "ready", "seq", "host")
 
     def __init__(self, client, buffer, make_baseline, arrival, seq):
         self.client, self.buffer, self.make_baseline, self.arrival, self.seq = client, buffer, make_baseline, arrival, seq
@@ -45,6 +47,7 @@ class Request:
         self.diff_len = None
         self.checksum = None
         self.ready = None
+        self.host = None          # the diff in pinned host memory (with enable_host_copy)
 
     @property
     def latency(self):
@@ -52,7 +55,7 @@ class Request:
 
 
 class _Client:
-    __slots__ = ("handle", "reserved", "last_use", "busy", "pending", "outstanding")
+    __slots__ = ("handle", "reserved", "last_use", "busy", "pending", "outstanding", "host")
 
     def __init__(self):
         self.handle = None
@@ -61,14 +64,15 @@ class _Client:
         self.busy = False                     # a request of this client is in a launched batch
         self.pending = collections.deque()   # admitted, not launched
         self.outstanding = 0                 # submitted, not completed
+        self.host = None                     # pinned buffer for diff copy-back
 
 
 class CheckpointServer:
     def __init__(self, hbm_budget=150e9, chunk_size=128, hash_kind=HASH_MURMUR3, max_batch=64, max_inflight=2,
                  evict=True, plain=False, checksum=False, clock=time.perf_counter, map_reserve=0, **batch_params):
-        """`map_reserve`: bytes of device memory mapped up front for digest-map growth
-        (``reserve_map_memory``), so a client whose map grows does not pay for fresh driver
-        allocations inside its request; released by ``close``."""
+        """`map_reserve`: bytes of device memory kept mapped for digest maps
+        (``reserve_growth``), so a client whose map grows does not pay for fresh driver
+        allocations (tens of ms per GB) inside its request; released by ``close``."""
         import torch
 
         self.budget = int(hbm_budget)
@@ -80,13 +84,15 @@ class CheckpointServer:
         self.resident = 0                        # bytes reserved by resident clients
         self.peak_resident = 0
         self.completed = []
+        self.copying = []                        # (event, requests) whose diffs are being copied back
+        self.to_host = False
         self.batches = 0
         self.seq = 0
         params = {"graph_cache": 256}
         params.update(batch_params)
-        self.map_reserve = int(map_reserve)
-        if self.map_reserve:
-            reserve_map_memory(self.map_reserve)
+        self.map_reserve = 0
+        if map_reserve:
+            self.reserve_growth(map_reserve)
         self.slots = [] if plain else [
             (CheckpointBatch(**params), torch.cuda.Stream(), []) for _ in range(max(1, int(max_inflight)))]
 
@@ -105,6 +111,13 @@ class CheckpointServer:
         self.clients[client].outstanding += 1
         return r
 
+    def reserve_growth(self, nbytes):
+        """Map `nbytes` of unused device memory for digest maps now.  New clients' baseline maps
+        are carved from it too, so a server calls this once its clients are resident (after their
+        first requests) to keep the memory for later map growth."""
+        reserve_map_memory(int(nbytes))
+        self.map_reserve = int(nbytes)
+
     def busy(self, client):
         """True while a request of `client` is not completed (its buffer must stay unchanged)."""
         c = self.clients.get(client)
@@ -112,7 +125,7 @@ class CheckpointServer:
 
     def idle(self):
         return (not self.waiting and not any(c.pending for c in self.clients.values())
-                and not any(reqs for _, _, reqs in self.slots))
+                and not any(reqs for _, _, reqs in self.slots) and not self.copying)
 
     def close(self):
         for b, _, reqs in self.slots:
@@ -226,18 +239,58 @@ class CheckpointServer:
         r.buffer = None
         self.completed.append(r)
 
+    def _host_buffer(self, c, n):
+        import torch
+
+        if c.host is None or c.host.numel() < n:
+            c.host = torch.empty(int(n * 1.25) + 4096, dtype=torch.uint8, pin_memory=True)
+        return c.host
+
+    def enable_host_copy(self, sizes=None, fraction=0.25):
+        """From now on a request completes when its diff is in pinned host memory (``Request.host``,
+        a view of the client's buffer, valid until its next request completes).  `sizes`
+        (client -> buffer bytes) pre-allocates each client's pinned buffer at `fraction` of it."""
+        self.to_host = True
+        for cid, nbytes in (sizes or {}).items():
+            self._host_buffer(self.clients[cid], int(nbytes * fraction))
+
     def _complete(self):
+        import torch
+
         out = []
-        for b, _, reqs in self.slots:
+        for b, stream, reqs in self.slots:
             if not reqs or not b.done():
                 continue
             rcs = b.wait(check_status=False)
             now = self.clock()
-            for r, rc in zip(reqs, rcs):
-                r.done = now
-                self._finish(r, rc)
-                out.append(r)
+            if self.to_host:
+                # copy the diffs back on the slot's stream; the requests complete when that lands
+                for r, rc in zip(reqs, rcs):
+                    r.rc = rc
+                    if rc == 0:
+                        h = self.clients[r.client].handle
+                        buf = self._host_buffer(self.clients[r.client], h.diff_device()[1])
+                        r.host = buf[:h.copy_diff_async(buf, stream)]
+                ev = torch.cuda.Event()
+                ev.record(stream)
+                self.copying.append((ev, list(reqs)))
+            else:
+                for r, rc in zip(reqs, rcs):
+                    r.done = now
+                    self._finish(r, rc)
+                    out.append(r)
             reqs.clear()
+        keep = []
+        for ev, reqs in self.copying:
+            if ev.query():
+                now = self.clock()
+                for r in reqs:
+                    r.done = now
+                    self._finish(r, r.rc)
+                    out.append(r)
+            else:
+                keep.append((ev, reqs))
+        self.copying = keep
         return out
 
     def _step_plain(self):
@@ -257,6 +310,9 @@ class CheckpointServer:
             c.handle.checkpoint_device(nxt.buffer, nxt.make_baseline)
         except Exception as e:   # noqa: BLE001 - the status travels with the request
             rc = getattr(e, "code", -8)
+        if rc == 0 and self.to_host:
+            buf = self._host_buffer(c, c.handle.diff_device()[1])
+            nxt.host = buf[:len(c.handle.copy_diff(buf.numpy()))]
         nxt.done = self.clock()
         self._finish(nxt, rc)
         self.batches += 1

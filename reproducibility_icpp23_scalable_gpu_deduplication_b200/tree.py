@@ -36,6 +36,16 @@ def _stream_handle():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream or 1)
 
 
+def _host_bytes(c):
+    """A diff as a uint8 numpy view without copying when it already is one (pinned memory stays
+    pinned, so the library copies it to the device directly)."""
+    if isinstance(c, np.ndarray) and c.dtype == np.uint8 and c.flags.c_contiguous:
+        return c
+    if isinstance(c, (bytes, bytearray, memoryview)):
+        return np.frombuffer(c, dtype=np.uint8)
+    return np.frombuffer(bytes(c), dtype=np.uint8)
+
+
 def parse_header(diff):
     """header_t (include/utils.hpp:29-37) of a diff as a dict."""
     h = np.frombuffer(bytes(diff[:HEADER_BYTES]), dtype=np.uint32)
@@ -102,6 +112,19 @@ class TreeDeduplicator:
         check(lib().b2d_copy_diff(self._h, ctypes.c_void_p(buf.ctypes.data), buf.nbytes), "b2d_copy_diff")
         return buf[:n]
 
+    def copy_diff_async(self, out, stream=None):
+        """Enqueue the copy of the last diff into `out` (a pinned uint8 tensor or array) on `stream`
+        (a torch.cuda.Stream; default the handle's) and return the diff length; the bytes are
+        there once that stream reaches the copy."""
+        _, n = self.diff_device()
+        if hasattr(out, "data_ptr"):
+            ptr, cap = out.data_ptr(), out.numel() * out.element_size()
+        else:
+            ptr, cap = out.ctypes.data, out.nbytes
+        sh = ctypes.c_void_p(stream.cuda_stream if stream is not None else None)
+        check(lib().b2d_copy_diff_async(self._h, ctypes.c_void_p(ptr), cap, sh), "b2d_copy_diff_async")
+        return n
+
     def checkpoint(self, data, make_baseline=False, filename=None, logname=None):
         """checkpoint(data_ptr, len, diff_h[, logname], make_baseline) / (.., filename, logname, ..).
 
@@ -126,7 +149,7 @@ class TreeDeduplicator:
     def restart(self, out, chkpts, chkpt_id, logname=None, check_status=True):
         self._sync_stream()
         p, n = _dev_ptr(out)
-        bufs = [np.frombuffer(bytes(c), dtype=np.uint8) for c in chkpts]
+        bufs = [_host_bytes(c) for c in chkpts]
         ptrs = (ctypes.c_void_p * len(bufs))(*[b.ctypes.data for b in bufs])
         sizes = (ctypes.c_uint64 * len(bufs))(*[b.size for b in bufs])
         rc = lib().b2d_restart(self._h, p, n, ptrs, sizes, len(bufs), int(chkpt_id),

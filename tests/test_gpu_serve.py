@@ -120,3 +120,26 @@ def test_served_diff_header(cuda):
         assert hdr["chkpt_id"] == 1 and hdr["ref_id"] == 0
     assert all(r.rc == 0 for r in reqs.values())
     srv.close()
+
+
+def test_served_diffs_copied_to_host(cuda):
+    """with host copy-back, a request completes with its diff in pinned host memory, byte-equal
+    to the diff of the same client's buffers checkpointed alone"""
+    rounds = 3
+    sizes = SIZES[:4]
+    for plain in (False, True):
+        srv = CheckpointServer(hbm_budget=8e9, max_batch=4, max_inflight=2, plain=plain)
+        srv.enable_host_copy({c: n for c, n in enumerate(sizes)})
+        reqs = drive(srv, sizes, rounds, order_seed=4)
+        got = {k: bytes(r.host.numpy() if hasattr(r.host, "numpy") else r.host) for k, r in reqs.items()}
+        srv.close()
+        for c, n in enumerate(sizes):
+            s = synth.DeviceSeries(n, 128, c, max_run=64)
+            h = TreeDeduplicator(128)
+            for k in range(rounds):
+                h.checkpoint_device(s.next(), k == 0)
+                # each request's host view stays valid until the client's next request completes:
+                # only the last one per client is still intact here
+                if k == rounds - 1:
+                    assert got[(c, k)] == bytes(h.copy_diff()), (plain, c, k)
+            h.close()
