@@ -53,6 +53,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--leaf-stages", type=int, default=0, help="TMA ring depth (0 = library default)")
     p.add_argument("--leaf-ctas", type=int, default=0, help="hashing CTAs per SM (0 = library default)")
+    p.add_argument("--leaf-unit", type=int, default=0, help="staged segment width (0 = library default)")
     p.add_argument("--form", default="plain", choices=["plain", "batched", "served"],
                    help="plain: one 4 GiB buffer (default); batched: 256 uneven buffers per step through "
                         "b2d_batch_checkpoint vs one at a time; served: Poisson request loop")
@@ -509,6 +510,8 @@ def main():
         dd.set_param("leaf_stages", args.leaf_stages)
     if args.leaf_ctas:
         dd.set_param("leaf_ctas_per_sm", args.leaf_ctas)
+    if args.leaf_unit:
+        dd.set_param("leaf_unit", args.leaf_unit)
     if args.graph is not None:
         dd.set_param("graph", args.graph)
     dd.checkpoint_device(series.next(), make_baseline=True)          # checkpoint 0: baseline

@@ -67,6 +67,8 @@ int b2d_set_stream(b2d_dedup* d, void* cuda_stream);
  *   "leaf_tma"          1 = TMA-staged chunk hashing when the chunk size allows (default), 0 = off
  *   "leaf_stages"       TMA ring depth per CTA, 2..16 (0 = default)
  *   "leaf_ctas_per_sm"  resident hashing CTAs per SM, 1..8 (0 = default 3)
+ *   "leaf_unit"         staged segment width 16/32/64/128 bytes, narrower than the default only
+ *                       (0 = the largest that divides the chunk; MD5 needs >= 64)
  *   "map_max_load_pct"  digest-map load limit, 10..90 (default 75): a checkpoint starts only
  *                       when the map's entries plus every node of the tree fit under it
  *   "map_headroom_pct"  size of a baseline's map over that minimum, 100..1000 (default 200);
@@ -219,6 +221,10 @@ int b2d_batch_wait(b2d_batch* b, int* rcs);
  * seconds from the start of its launch to the end of its completion */
 int b2d_batch_times(b2d_batch* b, double out[2]);
 int b2d_batch_launch_count(b2d_batch* b, uint32_t* out);
+
+/* The same digest of a host buffer, computed on the host (for tools that print the
+ * reference's checkpoint digests, include/hash_functions.hpp:47-63).  No device work. */
+int b2d_hash_host(int hash_kind, const void* data, uint64_t len, void* out16);
 
 const char* b2d_strerror(int status);
 

@@ -37,15 +37,39 @@ def _stale():
     return any(os.path.getmtime(p) > t for p in deps if os.path.exists(p))
 
 
+CLI_DIR = os.path.join(PKG_DIR, "cli")
+INCLUDE = os.path.join(PKG_DIR, "..", "include")
+# argv-compatible drivers of the reference's checkpoint-file tools, linked against the library
+TOOLS = {"dedup_files": "dedup_files.cpp", "restart_chkpt_files": "restart_chkpt_files.cpp"}
+
+
+def tool_path(name):
+    return os.path.join(PKG_DIR, name)
+
+
+def build_tools(force=False, verbose=False):
+    for name, src in TOOLS.items():
+        out, srcp = tool_path(name), os.path.join(CLI_DIR, src)
+        deps = [srcp, LIB_PATH, os.path.join(INCLUDE, "b200dedup.h"), os.path.join(INCLUDE, "b200dedup_tree.hpp")]
+        if not force and os.path.exists(out) and all(os.path.getmtime(d) <= os.path.getmtime(out) for d in deps):
+            continue
+        cmd = [_nvcc(), "-O2", "-std=c++17", "-Wno-deprecated-gpu-targets", "-I", INCLUDE, "-o", out + ".tmp", srcp, "-L", PKG_DIR, "-lb200dedup",
+               "-Xlinker", "-rpath", "-Xlinker", "$ORIGIN"]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True, cwd=CLI_DIR)
+        os.replace(out + ".tmp", out)
+
+
 def build(force=False, verbose=False):
-    if not force and not _stale():
-        return LIB_PATH
-    tmp = LIB_PATH + ".tmp"
-    cmd = [_nvcc()] + NVCC_FLAGS + ["-o", tmp] + sources()
-    if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True, cwd=CSRC)
-    os.replace(tmp, LIB_PATH)
+    if force or _stale():
+        tmp = LIB_PATH + ".tmp"
+        cmd = [_nvcc()] + NVCC_FLAGS + ["-o", tmp] + sources()
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True, cwd=CSRC)
+        os.replace(tmp, LIB_PATH)
+    build_tools(force, verbose)
     return LIB_PATH
 
 

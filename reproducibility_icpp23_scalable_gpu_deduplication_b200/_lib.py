@@ -66,6 +66,7 @@ SIGNATURES = [
     ("b2d_batch_wait", _int, [_vp, ctypes.POINTER(_int)]),
     ("b2d_batch_times", _int, [_vp, ctypes.POINTER(ctypes.c_double)]),
     ("b2d_batch_launch_count", _int, [_vp, ctypes.POINTER(_u32)]),
+    ("b2d_hash_host", _int, [_int, _vp, _u64, _vp]),
     ("b2d_strerror", ctypes.c_char_p, [_int]),
 ]
 

@@ -486,6 +486,7 @@ void graph_key(const b2d_dedup* d, const RoundState* rs_dev, std::vector<uint64_
             (uint64_t)d->bucket_start.p, (uint64_t)d->partial.p, (uint64_t)d->partial2.p, (uint64_t)d->diff.p,
             (uint64_t)d->state.p, (uint64_t)d->state_h.p, (uint64_t)d->round_h.p, (uint64_t)rs_dev, d->bcap,
             (uint64_t)d->tune.allow_tma, (uint64_t)d->tune.stages, (uint64_t)d->tune.ctas_per_sm, (uint64_t)d->graph_timing,
+            (uint64_t)d->tune.unit,
             (uint64_t)d->sm_count});
 }
 
@@ -1492,6 +1493,8 @@ int b2d_set_param(b2d_dedup* d, const char* name, int64_t value) {
   if (k == "leaf_tma") d->tune.allow_tma = value != 0;
   else if (k == "leaf_stages" && value >= 0 && value <= 16) d->tune.stages = (int)value;
   else if (k == "leaf_ctas_per_sm" && value >= 0 && value <= 8) d->tune.ctas_per_sm = (int)value;
+  else if (k == "leaf_unit" && (value == 0 || value == 16 || value == 32 || value == 64 || value == 128))
+    d->tune.unit = (int)value;
   else if (k == "map_max_load_pct" && value >= 10 && value <= 90) d->map_max_load = value / 100.0;
   else if (k == "map_headroom_pct" && value >= 100 && value <= 1000) d->map_headroom = value / 100.0;
   else if (k == "graph" && value >= 0 && value <= 2) {
@@ -1562,6 +1565,13 @@ int b2d_debug_labels(b2d_dedup* d, void* dst, uint64_t leaves) {
   B2D_CU(cudaStreamSynchronize(d->stream));
   return B2D_OK;
 }
+int b2d_hash_host(int kind, const void* data, uint64_t len, void* out16) {
+  if ((!data && len) || !out16 || (kind != HASH_MURMUR3 && kind != HASH_MD5)) return B2D_ERR_ARG;
+  const Digest dg = hash_bytes(kind, static_cast<const uint8_t*>(data), len);
+  std::memcpy(out16, dg.w, 16);
+  return B2D_OK;
+}
+
 int b2d_hash_chunks(int kind, const void* d_data, uint64_t len, uint32_t cs, void* d_out, void* stream) {
   if (!d_data || !d_out || cs == 0 || len == 0) return B2D_ERR_ARG;
   const uint64_t n = (len + cs - 1) / cs;

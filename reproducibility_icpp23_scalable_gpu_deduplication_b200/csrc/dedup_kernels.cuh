@@ -120,6 +120,7 @@ struct LeafTuning {
   int allow_tma = 1;
   int stages = 0;        // TMA ring depth per CTA (default: a 64 KB ring)
   int ctas_per_sm = 0;   // resident CTAs per SM (default 3)
+  int unit = 0;          // staged segment width in bytes (0: the largest of 128/64/32/16 dividing the chunk)
 };
 int launch_leaves(const LeafArgs& a, int sm_count, const LeafTuning& tune, cudaStream_t stream);
 

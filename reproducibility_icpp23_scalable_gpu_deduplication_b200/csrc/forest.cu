@@ -30,6 +30,14 @@
 
 namespace b2d {
 
+// resident CTAs per SM the band kernels are compiled for (register budget)
+#ifndef B2D_FF_MINB
+#define B2D_FF_MINB 1
+#endif
+#ifndef B2D_FAST_MINB
+#define B2D_FAST_MINB 1
+#endif
+
 constexpr uint32_t FOREST_THREADS = 512;
 constexpr uint32_t FAST_THREADS = 256;
 constexpr uint32_t FAST_LEVELS = 12;      // 4 in-thread + 5 warp + 3 CTA
@@ -195,7 +203,7 @@ __device__ __forceinline__ Digest shfl_down_digest(const Digest& d, uint32_t del
   return r;
 }
 
-__global__ void __launch_bounds__(FAST_THREADS) forest_first_kernel(ForestArgs a0, uint32_t in) {
+__global__ void __launch_bounds__(FAST_THREADS, B2D_FF_MINB) forest_first_kernel(ForestArgs a0, uint32_t in) {
   const ForestArgs a = with_round(a0);
   __shared__ uint32_t ff[FF_WORDS];
   __shared__ uint32_t wbit[FAST_THREADS / 32];
@@ -342,7 +350,7 @@ __global__ void __launch_bounds__(FAST_THREADS) forest_first_kernel(ForestArgs a
 
 // Fast band: inputs at level `in`, outputs at level in - 12.
 template <int PHASE>
-__global__ void __launch_bounds__(FAST_THREADS) forest_fast_kernel(ForestArgs a0, uint32_t in) {
+__global__ void __launch_bounds__(FAST_THREADS, B2D_FAST_MINB) forest_fast_kernel(ForestArgs a0, uint32_t in) {
   const ForestArgs a = with_round(a0);
   __shared__ uint8_t wlab[FAST_THREADS / 32];
   const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;

@@ -161,16 +161,16 @@ __host__ __device__ __forceinline__ Digest md5_digest(const uint32_t st[4]) {
 // ---------------------------------------------------------------- byte-granular hashing
 // Used for chunk sizes or alignments the staged kernels do not cover and for the short
 // last chunk.  Reads bytes, so it works for any address and length.
-__device__ __forceinline__ uint32_t ld_le32_bytes(const uint8_t* p) {
+__host__ __device__ __forceinline__ uint32_t ld_le32_bytes(const uint8_t* p) {
   return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
 }
-__device__ __forceinline__ uint32_t ld_le32_partial(const uint8_t* p, uint64_t avail) {
+__host__ __device__ __forceinline__ uint32_t ld_le32_partial(const uint8_t* p, uint64_t avail) {
   uint32_t v = 0;
   for (unsigned i = 0; i < 4 && i < avail; i++) v |= (uint32_t)p[i] << (8 * i);
   return v;
 }
 
-__device__ inline Digest hash_bytes_murmur3(const uint8_t* p, uint64_t len) {
+__host__ __device__ inline Digest hash_bytes_murmur3(const uint8_t* p, uint64_t len) {
   Murmur3 h;
   h.init();
   const uint64_t nb = len / 16;
@@ -197,7 +197,7 @@ __device__ inline Digest hash_bytes_murmur3(const uint8_t* p, uint64_t len) {
   return h.finish(len);
 }
 
-__device__ inline Digest hash_bytes_md5(const uint8_t* p, uint64_t len) {
+__host__ __device__ inline Digest hash_bytes_md5(const uint8_t* p, uint64_t len) {
   uint32_t st[4];
   md5_init(st);
   const uint64_t nb = len / 64;
@@ -236,7 +236,7 @@ __device__ inline Digest hash_bytes_md5(const uint8_t* p, uint64_t len) {
   return md5_digest(st);
 }
 
-__device__ __forceinline__ Digest hash_bytes(int kind, const uint8_t* p, uint64_t len) {
+__host__ __device__ __forceinline__ Digest hash_bytes(int kind, const uint8_t* p, uint64_t len) {
   return kind == HASH_MD5 ? hash_bytes_md5(p, len) : hash_bytes_murmur3(p, len);
 }
 

@@ -498,7 +498,11 @@ cudaError_t launch_leaves_batch(const BatchLeafItem* d_items, uint32_t nitems, u
 // Returns 1 if the staged TMA path was used, 0 for the generic path, negative on error.
 int launch_leaves(const LeafArgs& a, int sm_count, const LeafTuning& tune, cudaStream_t stream) {
   const uint32_t nfull = (uint32_t)(a.len / a.cs);
-  const int U = choose_unit(a.cs, a.kind);
+  int U = choose_unit(a.cs, a.kind);
+  // a narrower requested unit (must divide the chunk; MD5 needs whole 64-byte blocks)
+  if (U > 0 && tune.unit > 0 && tune.unit < U && a.cs % (uint32_t)tune.unit == 0 &&
+      (a.kind != HASH_MD5 || tune.unit >= 64))
+    U = tune.unit;
   const bool aligned = (reinterpret_cast<uintptr_t>(a.data) & 15u) == 0;
   CUtensorMap map;
   if (tune.allow_tma && U > 0 && aligned && nfull > 0) {

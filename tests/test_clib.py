@@ -58,3 +58,37 @@ def test_no_oracle_in_product():
             if f.endswith((".py", ".cu", ".cuh", ".h", ".cpp")):
                 txt = open(os.path.join(dirpath, f), errors="ignore").read()
                 assert "import oracle" not in txt and "from oracle" not in txt, f
+
+
+def test_host_digest_matches_reference_vectors():
+    """b2d_hash_host (the library's own Murmur3 variant and MD5, run on the host) against the
+    digests the reference's hash headers produced (tests/golden/hash_kat.json)"""
+    import json
+
+    with open(os.path.join(ROOT, "tests", "golden", "hash_kat.json")) as f:
+        kat = json.load(f)["kat"]
+    L = _lib.lib()
+    out = ctypes.create_string_buffer(16)
+    for e in kat:
+        data = bytes.fromhex(e["data"])
+        buf = ctypes.create_string_buffer(data, max(1, len(data)))
+        for kind, key in ((_lib.HASH_MURMUR3, "murmur3"), (_lib.HASH_MD5, "md5")):
+            assert L.b2d_hash_host(kind, buf, len(data), out) == 0
+            assert out.raw.hex() == e[key], (key, e["len"])
+    assert L.b2d_hash_host(7, buf, 1, out) != 0
+
+
+def test_file_tools_build_and_check_arguments():
+    """the argv-compatible file tools build with the library and reject what is not built here
+    before touching a GPU"""
+    _build.build()
+    for name in _build.TOOLS:
+        assert os.path.exists(_build.tool_path(name))
+    r = subprocess.run([_build.tool_path("dedup_files")], capture_output=True, text=True)
+    assert r.returncode == 1 and "usage" in r.stderr
+    r = subprocess.run([_build.tool_path("dedup_files"), "128", "1", "--run-list-chkpt", "x"],
+                       capture_output=True, text=True)
+    assert r.returncode == 2 and "only --run-tree-chkpt" in r.stderr
+    r = subprocess.run([_build.tool_path("restart_chkpt_files"), "0", "1", "1", "128", "--run-full-chkpt", "x"],
+                       capture_output=True, text=True)
+    assert r.returncode == 2
