@@ -30,9 +30,11 @@
 
 namespace b2d {
 
-// resident CTAs per SM the band kernels are compiled for (register budget)
+// resident CTAs per SM the band kernels are compiled for (register budget): phase 1 at 8
+// (32 registers) measured ~6% faster on its launches than the unconstrained 40 registers;
+// the phase-2 band gained nothing from a tighter budget
 #ifndef B2D_FF_MINB
-#define B2D_FF_MINB 1
+#define B2D_FF_MINB 8
 #endif
 #ifndef B2D_FAST_MINB
 #define B2D_FAST_MINB 1

@@ -29,13 +29,15 @@ def to_dev(a):
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
 
 
-def run_both(bufs, cs, kind=HASH_MURMUR3, baselines=None, restart=True, tma=True):
+def run_both(bufs, cs, kind=HASH_MURMUR3, baselines=None, restart=True, tma=True, params=None):
     """checkpoint every buffer on the GPU and in the oracle; assert identical diffs and restarts"""
     import torch
 
     g = TreeDeduplicator(cs, kind)
     if not tma:
         g.set_param("leaf_tma", 0)
+    for k, v in (params or {}).items():
+        g.set_param(k, v)
     o = O.OracleTreeDeduplicator(cs, kind)
     gd, od = [], []
     for i, b in enumerate(bufs):
@@ -53,6 +55,7 @@ def run_both(bufs, cs, kind=HASH_MURMUR3, baselines=None, restart=True, tma=True
             grc = g.restart(out, gd, i, check_status=False)
             assert (grc == 0) == (rc == 0), (i, grc, rc)
             assert out.cpu().numpy().tobytes() == want.tobytes(), i
+    run_both.map_stats = g.map_stats()
     g.close()
     return gd
 
@@ -168,3 +171,22 @@ def test_md5_float_series(cuda):
     s = synth.FloatSeries(64 << 20)
     bufs = [s.next().copy() for _ in range(4)]
     run_both(bufs, 256, HASH_MD5)
+
+
+def test_map_growth_keeps_output(cuda):
+    """a map with minimal headroom and a low load limit grows (allocate + rehash) during the
+    series; diffs and restarts stay identical to the oracle, also with CUDA-graph replay"""
+    s = synth.varied(4 << 20, 128, max_run=256, config_id=4, buf_id=3)
+    bufs = [s.next().copy() for _ in range(8)]
+    for graph in (0, 1):
+        run_both(bufs, 128, params={"map_headroom_pct": 100, "map_max_load_pct": 30, "graph": graph})
+        slots, entries, grows, _, _ = run_both.map_stats
+        assert grows >= 1 and entries <= 0.3 * slots
+
+
+@pytest.mark.parametrize("unit", [16, 32, 64])
+def test_narrow_staging_units(cuda, unit):
+    """the staged hashing kernel with segments narrower than the chunk allows"""
+    s = synth.plain_64m(nbytes=8 << 20)
+    bufs = [s.next().copy() for _ in range(3)]
+    run_both(bufs, 128, params={"leaf_unit": unit})
