@@ -202,8 +202,9 @@ int b2d_batch_set_stream(b2d_batch* b, void* cuda_stream);
  * incremental batch -- six batches -- measured by device time; "tuned" reads 1 once it has
  * settled and the knobs then read the chosen values), "graph" (2 = launch a composition directly
  * the first time and as a captured graph from its second batch on, default; 1 = always a graph;
- * 0 = never), "graph_cache" (instantiated graphs kept, one per batch composition, default 16).
- * Output never depends on them. */
+ * 0 = never), "graph_cache" (instantiated graphs kept, one per batch composition, default 16),
+ * "batch_diff" (1 = every handle's diff assembly in 12-13 shared launches after all trees are
+ * labelled, default; 0 = per handle in its own branch).  Output never depends on them. */
 int b2d_batch_set_param(b2d_batch* b, const char* name, int64_t value);
 int b2d_batch_get_param(b2d_batch* b, const char* name, int64_t* value);
 int b2d_batch_checkpoint(b2d_batch* b, b2d_dedup* const* handles, const void* const* d_data, const uint64_t* lens,

@@ -494,8 +494,18 @@ void graph_key(const b2d_dedup* d, const RoundState* rs_dev, std::vector<uint64_
 // RoundState; with `upload` the host copy (pinned) is copied there first.  `managed`: a batch
 // clears the DevState, writes the RoundState and reads the DevState back for all its handles
 // at once (and may have hashed the leaves already: `skip_leaves`).
+DiffArgs diff_args(b2d_dedup* d, const RoundState* rs_dev) {
+  MapView m;
+  map_view(d, m);
+  DevState* ds = d->state.p;
+  return DiffArgs{static_cast<const uint8_t*>(d->data), d->data_len, d->chunk_size, d->n, d->N, d->D, 0, 0,
+                  d->tree.p, d->push.p, m, &ds->status, &ds->meta, d->first_list.p, d->shift_list.p, d->tmp_first.p,
+                  d->tmp_shift.p, d->levels.p, d->region_off.p, d->sprev.p, d->skey.p, d->hist.p, d->bucket_start.p,
+                  d->partial.p, d->partial2.p, d->diff.p, rs_dev};
+}
+
 int enqueue_checkpoint(b2d_dedup* d, cudaStream_t s, RoundState* rs_dev, bool upload, bool timing, bool skip_leaves,
-                       bool managed = false) {
+                       bool managed = false, bool skip_diff = false) {
   MapView m;
   map_view(d, m);
   DevState* ds = d->state.p;
@@ -518,15 +528,12 @@ int enqueue_checkpoint(b2d_dedup* d, cudaStream_t s, RoundState* rs_dev, bool up
   B2D_CU(launch_zero_exists(&ds->zero_exists, rs_dev, s));
   B2D_CU(launch_forest(fa, 2, s));
   if (timing) B2D_CU(record_timing(d->ev[1], s));
-  // collect_diff (:511-710)
-  DiffArgs ga{static_cast<const uint8_t*>(d->data), d->data_len, d->chunk_size, d->n, d->N, d->D, 0, 0,
-              d->tree.p, d->push.p, m, &ds->status, &ds->meta, d->first_list.p, d->shift_list.p, d->tmp_first.p,
-              d->tmp_shift.p, d->levels.p, d->region_off.p, d->sprev.p, d->skey.p, d->hist.p, d->bucket_start.p,
-              d->partial.p, d->partial2.p, d->diff.p, rs_dev};
-  B2D_CU(launch_collect_diff(ga, d->bcap, d->sm_count, s));
+  // collect_diff (:511-710); a batch may assemble all its handles' diffs in shared launches
+  if (!skip_diff) B2D_CU(launch_collect_diff(diff_args(d, rs_dev), d->bcap, d->sm_count, s));
   if (timing) B2D_CU(record_timing(d->ev[2], s));
   if (!managed) B2D_CU(cudaMemcpyAsync(d->state_h.p, d->state.p, sizeof(DevState), cudaMemcpyDeviceToHost, s));
-  d->launches = (skip_leaves ? 0 : 1) + forest_launch_count(d->D, 1) + forest_launch_count(d->D, 2) + 1 + 14;
+  d->launches = (skip_leaves ? 0 : 1) + forest_launch_count(d->D, 1) + forest_launch_count(d->D, 2) + 1 +
+                (skip_diff ? 0 : 14);
   return B2D_OK;
 }
 
@@ -958,8 +965,11 @@ struct BatchTuner {
 };
 
 struct BatchLayout {
-  size_t items = 0, rounds = 0, states = 0, queues = 0, bstatus = 0, total = 0;
+  size_t items = 0, rounds = 0, states = 0, queues = 0, bstatus = 0, dargs = 0, dtab = 0, total = 0;
 };
+// u32 tables of the shared diff assembly, each n (+1) long, in this order in the blob
+enum DiffTable { DT_G, DT_GS, DT_BCAP, DT_ONE, DT_BEG_G, DT_BEG_GL, DT_BEG_GP, DT_BEG_GS, DT_BEG_GATHER, DT_COUNT };
+constexpr int DIFF_TABLES = DT_BEG_GATHER + GATHER_VARIANTS;
 
 }  // namespace
 
@@ -987,6 +997,7 @@ struct b2d_batch {
   std::vector<GraphEntry> graphs;
   size_t graph_cap = 16;
   int graph_mode = 2;                // 0 direct launches, 1 always a graph, 2 graph from the 2nd sighting
+  bool batch_diff = true;            // all handles' diff assembly in shared segmented launches
   std::vector<uint64_t> seen;        // compositions launched directly once
   uint64_t use_clock = 0;
   // the batch in flight (launched, not yet finished)
@@ -1122,7 +1133,10 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
   L.states = align_up(L.rounds + sizeof(RoundState) * count, 64);
   L.queues = align_up(L.states + sizeof(DevState*) * count, 64);
   L.bstatus = align_up(L.queues + sizeof(unsigned int) * (groups.size() + 1), 64);
-  L.total = align_up(L.bstatus + sizeof(DevStatus), 256);
+  L.dargs = align_up(L.bstatus + sizeof(DevStatus), 64);
+  L.dtab = align_up(L.dargs + (b->batch_diff ? sizeof(DiffArgs) * count : 0), 64);
+  const size_t tab_len = (size_t)count + 1;   // entries per table
+  L.total = align_up(L.dtab + (b->batch_diff ? sizeof(uint32_t) * tab_len * DIFF_TABLES : 0), 256);
   B2D_CU(b->blob.reserve(L.total));
   B2D_CU(b->blob_h.reserve(L.total));
   B2D_CU(b->coll.reserve(count));
@@ -1135,6 +1149,59 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
     std::memcpy(H + L.states + sizeof(DevState*) * i, &p, sizeof(p));
   }
   uint8_t* B = b->blob.p;
+  // shared diff assembly: every handle's DiffArgs, grid sizes and the CTA offset tables
+  DiffBatch dplan{};
+  if (b->batch_diff) {
+    auto tab = [&](int t) { return reinterpret_cast<uint32_t*>(H + L.dtab) + (size_t)t * tab_len; };
+    auto dtab = [&](int t) { return reinterpret_cast<const uint32_t*>(B + L.dtab) + (size_t)t * tab_len; };
+    uint32_t tot_g = 0, tot_gl = 0, tot_gp = 0, tot_gs = 0, tot_v[GATHER_VARIANTS] = {0};
+    uint32_t max_bcap = 1;
+    for (uint32_t i = 0; i < count; i++) {
+      b2d_dedup* d = hs[i];
+      const DiffArgs da = diff_args(d, &d->state.p->round);
+      std::memcpy(H + L.dargs + sizeof(DiffArgs) * i, &da, sizeof(da));
+      const DiffGrids dg = diff_grids(da, b->sm_count);
+      tab(DT_G)[i] = dg.g;
+      tab(DT_GS)[i] = dg.gs;
+      tab(DT_BCAP)[i] = d->bcap;
+      max_bcap = std::max(max_bcap, d->bcap);
+      tab(DT_ONE)[i] = i;
+      tab(DT_BEG_G)[i] = tot_g;
+      tot_g += dg.g;
+      tab(DT_BEG_GL)[i] = tot_gl;
+      tot_gl += dg.gl;
+      tab(DT_BEG_GP)[i] = tot_gp;
+      tot_gp += dg.gp;
+      tab(DT_BEG_GS)[i] = tot_gs;
+      tot_gs += dg.gs;
+      for (int v = 0; v < GATHER_VARIANTS; v++) {
+        tab(DT_BEG_GATHER + v)[i] = tot_v[v];
+        if (v == dg.variant) tot_v[v] += dg.gg;
+      }
+    }
+    tab(DT_ONE)[count] = count;
+    tab(DT_BEG_G)[count] = tot_g;
+    tab(DT_BEG_GL)[count] = tot_gl;
+    tab(DT_BEG_GP)[count] = tot_gp;
+    tab(DT_BEG_GS)[count] = tot_gs;
+    for (int v = 0; v < GATHER_VARIANTS; v++) tab(DT_BEG_GATHER + v)[count] = tot_v[v];
+    dplan.base = SegGrid{reinterpret_cast<const DiffArgs*>(B + L.dargs), nullptr, dtab(DT_G), dtab(DT_GS),
+                         dtab(DT_BCAP), count};
+    dplan.beg_one = dtab(DT_ONE);
+    dplan.beg_g = dtab(DT_BEG_G);
+    dplan.beg_gl = dtab(DT_BEG_GL);
+    dplan.beg_gp = dtab(DT_BEG_GP);
+    dplan.beg_gs = dtab(DT_BEG_GS);
+    for (int v = 0; v < GATHER_VARIANTS; v++) {
+      dplan.beg_gather[v] = dtab(DT_BEG_GATHER + v);
+      dplan.tot_gather[v] = tot_v[v];
+    }
+    dplan.tot_g = tot_g;
+    dplan.tot_gl = tot_gl;
+    dplan.tot_gp = tot_gp;
+    dplan.tot_gs = tot_gs;
+    dplan.max_bcap = max_bcap;
+  }
   auto* d_items = reinterpret_cast<BatchLeafItem*>(B + L.items);
   auto* d_rounds = reinterpret_cast<RoundState*>(B + L.rounds);
   auto* d_states = reinterpret_cast<DevState* const*>(B + L.states);
@@ -1149,7 +1216,8 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
     key.push_back((uint64_t)(int64_t)item_of[i]);
   }
   for (auto& g : groups) key.insert(key.end(), {(uint64_t)g.U, (uint64_t)g.kind, g.beg, g.end, g.tiles});
-  key.insert(key.end(), {(uint64_t)B, (uint64_t)H, L.total, (uint64_t)b->coll.p, (uint64_t)b->coll_h.p, (uint64_t)cand.stages,
+  key.insert(key.end(), {(uint64_t)B, (uint64_t)H, L.total, (uint64_t)b->batch_diff, (uint64_t)b->coll.p,
+                         (uint64_t)b->coll_h.p, (uint64_t)cand.stages,
                          (uint64_t)cand.ctas, (uint64_t)cand.tiles_per_pop, (uint64_t)cand.streams});
 
   const uint64_t kh = key_hash(key);
@@ -1200,12 +1268,17 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
       for (uint32_t i : branch[j]) {
         if (erc != B2D_OK) break;
         b2d_dedup* d = hs[i];
-        const int r = enqueue_checkpoint(d, s, &d->state.p->round, false, false, item_of[i] >= 0, true);
+        const int r = enqueue_checkpoint(d, s, &d->state.p->round, false, false, item_of[i] >= 0, true, b->batch_diff);
         if (r != B2D_OK) erc = r;
         launches += d->launches;
       }
       cap_err(cudaEventRecord(b->side_ev[j], s));
       cap_err(cudaStreamWaitEvent(main, b->side_ev[j], 0));
+    }
+    if (b->batch_diff && erc == B2D_OK) {
+      uint32_t dl = 0;
+      cap_err(launch_collect_diff_batch(dplan, main, &dl));
+      launches += dl;
     }
     batch_collect_kernel<<<(count + 127) / 128, 128, 0, main>>>(d_states, count, b->coll.p);
     cap_err(cudaGetLastError());
@@ -1693,6 +1766,7 @@ int b2d_batch_set_param(b2d_batch* b, const char* name, int64_t value) {
   else if (k == "streams" && value >= 1 && value <= 64) b->cur.streams = (int)value;
   else if (k == "graph_cache" && value >= 1 && value <= 4096) b->graph_cap = (size_t)value;
   else if (k == "graph" && value >= 0 && value <= 2) b->graph_mode = (int)value;
+  else if (k == "batch_diff" && (value == 0 || value == 1)) b->batch_diff = value != 0;
   else if (k == "autotune" && (value == 0 || value == 1)) {
     b->autotune = value != 0;
     b->tuner.reset(b->cur);
@@ -1712,6 +1786,7 @@ int b2d_batch_get_param(b2d_batch* b, const char* name, int64_t* value) {
   else if (k == "graph_cache") *value = (int64_t)b->graph_cap;
   else if (k == "graphs") *value = (int64_t)b->graphs.size();
   else if (k == "graph") *value = b->graph_mode;
+  else if (k == "batch_diff") *value = b->batch_diff ? 1 : 0;
   else return B2D_ERR_ARG;
   return B2D_OK;
 }

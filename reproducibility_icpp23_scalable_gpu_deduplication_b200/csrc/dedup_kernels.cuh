@@ -146,4 +146,37 @@ cudaError_t launch_zero_exists(int* flag, const RoundState* rs, cudaStream_t str
 // bcap: bucket capacity the scratch was sized for (>= rs->buckets of every checkpoint run)
 cudaError_t launch_collect_diff(const DiffArgs& a, uint32_t bcap, int sm_count, cudaStream_t stream);
 
+// Diff assembly of many handles in one launch per step (batched form).  A segmented launch
+// gives handle h the CTAs beg[h] .. beg[h+1]-1 and runs its kernels as if launched alone on
+// that many CTAs.
+struct SegGrid {
+  const DiffArgs* args;   // per handle
+  const uint32_t* beg;    // n + 1 CTA offsets of the launch
+  const uint32_t* g;      // per handle: CTAs of its compaction and region launches
+  const uint32_t* gs;     // per handle: CTAs of its shift-entry launches
+  const uint32_t* bcap;   // per handle: bucket capacity of its scratch
+  uint32_t n;
+};
+// grid sizes of one handle's diff assembly; variant = data-gather kernel (0..5: 16-byte copies
+// with 32/16/8/4/2/1 lanes per chunk, 6: byte copies)
+struct DiffGrids {
+  uint32_t g, gs, gl, gp, gg;
+  int variant;
+};
+constexpr int GATHER_VARIANTS = 7;
+DiffGrids diff_grids(const DiffArgs& a, int sm_count);
+struct DiffBatch {
+  SegGrid base;                     // beg unused
+  const uint32_t* beg_one;          // 0, 1, .., n: one CTA per handle
+  const uint32_t* beg_g;
+  const uint32_t* beg_gl;
+  const uint32_t* beg_gp;
+  const uint32_t* beg_gs;
+  const uint32_t* beg_gather[GATHER_VARIANTS];
+  uint32_t tot_g, tot_gl, tot_gp, tot_gs, tot_gather[GATHER_VARIANTS];
+  uint32_t max_bcap;
+};
+// launches (count returned in *launches); the handles' hist arrays are cleared here
+cudaError_t launch_collect_diff_batch(const DiffBatch& b, cudaStream_t stream, uint32_t* launches);
+
 }  // namespace b2d

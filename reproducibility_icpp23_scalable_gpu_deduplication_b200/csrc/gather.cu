@@ -19,7 +19,21 @@
 namespace b2d {
 
 constexpr uint32_t COMPACT_THREADS = 512;
-constexpr uint32_t SHIFT_GRID = 1184;   // 8 x 148 ranges for the shift-entry passes
+
+// Every kernel below is a body over a virtual grid (bid of nb CTAs) with two launchers: one
+// handle's launch (the CUDA grid) and a segmented launch over many handles' diff assembly in
+// one grid, where CTA b belongs to the handle h with beg[h] <= b < beg[h+1] (batched form).
+__device__ __forceinline__ uint32_t seg_locate(const SegGrid& s, uint32_t& bid, uint32_t& nb) {
+  uint32_t lo = 0, hi = s.n;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (s.beg[mid] <= blockIdx.x) lo = mid; else hi = mid;
+  }
+  bid = blockIdx.x - s.beg[lo];
+  nb = s.beg[lo + 1] - s.beg[lo];
+  return lo;
+}
+constexpr uint32_t SHIFT_GRID = 296;    // at most 2 x 148 ranges for the shift-entry passes
 
 // Region roots are flagged in `push` (node-indexed, zero-padded to a multiple of 16 nodes,
 // all-zero between checkpoints).  Compaction runs in node order with 16-byte loads; since the
@@ -42,12 +56,11 @@ __device__ __forceinline__ void count16(uint4 v, uint32_t& cf, uint32_t& cs) {
   }
 }
 
-__global__ void __launch_bounds__(COMPACT_THREADS) compact_count_kernel(DiffArgs a0) {
-  const DiffArgs a = with_round(a0);
+__device__ __forceinline__ void compact_count_body(const DiffArgs& a, uint32_t bid, uint32_t nb) {
   __shared__ uint32_t sh[COMPACT_THREADS / 32 + 1];
   const uint64_t groups = ((uint64_t)a.N + 15u) / 16u;
   uint64_t beg, end;
-  cta_range(groups, blockIdx.x, gridDim.x, beg, end);
+  cta_range(groups, bid, nb, beg, end);
   uint32_t cf = 0, cs = 0;
   for (uint64_t g = beg + threadIdx.x; g < end; g += blockDim.x) {
     const uint4 v = ld_push16(a.push, g);
@@ -56,13 +69,20 @@ __global__ void __launch_bounds__(COMPACT_THREADS) compact_count_kernel(DiffArgs
   const uint32_t tf = block_reduce_sum(cf, sh);
   const uint32_t ts = block_reduce_sum(cs, sh);
   if (threadIdx.x == 0) {
-    a.partial2[2 * blockIdx.x] = tf;
-    a.partial2[2 * blockIdx.x + 1] = ts;
+    a.partial2[2 * bid] = tf;
+    a.partial2[2 * bid + 1] = ts;
   }
 }
+__global__ void __launch_bounds__(COMPACT_THREADS) compact_count_kernel(DiffArgs a0) {
+  compact_count_body(with_round(a0), blockIdx.x, gridDim.x);
+}
+__global__ void __launch_bounds__(COMPACT_THREADS) compact_count_seg(SegGrid s) {
+  uint32_t bid, nb;
+  const uint32_t h = seg_locate(s, bid, nb);
+  compact_count_body(with_round(s.args[h]), bid, nb);
+}
 
-__global__ void __launch_bounds__(1024) compact_scan_kernel(DiffArgs a0, uint32_t g) {
-  const DiffArgs a = with_round(a0);
+__device__ __forceinline__ void compact_scan_body(const DiffArgs& a, uint32_t bid, uint32_t nb, uint32_t g) {
   __shared__ uint32_t sh[33];
   uint32_t tf, ts;
   const uint32_t i = threadIdx.x;
@@ -78,18 +98,27 @@ __global__ void __launch_bounds__(1024) compact_scan_kernel(DiffArgs a0, uint32_
     a.meta->S = ts;
   }
 }
+__global__ void __launch_bounds__(1024) compact_scan_kernel(DiffArgs a0, uint32_t g) {
+  compact_scan_body(with_round(a0), blockIdx.x, gridDim.x, g);
+}
+__global__ void __launch_bounds__(1024) compact_scan_seg(SegGrid s) {
+  uint32_t bid, nb;
+  const uint32_t h = seg_locate(s, bid, nb);
+  compact_scan_body(with_round(s.args[h]), bid, nb, s.g[h]);
+  // the per-checkpoint bucket counts start at zero (the single-handle path memsets them)
+  for (uint32_t t = threadIdx.x; t < s.bcap[h]; t += blockDim.x) s.args[h].hist[t] = 0u;
+}
 
 // node-order lists of first / shift roots; clears the flags it consumed.  Each thread owns
 // COMPACT_GROUPS consecutive 16-node groups of a tile, so one block scan covers
 // COMPACT_THREADS * COMPACT_GROUPS * 16 nodes and the loads of a thread are independent.
 constexpr uint32_t COMPACT_GROUPS = 4;   // tile of 32768 nodes keeps both packed 16-bit counts exact
-__global__ void __launch_bounds__(COMPACT_THREADS) compact_write_kernel(DiffArgs a0) {
-  const DiffArgs a = with_round(a0);
+__device__ __forceinline__ void compact_write_body(const DiffArgs& a, uint32_t bid, uint32_t nb) {
   __shared__ uint32_t sh[COMPACT_THREADS / 32 + 1];
   const uint64_t groups = ((uint64_t)a.N + 15u) / 16u;
   uint64_t beg, end;
-  cta_range(groups, blockIdx.x, gridDim.x, beg, end);
-  uint32_t bf = a.partial2[2 * blockIdx.x], bs = a.partial2[2 * blockIdx.x + 1];
+  cta_range(groups, bid, nb, beg, end);
+  uint32_t bf = a.partial2[2 * bid], bs = a.partial2[2 * bid + 1];
   constexpr uint32_t TILE = COMPACT_THREADS * COMPACT_GROUPS;
   for (uint64_t t0 = beg; t0 < end; t0 += TILE) {
     const uint64_t g0 = t0 + (uint64_t)threadIdx.x * COMPACT_GROUPS;
@@ -132,6 +161,14 @@ __global__ void __launch_bounds__(COMPACT_THREADS) compact_write_kernel(DiffArgs
     bs += tot & 0xffffu;
   }
 }
+__global__ void __launch_bounds__(COMPACT_THREADS) compact_write_kernel(DiffArgs a0) {
+  compact_write_body(with_round(a0), blockIdx.x, gridDim.x);
+}
+__global__ void __launch_bounds__(COMPACT_THREADS) compact_write_seg(SegGrid s) {
+  uint32_t bid, nb;
+  const uint32_t h = seg_locate(s, bid, nb);
+  compact_write_body(with_round(s.args[h]), bid, nb);
+}
 
 // warp-parallel lower bound: first index of sorted v[0..cnt) with v[idx] >= key (32-ary search)
 __device__ __forceinline__ uint32_t warp_lower_bound(const uint32_t* v, uint32_t cnt, uint64_t key) {
@@ -153,9 +190,8 @@ __device__ __forceinline__ uint32_t warp_lower_bound(const uint32_t* v, uint32_t
 
 // level runs of the node-order lists: levels[L] = start of level L in tmp_first,
 // levels[34 + L] in tmp_shift (L = 0..D+1); one warp per search
-__global__ void compact_levels_kernel(DiffArgs a0) {
-  const DiffArgs a = with_round(a0);
-  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+__device__ __forceinline__ void compact_levels_body(const DiffArgs& a, uint32_t bid, uint32_t nb) {
+  const uint32_t gw = (bid * blockDim.x + threadIdx.x) >> 5;
   const uint32_t L = gw >> 1;
   if (L > a.D + 1u) return;
   const uint64_t key = (1ull << L) - 1ull;   // first node of level L
@@ -167,13 +203,20 @@ __global__ void compact_levels_kernel(DiffArgs a0) {
     if ((threadIdx.x & 31u) == 0) a.levels[34 + L] = r;
   }
 }
+__global__ void compact_levels_kernel(DiffArgs a0) {
+  compact_levels_body(with_round(a0), blockIdx.x, gridDim.x);
+}
+__global__ void compact_levels_seg(SegGrid s) {
+  uint32_t bid, nb;
+  const uint32_t h = seg_locate(s, bid, nb);
+  compact_levels_body(with_round(s.args[h]), bid, nb);
+}
 
 // canonical position of node-order entry i at level L: entries of deeper levels first
-__global__ void compact_permute_kernel(DiffArgs a0) {
-  const DiffArgs a = with_round(a0);
+__device__ __forceinline__ void compact_permute_body(const DiffArgs& a, uint32_t bid, uint32_t nb) {
   const uint32_t F = a.meta->F, S = a.meta->S;
   const uint64_t tot = (uint64_t)F + S;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < tot; i += (uint64_t)gridDim.x * blockDim.x) {
+  for (uint64_t i = bid * (uint64_t)blockDim.x + threadIdx.x; i < tot; i += (uint64_t)nb * blockDim.x) {
     const bool isf = i < F;
     const uint32_t j = isf ? (uint32_t)i : (uint32_t)(i - F);
     const uint32_t* lv = a.levels + (isf ? 0 : 34);
@@ -186,13 +229,20 @@ __global__ void compact_permute_kernel(DiffArgs a0) {
     else a.shift_list[pos] = node;
   }
 }
+__global__ void compact_permute_kernel(DiffArgs a0) {
+  compact_permute_body(with_round(a0), blockIdx.x, gridDim.x);
+}
+__global__ void compact_permute_seg(SegGrid s) {
+  uint32_t bid, nb;
+  const uint32_t h = seg_locate(s, bid, nb);
+  compact_permute_body(with_round(s.args[h]), bid, nb);
+}
 
 // ---------------------------------------------------------------- region sizes and offsets
-__global__ void __launch_bounds__(COMPACT_THREADS) region_count_kernel(DiffArgs a0) {
-  const DiffArgs a = with_round(a0);
+__device__ __forceinline__ void region_count_body(const DiffArgs& a, uint32_t bid, uint32_t nb) {
   __shared__ uint32_t sh[COMPACT_THREADS / 32 + 1];
   uint64_t beg, end;
-  cta_range(a.meta->F, blockIdx.x, gridDim.x, beg, end);
+  cta_range(a.meta->F, bid, nb, beg, end);
   uint32_t c = 0;
   for (uint64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
     const uint32_t node = a.first_list[i];
@@ -204,11 +254,18 @@ __global__ void __launch_bounds__(COMPACT_THREADS) region_count_kernel(DiffArgs 
       set_error(a.st, DERR_INTERNAL, 20);
   }
   const uint32_t t = block_reduce_sum(c, sh);
-  if (threadIdx.x == 0) a.partial2[blockIdx.x] = t;
+  if (threadIdx.x == 0) a.partial2[bid] = t;
+}
+__global__ void __launch_bounds__(COMPACT_THREADS) region_count_kernel(DiffArgs a0) {
+  region_count_body(with_round(a0), blockIdx.x, gridDim.x);
+}
+__global__ void __launch_bounds__(COMPACT_THREADS) region_count_seg(SegGrid s) {
+  uint32_t bid, nb;
+  const uint32_t h = seg_locate(s, bid, nb);
+  region_count_body(with_round(s.args[h]), bid, nb);
 }
 
-__global__ void __launch_bounds__(1024) region_scan_kernel(DiffArgs a0, uint32_t g) {
-  const DiffArgs a = with_round(a0);
+__device__ __forceinline__ void region_scan_body(const DiffArgs& a, uint32_t bid, uint32_t nb, uint32_t g) {
   __shared__ uint32_t sh[33];
   uint32_t tot;
   const uint32_t i = threadIdx.x;
@@ -217,13 +274,20 @@ __global__ void __launch_bounds__(1024) region_scan_kernel(DiffArgs a0, uint32_t
   if (i < g) a.partial2[i] = e;
   if (i == 0) a.meta->T = tot;
 }
+__global__ void __launch_bounds__(1024) region_scan_kernel(DiffArgs a0, uint32_t g) {
+  region_scan_body(with_round(a0), blockIdx.x, gridDim.x, g);
+}
+__global__ void __launch_bounds__(1024) region_scan_seg(SegGrid s) {
+  uint32_t bid, nb;
+  const uint32_t h = seg_locate(s, bid, nb);
+  region_scan_body(with_round(s.args[h]), bid, nb, s.g[h]);
+}
 
-__global__ void __launch_bounds__(COMPACT_THREADS) region_write_kernel(DiffArgs a0) {
-  const DiffArgs a = with_round(a0);
+__device__ __forceinline__ void region_write_body(const DiffArgs& a, uint32_t bid, uint32_t nb) {
   __shared__ uint32_t sh[COMPACT_THREADS / 32 + 1];
   uint64_t beg, end;
-  cta_range(a.meta->F, blockIdx.x, gridDim.x, beg, end);
-  uint32_t base = a.partial2[blockIdx.x];
+  cta_range(a.meta->F, bid, nb, beg, end);
+  uint32_t base = a.partial2[bid];
   for (uint64_t t0 = beg; t0 < end; t0 += blockDim.x) {
     const uint64_t i = t0 + threadIdx.x;
     const uint32_t len = i < end ? num_leaf_descendents(a.first_list[i], a.N) : 0u;
@@ -233,15 +297,22 @@ __global__ void __launch_bounds__(COMPACT_THREADS) region_write_kernel(DiffArgs 
     base += tot;
   }
 }
+__global__ void __launch_bounds__(COMPACT_THREADS) region_write_kernel(DiffArgs a0) {
+  region_write_body(with_round(a0), blockIdx.x, gridDim.x);
+}
+__global__ void __launch_bounds__(COMPACT_THREADS) region_write_seg(SegGrid s) {
+  uint32_t bid, nb;
+  const uint32_t h = seg_locate(s, bid, nb);
+  region_write_body(with_round(s.args[h]), bid, nb);
+}
 
 // ---------------------------------------------------------------- shifted duplicates
 // source NodeID of each entry (:572-580, :672-674) and per-range histograms by checkpoint
-__global__ void __launch_bounds__(128) shift_prev_kernel(DiffArgs a0, uint32_t bcap) {
-  const DiffArgs a = with_round(a0);
-  const uint32_t B = a0.rs->buckets <= bcap ? a0.rs->buckets : bcap;
+__device__ __forceinline__ void shift_prev_body(const DiffArgs& a, uint32_t bid, uint32_t nb, uint32_t bcap) {
+  const uint32_t B = a.rs->buckets <= bcap ? a.rs->buckets : bcap;
   extern __shared__ uint32_t hs[];
   uint64_t beg, end;
-  cta_range(a.meta->S, blockIdx.x, gridDim.x, beg, end);
+  cta_range(a.meta->S, bid, nb, beg, end);
   for (uint32_t t = threadIdx.x; t < B; t += blockDim.x) hs[t] = 0;
   __syncthreads();
   for (uint64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
@@ -265,15 +336,22 @@ __global__ void __launch_bounds__(128) shift_prev_kernel(DiffArgs a0, uint32_t b
   __syncthreads();
   for (uint32_t t = threadIdx.x; t < B; t += blockDim.x) {
     const uint32_t v = hs[t];
-    a.partial[(uint64_t)t * gridDim.x + blockIdx.x] = v;
+    a.partial[(uint64_t)t * nb + bid] = v;
     if (v) atomicAdd(&a.hist[t], v);
   }
 }
+__global__ void __launch_bounds__(128) shift_prev_kernel(DiffArgs a0, uint32_t bcap) {
+  shift_prev_body(with_round(a0), blockIdx.x, gridDim.x, bcap);
+}
+__global__ void __launch_bounds__(128) shift_prev_seg(SegGrid s) {
+  uint32_t bid, nb;
+  const uint32_t h = seg_locate(s, bid, nb);
+  shift_prev_body(with_round(s.args[h]), bid, nb, s.bcap[h]);
+}
 
 // one CTA: bucket starts, repeat table, per-range scatter bases, header, byte layout
-__global__ void __launch_bounds__(1024) layout_kernel(DiffArgs a0, uint32_t bcap, uint32_t g) {
-  const DiffArgs a = with_round(a0);
-  const uint32_t B = a0.rs->buckets <= bcap ? a0.rs->buckets : bcap;
+__device__ __forceinline__ void layout_body(const DiffArgs& a, uint32_t bid, uint32_t nb, uint32_t bcap, uint32_t g) {
+  const uint32_t B = a.rs->buckets <= bcap ? a.rs->buckets : bcap;
   __shared__ uint32_t sh[33];
   __shared__ uint32_t carry_start, carry_rows;
   if (threadIdx.x == 0) { carry_start = 0; carry_rows = 0; }
@@ -356,16 +434,23 @@ __global__ void __launch_bounds__(1024) layout_kernel(DiffArgs a0, uint32_t bcap
     m->map_size = *a.map.size;
   }
 }
+__global__ void __launch_bounds__(1024) layout_kernel(DiffArgs a0, uint32_t bcap, uint32_t g) {
+  layout_body(with_round(a0), blockIdx.x, gridDim.x, bcap, g);
+}
+__global__ void __launch_bounds__(1024) layout_seg(SegGrid s) {
+  uint32_t bid, nb;
+  const uint32_t h = seg_locate(s, bid, nb);
+  layout_body(with_round(s.args[h]), bid, nb, s.bcap[h], s.gs[h]);
+}
 
 // stable scatter of shift entries: one warp walks its range in order
-__global__ void __launch_bounds__(32) shift_write_kernel(DiffArgs a0, uint32_t bcap) {
-  const DiffArgs a = with_round(a0);
-  const uint32_t B = a0.rs->buckets <= bcap ? a0.rs->buckets : bcap;
+__device__ __forceinline__ void shift_write_body(const DiffArgs& a, uint32_t bid, uint32_t nb, uint32_t bcap) {
+  const uint32_t B = a.rs->buckets <= bcap ? a.rs->buckets : bcap;
   extern __shared__ uint32_t run[];
   uint64_t beg, end;
-  cta_range(a.meta->S, blockIdx.x, gridDim.x, beg, end);
+  cta_range(a.meta->S, bid, nb, beg, end);
   if (beg >= end) return;
-  for (uint32_t t = threadIdx.x; t < B; t += 32) run[t] = a.partial[(uint64_t)t * gridDim.x + blockIdx.x];
+  for (uint32_t t = threadIdx.x; t < B; t += 32) run[t] = a.partial[(uint64_t)t * nb + bid];
   __syncwarp();
   const uint64_t shift_off = a.meta->shift_off;
   const uint32_t lane = threadIdx.x;
@@ -387,6 +472,14 @@ __global__ void __launch_bounds__(32) shift_write_kernel(DiffArgs a0, uint32_t b
     }
   }
 }
+__global__ void __launch_bounds__(32) shift_write_kernel(DiffArgs a0, uint32_t bcap) {
+  shift_write_body(with_round(a0), blockIdx.x, gridDim.x, bcap);
+}
+__global__ void __launch_bounds__(32) shift_write_seg(SegGrid s) {
+  uint32_t bid, nb;
+  const uint32_t h = seg_locate(s, bid, nb);
+  shift_write_body(with_round(s.args[h]), bid, nb, s.bcap[h]);
+}
 
 // ---------------------------------------------------------------- metadata + data gather
 __device__ __forceinline__ uint32_t find_region(const uint32_t* off, uint32_t F, uint64_t k) {
@@ -403,13 +496,12 @@ __device__ __forceinline__ uint32_t find_region(const uint32_t* off, uint32_t F,
 // once and then walks forward; LPC lanes copy one chunk with 16-byte vectors (chunk size a
 // multiple of 16, both sides 16-byte aligned); the short last chunk is zero-padded (:643-645).
 template <uint32_t LPC>
-__global__ void __launch_bounds__(256) gather_vec_kernel(DiffArgs a0) {
-  const DiffArgs a = with_round(a0);
+__device__ __forceinline__ void gather_vec_body(const DiffArgs& a, uint32_t bid, uint32_t nb) {
   const DevMeta m = *a.meta;
   uint8_t* dst_base = a.diff + m.data_off;
   uint32_t* first_meta = reinterpret_cast<uint32_t*>(a.diff + m.first_off);
-  const uint64_t gtid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  const uint64_t nthr = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t gtid = bid * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t nthr = (uint64_t)nb * blockDim.x;
   for (uint64_t i = gtid; i < m.F; i += nthr) first_meta[i] = a.first_list[i];
   if (m.T == 0) return;
   constexpr uint32_t CPW = 32u / LPC;   // chunks per warp iteration
@@ -487,15 +579,24 @@ __global__ void __launch_bounds__(256) gather_vec_kernel(DiffArgs a0) {
     r = __reduce_max_sync(0xffffffffu, rr);
   }
 }
+template <uint32_t LPC>
+__global__ void __launch_bounds__(256) gather_vec_kernel(DiffArgs a0) {
+  gather_vec_body<LPC>(with_round(a0), blockIdx.x, gridDim.x);
+}
+template <uint32_t LPC>
+__global__ void __launch_bounds__(256) gather_vec_seg(SegGrid s) {
+  uint32_t bid, nb;
+  const uint32_t h = seg_locate(s, bid, nb);
+  gather_vec_body<LPC>(with_round(s.args[h]), bid, nb);
+}
 
 // any chunk size / alignment: one thread per chunk, byte copies
-__global__ void __launch_bounds__(256) gather_bytes_kernel(DiffArgs a0) {
-  const DiffArgs a = with_round(a0);
+__device__ __forceinline__ void gather_bytes_body(const DiffArgs& a, uint32_t bid, uint32_t nb) {
   const DevMeta m = *a.meta;
   uint8_t* dst_base = a.diff + m.data_off;
   uint8_t* first_meta = a.diff + m.first_off;
-  const uint64_t gtid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  const uint64_t nthr = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t gtid = bid * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t nthr = (uint64_t)nb * blockDim.x;
   for (uint64_t i = gtid; i < m.F; i += nthr) {
     const uint32_t v = a.first_list[i];
     memcpy(first_meta + 4 * i, &v, 4);
@@ -512,24 +613,82 @@ __global__ void __launch_bounds__(256) gather_bytes_kernel(DiffArgs a0) {
     for (uint64_t b = 0; b < a.cs; b++) d[b] = b < avail ? s[b] : 0u;
   }
 }
+__global__ void __launch_bounds__(256) gather_bytes_kernel(DiffArgs a0) {
+  gather_bytes_body(with_round(a0), blockIdx.x, gridDim.x);
+}
+__global__ void __launch_bounds__(256) gather_bytes_seg(SegGrid s) {
+  uint32_t bid, nb;
+  const uint32_t h = seg_locate(s, bid, nb);
+  gather_bytes_body(with_round(s.args[h]), bid, nb);
+}
 
 static uint32_t grid_for(uint64_t units, uint64_t per_cta, uint32_t cap) {
   const uint64_t g = (units + per_cta - 1) / per_cta;
   return g < 1 ? 1u : (g > cap ? cap : (uint32_t)g);
 }
 
+// grids follow the buffer size (host-known bounds: F, S <= n), so a small buffer is not charged
+// for hundreds of idle CTAs per launch; large buffers get the full grids
+DiffGrids diff_grids(const DiffArgs& a, int sm_count) {
+  DiffGrids r;
+  r.g = grid_for(((uint64_t)a.N + 15u) / 16u, 512, SCAN_GRID);   // ~1 16-node load per thread
+  // shift-entry ranges: the layout kernel scans every range's count per bucket in one CTA, so
+  // fewer, longer ranges (<= 296) keep it short; the scatter walks each range with one warp
+  r.gs = grid_for(a.n, 8192, SHIFT_GRID);
+  r.gl = (2u * (a.D + 2u) * 32u + 255u) / 256u;
+  r.gp = grid_for(a.n, 2048, (uint32_t)sm_count * 2u);
+  r.gg = grid_for((uint64_t)a.n * a.cs, 32768, (uint32_t)sm_count * 4u);
+  const bool vec = (a.cs % 16u == 0) && ((reinterpret_cast<uintptr_t>(a.data) & 15u) == 0) &&
+                   ((reinterpret_cast<uintptr_t>(a.diff) & 15u) == 0);
+  const uint32_t units = a.cs / 16u;
+  r.variant = !vec ? 6 : units >= 32 ? 0 : units >= 16 ? 1 : units >= 8 ? 2 : units >= 4 ? 3 : units >= 2 ? 4 : 5;
+  return r;
+}
+
+cudaError_t launch_collect_diff_batch(const DiffBatch& b, cudaStream_t stream, uint32_t* launches) {
+  if (b.max_bcap > MAX_BUCKETS || b.base.n == 0) return cudaErrorInvalidValue;
+  SegGrid s = b.base;
+  uint32_t c = 0;
+  const size_t hsm = sizeof(uint32_t) * b.max_bcap;
+  s.beg = b.beg_g;   compact_count_seg<<<b.tot_g, COMPACT_THREADS, 0, stream>>>(s); c++;
+  s.beg = b.beg_one; compact_scan_seg<<<s.n, 1024, 0, stream>>>(s); c++;
+  s.beg = b.beg_g;   compact_write_seg<<<b.tot_g, COMPACT_THREADS, 0, stream>>>(s); c++;
+  s.beg = b.beg_gl;  compact_levels_seg<<<b.tot_gl, 256, 0, stream>>>(s); c++;
+  s.beg = b.beg_gp;  compact_permute_seg<<<b.tot_gp, 256, 0, stream>>>(s); c++;
+  s.beg = b.beg_g;   region_count_seg<<<b.tot_g, COMPACT_THREADS, 0, stream>>>(s); c++;
+  s.beg = b.beg_one; region_scan_seg<<<s.n, 1024, 0, stream>>>(s); c++;
+  s.beg = b.beg_g;   region_write_seg<<<b.tot_g, COMPACT_THREADS, 0, stream>>>(s); c++;
+  s.beg = b.beg_gs;  shift_prev_seg<<<b.tot_gs, 128, hsm, stream>>>(s); c++;
+  s.beg = b.beg_one; layout_seg<<<s.n, 1024, 0, stream>>>(s); c++;
+  s.beg = b.beg_gs;  shift_write_seg<<<b.tot_gs, 32, hsm, stream>>>(s); c++;
+  for (int v = 0; v < GATHER_VARIANTS; v++) {
+    if (!b.tot_gather[v]) continue;
+    s.beg = b.beg_gather[v];
+    switch (v) {
+      case 0: gather_vec_seg<32><<<b.tot_gather[v], 256, 0, stream>>>(s); break;
+      case 1: gather_vec_seg<16><<<b.tot_gather[v], 256, 0, stream>>>(s); break;
+      case 2: gather_vec_seg<8><<<b.tot_gather[v], 256, 0, stream>>>(s); break;
+      case 3: gather_vec_seg<4><<<b.tot_gather[v], 256, 0, stream>>>(s); break;
+      case 4: gather_vec_seg<2><<<b.tot_gather[v], 256, 0, stream>>>(s); break;
+      case 5: gather_vec_seg<1><<<b.tot_gather[v], 256, 0, stream>>>(s); break;
+      default: gather_bytes_seg<<<b.tot_gather[v], 256, 0, stream>>>(s); break;
+    }
+    c++;
+  }
+  if (launches) *launches = c;
+  return cudaGetLastError();
+}
+
 cudaError_t launch_collect_diff(const DiffArgs& a, uint32_t bcap, int sm_count, cudaStream_t stream) {
-  // grids follow the buffer size (host-known bounds: F, S <= n), so a small buffer is not
-  // charged for hundreds of idle CTAs per launch; large buffers get the full grids
-  const uint32_t g = grid_for(((uint64_t)a.N + 15u) / 16u, 512, SCAN_GRID);   // ~1 16-node load per thread
-  const uint32_t gs = grid_for(a.n, 2048, SHIFT_GRID);
+  const DiffGrids dg = diff_grids(a, sm_count);
+  const uint32_t g = dg.g, gs = dg.gs;
   const uint32_t B = bcap;   // capacity; each kernel reads the checkpoint's bucket count from rs
   if (B > MAX_BUCKETS) return cudaErrorInvalidValue;
   compact_count_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);
   compact_scan_kernel<<<1, 1024, 0, stream>>>(a, g);
   compact_write_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);
-  compact_levels_kernel<<<(2u * (a.D + 2u) * 32u + 255u) / 256u, 256, 0, stream>>>(a);
-  compact_permute_kernel<<<grid_for(a.n, 2048, (uint32_t)sm_count * 2u), 256, 0, stream>>>(a);
+  compact_levels_kernel<<<dg.gl, 256, 0, stream>>>(a);
+  compact_permute_kernel<<<dg.gp, 256, 0, stream>>>(a);
   region_count_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);
   region_scan_kernel<<<1, 1024, 0, stream>>>(a, g);
   region_write_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);
@@ -539,7 +698,7 @@ cudaError_t launch_collect_diff(const DiffArgs& a, uint32_t bcap, int sm_count, 
   shift_prev_kernel<<<gs, 128, hsm, stream>>>(a, B);
   layout_kernel<<<1, 1024, 0, stream>>>(a, B, gs);
   shift_write_kernel<<<gs, 32, hsm, stream>>>(a, B);
-  const uint32_t gblocks = grid_for((uint64_t)a.n * a.cs, 32768, (uint32_t)sm_count * 4u);
+  const uint32_t gblocks = dg.gg;
   const bool vec = (a.cs % 16u == 0) && ((reinterpret_cast<uintptr_t>(a.data) & 15u) == 0) &&
                    ((reinterpret_cast<uintptr_t>(a.diff) & 15u) == 0);
   if (vec) {
