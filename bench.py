@@ -368,7 +368,9 @@ def serve_stream(server_kw, sizes, clients, arrivals, dev, warm_rounds=2, reserv
     print(json.dumps({"diag": "served_stream", "plain": bool(server_kw.get("plain")), "map_grows_total": grows,
                       "queue_ms_p50_p99_max": [queue[len(queue) // 2], queue[int(0.99 * len(queue))], queue[-1]],
                       "exec_ms_p50_p99_max": [execu[len(execu) // 2], execu[int(0.99 * len(execu))], execu[-1]],
-                      "slowest": sorted(((round(1e3 * (r.done - t), 1), r.client, r.nbytes >> 20)
+                      "slowest": sorted(((round(1e3 * (r.done - t), 1), r.client, r.nbytes >> 20,
+                                          round(1e3 * (r.launch_s or 0), 2), r.batch_size,
+                                          round(1e3 * (r.done - r.launched), 1))
                                          for r, t in zip(reqs, submitted)), reverse=True)[:8]}),
           file=sys.stderr, flush=True)
     srv.close()

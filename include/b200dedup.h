@@ -204,7 +204,9 @@ int b2d_batch_set_stream(b2d_batch* b, void* cuda_stream);
  * the first time and as a captured graph from its second batch on, default; 1 = always a graph;
  * 0 = never), "graph_cache" (instantiated graphs kept, one per batch composition, default 16),
  * "batch_diff" (1 = every handle's diff assembly in 12-13 shared launches after all trees are
- * labelled, default; 0 = per handle in its own branch).  Output never depends on them. */
+ * labelled, default; 0 = per handle in its own branch), "batch_forest" (1 = every handle's
+ * Merkle-forest phases in shared launches, one per tree step, default; needs batch_diff).
+ * Output never depends on them. */
 int b2d_batch_set_param(b2d_batch* b, const char* name, int64_t value);
 int b2d_batch_get_param(b2d_batch* b, const char* name, int64_t* value);
 int b2d_batch_checkpoint(b2d_batch* b, b2d_dedup* const* handles, const void* const* d_data, const uint64_t* lens,

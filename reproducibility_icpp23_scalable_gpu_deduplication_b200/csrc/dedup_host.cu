@@ -504,10 +504,16 @@ DiffArgs diff_args(b2d_dedup* d, const RoundState* rs_dev) {
                   d->partial.p, d->partial2.p, d->diff.p, rs_dev};
 }
 
-int enqueue_checkpoint(b2d_dedup* d, cudaStream_t s, RoundState* rs_dev, bool upload, bool timing, bool skip_leaves,
-                       bool managed = false, bool skip_diff = false) {
+ForestArgs forest_args(b2d_dedup* d, const RoundState* rs_dev) {
   MapView m;
   map_view(d, m);
+  DevState* ds = d->state.p;
+  return ForestArgs{d->tree.p, d->lab.p, d->leaflab.p, d->push.p, m, &ds->status, &ds->zero_exists, d->dupflag.p,
+                    d->n, d->N, d->D, 0, d->kind, 0, rs_dev};
+}
+
+int enqueue_checkpoint(b2d_dedup* d, cudaStream_t s, RoundState* rs_dev, bool upload, bool timing, bool skip_leaves,
+                       bool managed = false, bool skip_diff = false, bool skip_forest = false) {
   DevState* ds = d->state.p;
   if (!managed) {
     B2D_CU(cudaMemsetAsync(ds, 0, sizeof(DevState), s));
@@ -522,17 +528,19 @@ int enqueue_checkpoint(b2d_dedup* d, cudaStream_t s, RoundState* rs_dev, bool up
     d->leaf_tma = leaf_path == 1;
   }
   if (timing) B2D_CU(record_timing(d->ev[3], s));
-  ForestArgs fa{d->tree.p, d->lab.p, d->leaflab.p, d->push.p, m, &ds->status, &ds->zero_exists, d->dupflag.p,
-                d->n, d->N, d->D, 0, d->kind, 0, rs_dev};
-  B2D_CU(launch_forest(fa, 1, s));
-  B2D_CU(launch_zero_exists(&ds->zero_exists, rs_dev, s));
-  B2D_CU(launch_forest(fa, 2, s));
+  if (!skip_forest) {
+    const ForestArgs fa = forest_args(d, rs_dev);
+    B2D_CU(launch_forest(fa, 1, s));
+    B2D_CU(launch_zero_exists(&ds->zero_exists, rs_dev, s));
+    B2D_CU(launch_forest(fa, 2, s));
+  }
   if (timing) B2D_CU(record_timing(d->ev[1], s));
   // collect_diff (:511-710); a batch may assemble all its handles' diffs in shared launches
   if (!skip_diff) B2D_CU(launch_collect_diff(diff_args(d, rs_dev), d->bcap, d->sm_count, s));
   if (timing) B2D_CU(record_timing(d->ev[2], s));
   if (!managed) B2D_CU(cudaMemcpyAsync(d->state_h.p, d->state.p, sizeof(DevState), cudaMemcpyDeviceToHost, s));
-  d->launches = (skip_leaves ? 0 : 1) + forest_launch_count(d->D, 1) + forest_launch_count(d->D, 2) + 1 +
+  d->launches = (skip_leaves ? 0 : 1) +
+                (skip_forest ? 0 : forest_launch_count(d->D, 1) + forest_launch_count(d->D, 2) + 1) +
                 (skip_diff ? 0 : 14);
   return B2D_OK;
 }
@@ -965,7 +973,8 @@ struct BatchTuner {
 };
 
 struct BatchLayout {
-  size_t items = 0, rounds = 0, states = 0, queues = 0, bstatus = 0, dargs = 0, dtab = 0, total = 0;
+  size_t items = 0, rounds = 0, states = 0, queues = 0, bstatus = 0, dargs = 0, dtab = 0, fargs = 0, ftab = 0,
+         total = 0;
 };
 // u32 tables of the shared diff assembly, each n (+1) long, in this order in the blob
 enum DiffTable { DT_G, DT_GS, DT_BCAP, DT_ONE, DT_BEG_G, DT_BEG_GL, DT_BEG_GP, DT_BEG_GS, DT_BEG_GATHER, DT_COUNT };
@@ -998,6 +1007,7 @@ struct b2d_batch {
   size_t graph_cap = 16;
   int graph_mode = 2;                // 0 direct launches, 1 always a graph, 2 graph from the 2nd sighting
   bool batch_diff = true;            // all handles' diff assembly in shared segmented launches
+  bool batch_forest = true;          // and their forest phases (needs batch_diff)
   std::vector<uint64_t> seen;        // compositions launched directly once
   uint64_t use_clock = 0;
   // the batch in flight (launched, not yet finished)
@@ -1136,7 +1146,37 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
   L.dargs = align_up(L.bstatus + sizeof(DevStatus), 64);
   L.dtab = align_up(L.dargs + (b->batch_diff ? sizeof(DiffArgs) * count : 0), 64);
   const size_t tab_len = (size_t)count + 1;   // entries per table
-  L.total = align_up(L.dtab + (b->batch_diff ? sizeof(uint32_t) * tab_len * DIFF_TABLES : 0), 256);
+  // shared forest phases: every handle's launch steps, one segmented launch per (phase, step,
+  // kind) with three tables (CTA offsets, p0, p1)
+  const bool seg_forest = b->batch_forest && b->batch_diff;
+  std::vector<std::vector<ForestStep>> fsteps[2];
+  struct FLaunch {
+    int phase, kind;
+    uint32_t k, ctas;
+    size_t off;
+  };
+  std::vector<FLaunch> flaunch;
+  if (seg_forest) {
+    for (int ph = 0; ph < 2; ph++) {
+      fsteps[ph].resize(count);
+      uint32_t K = 0;
+      for (uint32_t i = 0; i < count; i++) {
+        forest_steps(hs[i]->D, hs[i]->N, ph + 1, fsteps[ph][i]);
+        K = std::max<uint32_t>(K, (uint32_t)fsteps[ph][i].size());
+      }
+      for (uint32_t k = 0; k < K; k++)
+        for (int kind = 0; kind < 2; kind++) {
+          uint32_t ctas = 0;
+          for (uint32_t i = 0; i < count; i++)
+            if (k < fsteps[ph][i].size() && fsteps[ph][i][k].kind == kind) ctas += fsteps[ph][i][k].ctas;
+          if (ctas) flaunch.push_back(FLaunch{ph + 1, kind, k, ctas, 0});
+        }
+    }
+  }
+  L.fargs = align_up(L.dtab + (b->batch_diff ? sizeof(uint32_t) * tab_len * DIFF_TABLES : 0), 64);
+  L.ftab = align_up(L.fargs + (seg_forest ? sizeof(ForestArgs) * count : 0), 64);
+  for (size_t q = 0; q < flaunch.size(); q++) flaunch[q].off = L.ftab + sizeof(uint32_t) * 3 * tab_len * q;
+  L.total = align_up(L.ftab + sizeof(uint32_t) * 3 * tab_len * flaunch.size(), 256);
   B2D_CU(b->blob.reserve(L.total));
   B2D_CU(b->blob_h.reserve(L.total));
   B2D_CU(b->coll.reserve(count));
@@ -1202,6 +1242,35 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
     dplan.tot_gs = tot_gs;
     dplan.max_bcap = max_bcap;
   }
+  // shared forest phases: ForestArgs and per-launch tables
+  std::vector<ForestSeg> fseg(flaunch.size());
+  if (seg_forest) {
+    for (uint32_t i = 0; i < count; i++) {
+      const ForestArgs fa = forest_args(hs[i], &hs[i]->state.p->round);
+      std::memcpy(H + L.fargs + sizeof(ForestArgs) * i, &fa, sizeof(fa));
+    }
+    for (size_t q = 0; q < flaunch.size(); q++) {
+      const FLaunch& f = flaunch[q];
+      uint32_t* beg = reinterpret_cast<uint32_t*>(H + f.off);
+      uint32_t* p0 = beg + tab_len;
+      uint32_t* p1 = p0 + tab_len;
+      uint32_t acc = 0;
+      for (uint32_t i = 0; i < count; i++) {
+        beg[i] = acc;
+        p0[i] = p1[i] = 0;
+        const auto& st = fsteps[f.phase - 1][i];
+        if (f.k < st.size() && st[f.k].kind == f.kind) {
+          acc += st[f.k].ctas;
+          p0[i] = st[f.k].p0;
+          p1[i] = st[f.k].p1;
+        }
+      }
+      beg[count] = acc;
+      const uint32_t* dbeg = reinterpret_cast<const uint32_t*>(B + f.off);
+      fseg[q] = ForestSeg{reinterpret_cast<const ForestArgs*>(B + L.fargs), dbeg, dbeg + tab_len,
+                          dbeg + 2 * tab_len, count};
+    }
+  }
   auto* d_items = reinterpret_cast<BatchLeafItem*>(B + L.items);
   auto* d_rounds = reinterpret_cast<RoundState*>(B + L.rounds);
   auto* d_states = reinterpret_cast<DevState* const*>(B + L.states);
@@ -1216,7 +1285,8 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
     key.push_back((uint64_t)(int64_t)item_of[i]);
   }
   for (auto& g : groups) key.insert(key.end(), {(uint64_t)g.U, (uint64_t)g.kind, g.beg, g.end, g.tiles});
-  key.insert(key.end(), {(uint64_t)B, (uint64_t)H, L.total, (uint64_t)b->batch_diff, (uint64_t)b->coll.p,
+  key.insert(key.end(), {(uint64_t)B, (uint64_t)H, L.total, (uint64_t)b->batch_diff, (uint64_t)seg_forest,
+                         (uint64_t)b->coll.p,
                          (uint64_t)b->coll_h.p, (uint64_t)cand.stages,
                          (uint64_t)cand.ctas, (uint64_t)cand.tiles_per_pop, (uint64_t)cand.streams});
 
@@ -1268,12 +1338,30 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
       for (uint32_t i : branch[j]) {
         if (erc != B2D_OK) break;
         b2d_dedup* d = hs[i];
-        const int r = enqueue_checkpoint(d, s, &d->state.p->round, false, false, item_of[i] >= 0, true, b->batch_diff);
+        const bool skip_leaves = item_of[i] >= 0;
+        if (seg_forest && skip_leaves) continue;   // nothing of this handle runs in a branch
+        const int r = enqueue_checkpoint(d, s, &d->state.p->round, false, false, skip_leaves, true, b->batch_diff,
+                                         seg_forest);
         if (r != B2D_OK) erc = r;
         launches += d->launches;
       }
       cap_err(cudaEventRecord(b->side_ev[j], s));
       cap_err(cudaStreamWaitEvent(main, b->side_ev[j], 0));
+    }
+    if (seg_forest && erc == B2D_OK) {
+      // phase 1 steps, the zero-digest probe, phase 2 steps: each over every handle at once
+      for (size_t q = 0; q < flaunch.size() && erc == B2D_OK; q++) {
+        if (flaunch[q].phase != 1) continue;
+        cap_err(launch_forest_seg(fseg[q], 1, flaunch[q].kind, flaunch[q].ctas, main));
+        launches++;
+      }
+      cap_err(launch_zero_exists_seg(reinterpret_cast<const ForestArgs*>(B + L.fargs), count, main));
+      launches++;
+      for (size_t q = 0; q < flaunch.size() && erc == B2D_OK; q++) {
+        if (flaunch[q].phase != 2) continue;
+        cap_err(launch_forest_seg(fseg[q], 2, flaunch[q].kind, flaunch[q].ctas, main));
+        launches++;
+      }
     }
     if (b->batch_diff && erc == B2D_OK) {
       uint32_t dl = 0;
@@ -1767,6 +1855,7 @@ int b2d_batch_set_param(b2d_batch* b, const char* name, int64_t value) {
   else if (k == "graph_cache" && value >= 1 && value <= 4096) b->graph_cap = (size_t)value;
   else if (k == "graph" && value >= 0 && value <= 2) b->graph_mode = (int)value;
   else if (k == "batch_diff" && (value == 0 || value == 1)) b->batch_diff = value != 0;
+  else if (k == "batch_forest" && (value == 0 || value == 1)) b->batch_forest = value != 0;
   else if (k == "autotune" && (value == 0 || value == 1)) {
     b->autotune = value != 0;
     b->tuner.reset(b->cur);
@@ -1787,6 +1876,7 @@ int b2d_batch_get_param(b2d_batch* b, const char* name, int64_t* value) {
   else if (k == "graphs") *value = (int64_t)b->graphs.size();
   else if (k == "graph") *value = b->graph_mode;
   else if (k == "batch_diff") *value = b->batch_diff ? 1 : 0;
+  else if (k == "batch_forest") *value = b->batch_forest ? 1 : 0;
   else return B2D_ERR_ARG;
   return B2D_OK;
 }

@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda.h>
 
+#include <vector>
+
 #include "common.cuh"
 #include "map.cuh"
 
@@ -141,6 +143,36 @@ cudaError_t launch_leaves_batch(const BatchLeafItem* d_items, uint32_t nitems, u
                                 unsigned int* queue, DevStatus* st, int sm_count, const LeafTuning& tune,
                                 uint32_t tiles_per_pop, cudaStream_t stream);
 cudaError_t launch_forest(const ForestArgs& a, int phase, cudaStream_t stream);
+
+// CTA b of a segmented launch belongs to the handle h with beg[h] <= b < beg[h+1]
+__device__ __forceinline__ uint32_t seg_find(const uint32_t* beg, uint32_t n, uint32_t& bid, uint32_t& nb) {
+  uint32_t lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (beg[mid] <= blockIdx.x) lo = mid; else hi = mid;
+  }
+  bid = blockIdx.x - beg[lo];
+  nb = beg[lo + 1] - beg[lo];
+  return lo;
+}
+// one launch of a forest phase of a tree: kind 0 = a full band with input level p0, kind 1 = a
+// general band of levels p0 (top) .. p1 (bottom); `ctas` CTAs
+struct ForestStep {
+  uint8_t kind;
+  uint32_t p0, p1, ctas;
+};
+void forest_steps(uint32_t D, uint64_t N, int phase, std::vector<ForestStep>& out);
+// the same step of many handles' trees in one launch (batched form); handles without this
+// step have no CTAs
+struct ForestSeg {
+  const ForestArgs* args;
+  const uint32_t* beg;   // n + 1
+  const uint32_t* p0;    // per handle
+  const uint32_t* p1;
+  uint32_t n;
+};
+cudaError_t launch_forest_seg(const ForestSeg& s, int phase, int kind, uint32_t ctas, cudaStream_t stream);
+cudaError_t launch_zero_exists_seg(const ForestArgs* args, uint32_t n, cudaStream_t stream);
 int forest_launch_count(uint32_t D, int phase);
 cudaError_t launch_zero_exists(int* flag, const RoundState* rs, cudaStream_t stream);
 // bcap: bucket capacity the scratch was sized for (>= rs->buckets of every checkpoint run)

@@ -24,6 +24,8 @@
 // 1 + height, baseline per-level inserts 64 + height (height = D - level).
 // `push` holds only nonzero flags: it is all-zero between checkpoints (the compaction clears
 // what it reads), so a region-free subtree writes nothing.
+#include <vector>
+
 #include "dedup_kernels.cuh"
 #include "hash.cuh"
 #include "map.cuh"
@@ -205,8 +207,7 @@ __device__ __forceinline__ Digest shfl_down_digest(const Digest& d, uint32_t del
   return r;
 }
 
-__global__ void __launch_bounds__(FAST_THREADS, B2D_FF_MINB) forest_first_kernel(ForestArgs a0, uint32_t in) {
-  const ForestArgs a = with_round(a0);
+__device__ __forceinline__ void forest_first_body(const ForestArgs& a, uint32_t bid, uint32_t in) {
   __shared__ uint32_t ff[FF_WORDS];
   __shared__ uint32_t wbit[FAST_THREADS / 32];
   __shared__ Digest wdig[FAST_THREADS / 32];
@@ -214,7 +215,7 @@ __global__ void __launch_bounds__(FAST_THREADS, B2D_FF_MINB) forest_first_kernel
   const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
   if (t < FF_WORDS) ff[t] = 0;
   __syncthreads();
-  const uint64_t root = ((1ull << (in - FF_LEVELS)) - 1ull) + blockIdx.x;
+  const uint64_t root = ((1ull << (in - FF_LEVELS)) - 1ull) + bid;
   const uint64_t x0 = (root << FF_LEVELS) + ((1ull << FF_LEVELS) - 1ull) + 4ull * t;
   const uint64_t p0 = (x0 - 1ull) >> 1;
   uint32_t m0 = 0;   // first-occurrence inputs
@@ -349,14 +350,21 @@ __global__ void __launch_bounds__(FAST_THREADS, B2D_FF_MINB) forest_first_kernel
     insert_first_parent(a, x, a.tree[x]);
   }
 }
+__global__ void __launch_bounds__(FAST_THREADS, B2D_FF_MINB) forest_first_kernel(ForestArgs a0, uint32_t in) {
+  forest_first_body(with_round(a0), blockIdx.x, in);
+}
+__global__ void __launch_bounds__(FAST_THREADS, B2D_FF_MINB) forest_first_seg(ForestSeg s) {
+  uint32_t bid, nb;
+  const uint32_t h = seg_find(s.beg, s.n, bid, nb);
+  forest_first_body(with_round(s.args[h]), bid, s.p0[h]);
+}
 
 // Fast band: inputs at level `in`, outputs at level in - 12.
 template <int PHASE>
-__global__ void __launch_bounds__(FAST_THREADS, B2D_FAST_MINB) forest_fast_kernel(ForestArgs a0, uint32_t in) {
-  const ForestArgs a = with_round(a0);
+__device__ __forceinline__ void forest_fast_body(const ForestArgs& a, uint32_t bid, uint32_t in) {
   __shared__ uint8_t wlab[FAST_THREADS / 32];
   const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
-  const uint64_t root = ((1ull << (in - FAST_LEVELS)) - 1ull) + blockIdx.x;
+  const uint64_t root = ((1ull << (in - FAST_LEVELS)) - 1ull) + bid;
   const uint64_t x0 = (root << FAST_LEVELS) + ((1ull << FAST_LEVELS) - 1ull) + 16ull * t;
   uint8_t v[16];
   bool fast = !a.baseline;
@@ -436,15 +444,24 @@ __global__ void __launch_bounds__(FAST_THREADS, B2D_FAST_MINB) forest_fast_kerne
     if (lane == 0) band_output<PHASE>(a, root, lab);
   }
 }
+template <int PHASE>
+__global__ void __launch_bounds__(FAST_THREADS, B2D_FAST_MINB) forest_fast_kernel(ForestArgs a0, uint32_t in) {
+  forest_fast_body<PHASE>(with_round(a0), blockIdx.x, in);
+}
+template <int PHASE>
+__global__ void __launch_bounds__(FAST_THREADS, B2D_FAST_MINB) forest_fast_seg(ForestSeg s) {
+  uint32_t bid, nb;
+  const uint32_t h = seg_find(s.beg, s.n, bid, nb);
+  forest_fast_body<PHASE>(with_round(s.args[h]), bid, s.p0[h]);
+}
 
 // General band: levels [top, bot] (top <= bot <= D), level by level through shared memory.
 // Nodes at level `bot` are leaves or combine children at level bot+1 read from `lab`.
 template <int PHASE>
-__global__ void __launch_bounds__(FOREST_THREADS) forest_band_kernel(ForestArgs a0, uint32_t top, uint32_t bot) {
-  const ForestArgs a = with_round(a0);
+__device__ __forceinline__ void forest_band_body(const ForestArgs& a, uint32_t bid, uint32_t top, uint32_t bot) {
   __shared__ uint8_t buf[2][1u << (FOREST_BAND_LEVELS - 1)];
   const uint32_t H = bot - top;
-  const uint64_t root = ((1ull << top) - 1ull) + blockIdx.x;
+  const uint64_t root = ((1ull << top) - 1ull) + bid;
   uint8_t* below = buf[0];
   uint8_t* here = buf[1];
   for (int k = (int)H; k >= 0; k--) {
@@ -468,60 +485,94 @@ __global__ void __launch_bounds__(FOREST_THREADS) forest_band_kernel(ForestArgs 
     here = t;
   }
 }
+template <int PHASE>
+__global__ void __launch_bounds__(FOREST_THREADS) forest_band_kernel(ForestArgs a0, uint32_t top, uint32_t bot) {
+  forest_band_body<PHASE>(with_round(a0), blockIdx.x, top, bot);
+}
+template <int PHASE>
+__global__ void __launch_bounds__(FOREST_THREADS) forest_band_seg(ForestSeg s) {
+  uint32_t bid, nb;
+  const uint32_t h = seg_find(s.beg, s.n, bid, nb);
+  forest_band_body<PHASE>(with_round(s.args[h]), bid, s.p0[h], s.p1[h]);
+}
 
 static uint32_t band_levels(int phase) { return phase == 1 ? FF_LEVELS : FAST_LEVELS; }
 
-cudaError_t launch_forest(const ForestArgs& a, int phase, cudaStream_t stream) {
-  if (a.N <= 1) return cudaSuccess;   // one chunk: no inner nodes; the reference never pushes a region
+// The launches of one phase for a tree of depth D: full bands of band_levels(phase) levels from
+// the leaves up (kind 0, p0 = input level), then general bands of up to FOREST_BAND_LEVELS
+// levels (kind 1, p0 = top, p1 = bottom level) for what is left above.
+void forest_steps(uint32_t D, uint64_t N, int phase, std::vector<ForestStep>& out) {
+  out.clear();
+  if (N <= 1) return;   // one chunk: no inner nodes; the reference never pushes a region
   const uint32_t L = band_levels(phase);
-  uint32_t in = a.D;                  // labels at level `in` are known (leaves, or a band's output)
+  uint32_t in = D;      // labels at level `in` are known (leaves, or a band's output)
   while (in >= L) {
-    const uint32_t ctas = 1u << (in - L);
-    if (phase == 1) forest_first_kernel<<<ctas, FAST_THREADS, 0, stream>>>(a, in);
-    else forest_fast_kernel<2><<<ctas, FAST_THREADS, 0, stream>>>(a, in);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
+    out.push_back(ForestStep{0, in, 0, 1u << (in - L)});
     in -= L;
   }
-  if (in == 0) return cudaSuccess;    // the root was a fast band output
-  // remaining levels [0, bot]: bot = D when no fast band ran (start from the leaves), else in-1
-  int bot = (in == a.D) ? (int)a.D : (int)in - 1;
+  if (in == 0) return;  // the root was a full band's output
+  // remaining levels [0, bot]: bot = D when no full band ran (start from the leaves), else in-1
+  int bot = (in == D) ? (int)D : (int)in - 1;
   while (bot >= 0) {
     int top = bot - (int)FOREST_BAND_LEVELS + 1;
     if (top < 0) top = 0;
-    const uint32_t ctas = 1u << top;
-    if (phase == 1) forest_band_kernel<1><<<ctas, FOREST_THREADS, 0, stream>>>(a, (uint32_t)top, (uint32_t)bot);
-    else forest_band_kernel<2><<<ctas, FOREST_THREADS, 0, stream>>>(a, (uint32_t)top, (uint32_t)bot);
+    out.push_back(ForestStep{1, (uint32_t)top, (uint32_t)bot, 1u << top});
+    bot = top - 1;
+  }
+}
+
+cudaError_t launch_forest(const ForestArgs& a, int phase, cudaStream_t stream) {
+  std::vector<ForestStep> steps;
+  forest_steps(a.D, a.N, phase, steps);
+  for (const ForestStep& st : steps) {
+    if (st.kind == 0) {
+      if (phase == 1) forest_first_kernel<<<st.ctas, FAST_THREADS, 0, stream>>>(a, st.p0);
+      else forest_fast_kernel<2><<<st.ctas, FAST_THREADS, 0, stream>>>(a, st.p0);
+    } else {
+      if (phase == 1) forest_band_kernel<1><<<st.ctas, FOREST_THREADS, 0, stream>>>(a, st.p0, st.p1);
+      else forest_band_kernel<2><<<st.ctas, FOREST_THREADS, 0, stream>>>(a, st.p0, st.p1);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    bot = top - 1;
   }
   return cudaSuccess;
 }
 
 int forest_launch_count(uint32_t D, int phase) {
-  if (D == 0) return 0;
-  int c = 0;
-  uint32_t in = D;
-  const uint32_t L = band_levels(phase);
-  while (in >= L) { c++; in -= L; }
-  if (in == 0) return c;
-  int bot = (in == D) ? (int)D : (int)in - 1;
-  while (bot >= 0) {
-    int top = bot - (int)FOREST_BAND_LEVELS + 1;
-    if (top < 0) top = 0;
-    c++;
-    bot = top - 1;
-  }
-  return c;
+  std::vector<ForestStep> steps;
+  forest_steps(D, D == 0 ? 1 : 2, phase, steps);
+  return (int)steps.size();
 }
 
-__global__ void zero_exists_kernel(int* flag, const RoundState* rs) {
+cudaError_t launch_forest_seg(const ForestSeg& s, int phase, int kind, uint32_t ctas, cudaStream_t stream) {
+  if (ctas == 0) return cudaSuccess;
+  if (kind == 0) {
+    if (phase == 1) forest_first_seg<<<ctas, FAST_THREADS, 0, stream>>>(s);
+    else forest_fast_seg<2><<<ctas, FAST_THREADS, 0, stream>>>(s);
+  } else {
+    if (phase == 1) forest_band_seg<1><<<ctas, FOREST_THREADS, 0, stream>>>(s);
+    else forest_band_seg<2><<<ctas, FOREST_THREADS, 0, stream>>>(s);
+  }
+  return cudaGetLastError();
+}
+
+__device__ __forceinline__ void zero_exists_kernel_body(int* flag, const RoundState* rs) {
   if (!rs->baseline) return;   // only the baseline tests the stale zero digest
   Digest z;
   z.w[0] = z.w[1] = z.w[2] = z.w[3] = 0u;
   const MapView m = rs->map;
   *flag = map_find(m, z) <= m.cap ? 1 : 0;
+}
+__global__ void zero_exists_kernel(int* flag, const RoundState* rs) { zero_exists_kernel_body(flag, rs); }
+
+__global__ void zero_exists_seg(const ForestArgs* args, uint32_t n) {
+  const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h < n) zero_exists_kernel_body(const_cast<int*>(args[h].zero_exists), args[h].rs);   // the flag this step sets
+}
+
+cudaError_t launch_zero_exists_seg(const ForestArgs* args, uint32_t n, cudaStream_t stream) {
+  zero_exists_seg<<<(n + 127) / 128, 128, 0, stream>>>(args, n);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_zero_exists(int* flag, const RoundState* rs, cudaStream_t stream) {

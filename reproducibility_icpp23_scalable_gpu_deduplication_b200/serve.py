@@ -37,7 +37,7 @@ __all__ = ["CheckpointServer", "Request"]
 
 class Request:
     __slots__ = ("client", "buffer", "nbytes", "make_baseline", "arrival", "admitted", "launched", "done", "rc",
-                 "diff_len", "checksum", "ready", "seq", "host")
+                 "diff_len", "checksum", "ready", "seq", "host", "launch_s", "batch_size")
 
     def __init__(self, client, buffer, make_baseline, arrival, seq):
         self.client, self.buffer, self.make_baseline, self.arrival, self.seq = client, buffer, make_baseline, arrival, seq
@@ -48,6 +48,8 @@ class Request:
         self.checksum = None
         self.ready = None
         self.host = None          # the diff in pinned host memory (with enable_host_copy)
+        self.launch_s = None      # host seconds its batch's launch call took
+        self.batch_size = 1
 
     @property
     def latency(self):
@@ -218,6 +220,10 @@ class CheckpointServer:
                 r.launched = now
             b.launch([self.clients[r.client].handle for r in batch], [r.buffer for r in batch],
                      [r.make_baseline for r in batch], stream=stream)
+            host = self.clock() - now
+            for r in batch:
+                r.launch_s = host
+                r.batch_size = len(batch)
             reqs.extend(batch)
             self.batches += 1
 

@@ -150,14 +150,15 @@ def test_batch_rejects_duplicate_handles(cuda):
             b.checkpoint([h, h], [x, x])
 
 
-@pytest.mark.parametrize("mode,batch_diff", [(0, 1), (1, 1), (2, 1), (0, 0), (1, 0)])
-def test_batch_graph_modes_same(cuda, mode, batch_diff):
-    """direct launches, graph replay and graph-from-second-batch, with the diff assembly shared
-    across handles or per handle, give the same diffs"""
+@pytest.mark.parametrize("mode,batch_diff,batch_forest",
+                         [(0, 1, 1), (1, 1, 1), (2, 1, 1), (0, 1, 0), (1, 1, 0), (0, 0, 0), (1, 0, 1)])
+def test_batch_graph_modes_same(cuda, mode, batch_diff, batch_forest):
+    """direct launches, graph replay and graph-from-second-batch, with the forest phases and the
+    diff assembly shared across handles or per handle, give the same diffs"""
     specs = SPECS[:4] + SPECS[7:9]
     rounds = 3
     baselines = [[True] * len(specs)] + [[False] * len(specs) for _ in range(rounds - 1)]
-    with CheckpointBatch(graph=mode, batch_diff=batch_diff) as b:
+    with CheckpointBatch(graph=mode, batch_diff=batch_diff, batch_forest=batch_forest) as b:
         got, _, _ = run_batch(specs, rounds, baselines, b)
         assert b.get_param("graph") == mode
         assert b.get_param("graphs") == {0: 0, 1: 1, 2: 1}[mode]
