@@ -606,9 +606,23 @@ def main():
         r1.record(stream)
         torch.cuda.synchronize()
         r_ms = r0.elapsed_time(r1)
+        ok = bool(torch.equal(out, x.view(torch.uint8).reshape(-1)[:nbytes]))
+        # the same chain with the diffs resident in device memory
+        ddiffs = [torch.from_numpy(dh).to(dev) for dh in diffs]
+        out.zero_()
+        rd.restart_device(out, ddiffs, 3)
+        torch.cuda.synchronize()
+        r0.record(stream)
+        rd.restart_device(out, ddiffs, 3)
+        r1.record(stream)
+        torch.cuda.synchronize()
+        rd_ms = r0.elapsed_time(r1)
+        ok_d = bool(torch.equal(out, x.view(torch.uint8).reshape(-1)[:nbytes]))
         restart = {"value": round(nbytes / (r_ms * 1e-3) / GB, 2), "unit": "GB/s", "ms": round(r_ms, 3),
-                   "diffs": 4, "h2d_bytes": int(sum(d.nbytes for d in diffs)),
-                   "identical": bool(torch.equal(out, x.view(torch.uint8).reshape(-1)[:nbytes]))}
+                   "diffs": 4, "h2d_bytes": int(sum(d.nbytes for d in diffs)), "identical": ok,
+                   "device_diffs": {"value": round(nbytes / (rd_ms * 1e-3) / GB, 2), "unit": "GB/s",
+                                    "ms": round(rd_ms, 3), "identical": ok_d}}
+        del ddiffs
         rd.close()
         del rs, diffs, out, x
         torch.cuda.empty_cache()

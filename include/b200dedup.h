@@ -123,6 +123,13 @@ int b2d_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* d
 int b2d_restart_files(b2d_dedup* d, void* d_out, uint64_t len, const char* const* chkpt_filenames,
                       uint32_t num_files, uint32_t chkpt_id, const char* logname);
 
+/* b2d_restart with the diffs already in device memory (d_diffs[i]: device pointer, sizes[i]:
+ * bytes): no host copies of the diffs, only of their 32-byte headers and repeat tables, so a
+ * restart chain kept on the GPU runs at device speed.  No reference counterpart (the
+ * reference's restart takes host views, src/tree_approach.cpp:1807-1813). */
+int b2d_restart_device(b2d_dedup* d, void* d_out, uint64_t len, const void* const* d_diffs, const uint64_t* sizes,
+                       uint32_t num_diffs, uint32_t chkpt_id);
+
 /* Restart that allocates nothing (no counterpart in the reference).  For callers that cannot
  * call cudaMalloc: a process restoring a checkpoint after the device ran out of memory, or a
  * runtime whose device memory is all owned by its own pool and budget.  Same result as

@@ -36,6 +36,7 @@ SIGNATURES = [
     ("b2d_checkpoint_file", _int, [_vp, _vp, _u64, _cc, _cc, _int]),
     ("b2d_restart", _int, [_vp, _vp, _u64, ctypes.POINTER(_vp), ctypes.POINTER(_u64), _u32, _u32, _cc]),
     ("b2d_restart_files", _int, [_vp, _vp, _u64, ctypes.POINTER(_cc), _u32, _u32, _cc]),
+    ("b2d_restart_device", _int, [_vp, _vp, _u64, ctypes.POINTER(_vp), ctypes.POINTER(_u64), _u32, _u32]),
     ("b2d_restart_noalloc", _int, [_vp, _u64, ctypes.POINTER(_vp), ctypes.POINTER(_u64), _u32, _u32, _vp]),
     ("b2d_num_first_ocur", _int, [_vp, ctypes.POINTER(_u64)]),
     ("b2d_num_shift_dupl", _int, [_vp, ctypes.POINTER(_u64)]),

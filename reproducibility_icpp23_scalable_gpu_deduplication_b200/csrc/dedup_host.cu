@@ -86,7 +86,7 @@ __global__ void map_special_init_kernel(MapSlot* special) {
   special->key_lo = 0;
   special->key_hi = 0;
   special->val = ~0ull;
-  special->tree = MAP_TREE_PENDING;
+  special->spare = 0;
   special->pad = 0;   // unoccupied
 }
 
@@ -103,11 +103,8 @@ __global__ void map_rehash_kernel(MapView from, MapView to, DevStatus* st) {
     Digest d;
     d.w[0] = (uint32_t)s.key_lo; d.w[1] = (uint32_t)(s.key_lo >> 32);
     d.w[2] = (uint32_t)s.key_hi; d.w[3] = (uint32_t)(s.key_hi >> 32);
-    const MapRef r = map_insert(to, d, s.val, s.tree, st);
-    if (r.found) {
-      to.slots[r.slot].val = s.val;
-      to.slots[r.slot].tree = s.tree;
-    }
+    const MapRef r = map_insert_packed(to, d, s.val, st);
+    if (r.found) to.slots[r.slot].val = s.val;
   }
 }
 
@@ -415,7 +412,8 @@ int prepare_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, bool make
   if (nc > 0x7fffffffull) return B2D_ERR_ARG;
   const bool baseline = (d->current_id == 0) || make_baseline;
   if (!baseline && (!d->have_tree || nc != d->n)) return B2D_ERR_LEN_CHANGED;
-  if (d->current_id + 1u > MAX_BUCKETS) return B2D_ERR_UNSUPPORTED;   // source-checkpoint buckets
+  // source-checkpoint buckets, and the map's checkpoint field (MAP_TREE_PENDING is reserved)
+  if (d->current_id + 1u > MAX_BUCKETS || d->current_id >= MAP_TREE_PENDING) return B2D_ERR_UNSUPPORTED;
   d->diff_valid = false;
   d->data = d_data;
   d->data_len = len;
@@ -741,10 +739,33 @@ bool parse_hdr(const uint8_t* b, uint64_t size, HostHdr& h) {
 }
 
 int do_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* diffs, const uint64_t* sizes,
-               uint32_t count, uint32_t id) {
+               uint32_t count, uint32_t id, const void* const* ddiffs = nullptr) {
   using clk = std::chrono::high_resolution_clock;
   const auto t0 = clk::now();
-  if (!d_out || !diffs || !sizes || id >= count) return B2D_ERR_ARG;
+  if (!d_out || (!diffs && !ddiffs) || !sizes || id >= count) return B2D_ERR_ARG;
+  // device-resident diffs: the host reads only their headers and repeat tables (small copies)
+  std::vector<std::vector<uint8_t>> hmeta;
+  std::vector<const uint8_t*> hptr;
+  if (ddiffs) {
+    hmeta.resize(count);
+    hptr.assign(count, nullptr);
+    // the same chain walk as below: from `id` down while the index is not below the last ref_id
+    for (int idx = (int)id; idx >= 0; idx--) {
+      if (!ddiffs[idx] || sizes[idx] < 32) return B2D_ERR_FORMAT;
+      uint8_t hdr[32];
+      B2D_CU(cudaMemcpy(hdr, ddiffs[idx], 32, cudaMemcpyDeviceToHost));
+      HostHdr hh;
+      if (!parse_hdr(hdr, sizes[idx], hh)) return B2D_ERR_FORMAT;
+      auto& m = hmeta[idx];
+      m.assign(hh.count_off + 8ull * hh.P, 0);
+      std::memcpy(m.data(), hdr, 32);
+      if (hh.P) B2D_CU(cudaMemcpy(m.data() + hh.count_off, static_cast<const uint8_t*>(ddiffs[idx]) + hh.count_off,
+                                  8ull * hh.P, cudaMemcpyDeviceToHost));
+      hptr[idx] = m.data();
+      if (idx - 1 < (int)hh.ref_id) break;
+    }
+    diffs = hptr.data();
+  }
   HostHdr h;
   if (!parse_hdr(diffs[id], sizes[id], h)) return B2D_ERR_FORMAT;
   if (len < h.datalen) return B2D_ERR_ARG;
@@ -774,7 +795,7 @@ int do_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* di
   B2D_CU(d->r_diff.reserve(max_size + 16));
   B2D_CU(d->state.reserve(1));
   B2D_CU(d->state_h.reserve(1));
-  B2D_CU(d->r_stage.reserve(max_size + 16 + 8 * max_ids));
+  if (!ddiffs) B2D_CU(d->r_stage.reserve(max_size + 16 + 8 * max_ids));
   B2D_CU(cudaMemsetAsync(d->state.p, 0, sizeof(DevState), d->stream));
   d->launches = 0;
   double copy_time = 0;
@@ -801,14 +822,17 @@ int do_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* di
     // stage the diff (plus its repeat-table running counts) in pinned memory, then one copy
     const uint32_t delta = (uint32_t)((16u - (hh.data_off & 15u)) & 15u);
     const uint64_t ncum = (uint64_t)hh.chkpt_id + 1;
-    // pinned (page-locked) diffs are copied straight to the device; others go through the
-    // handle's pinned staging buffer, reused per diff
-    cudaPointerAttributes pa;
-    const bool pinned = cudaPointerGetAttributes(&pa, diffs[idx]) == cudaSuccess && pa.type == cudaMemoryTypeHost;
-    if (!pinned) (void)cudaGetLastError();
+    // device diffs and pinned (page-locked) host diffs are copied straight to the scratch;
+    // other host diffs go through the handle's pinned staging buffer, reused per diff
+    bool pinned = ddiffs != nullptr;
+    if (!ddiffs) {
+      cudaPointerAttributes pa;
+      pinned = cudaPointerGetAttributes(&pa, diffs[idx]) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+      if (!pinned) (void)cudaGetLastError();
+    }
     if (!pinned) B2D_CU(cudaStreamSynchronize(d->stream));
     const auto c0 = clk::now();
-    const uint8_t* src = diffs[idx];
+    const uint8_t* src = ddiffs ? static_cast<const uint8_t*>(ddiffs[idx]) : diffs[idx];
     if (!pinned) {
       memcpy(d->r_stage.p + delta, diffs[idx], sizes[idx]);
       src = d->r_stage.p + delta;
@@ -822,7 +846,8 @@ int do_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* di
       if (ck < ncum) cum[ck] = cnt; else bad_row = true;
     }
     for (uint64_t t = 1; t < ncum; t++) cum[t] += cum[t - 1];
-    B2D_CU(cudaMemcpyAsync(d->r_diff.p + delta, src, sizes[idx], cudaMemcpyHostToDevice, d->stream));
+    B2D_CU(cudaMemcpyAsync(d->r_diff.p + delta, src, sizes[idx],
+                           ddiffs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, d->stream));
     B2D_CU(cudaMemcpyAsync(d->r_cum.p, cum.data(), sizeof(unsigned long long) * ncum, cudaMemcpyHostToDevice,
                            d->stream));
     if (idx == (int)id) {
@@ -1624,6 +1649,14 @@ int b2d_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* d
       write_restart_log(d, chkpt_id, ln);
     }
     return rc;
+  })
+}
+
+int b2d_restart_device(b2d_dedup* d, void* d_out, uint64_t len, const void* const* d_diffs, const uint64_t* sizes,
+                       uint32_t num_diffs, uint32_t chkpt_id) {
+  B2D_GUARD({
+    if (!d || !d_diffs) return B2D_ERR_ARG;
+    return do_restart(d, d_out, len, nullptr, sizes, num_diffs, chkpt_id, d_diffs);
   })
 }
 

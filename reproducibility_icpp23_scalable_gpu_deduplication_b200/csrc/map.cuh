@@ -7,12 +7,14 @@
 //
 // Slot layout (32 bytes, one quarter of a 128-byte line):
 //   key  : two u64 words, claimed with one 128-bit atomicCAS (EMPTY = all ones)
-//   val  : u64 = (priority << 32) | node.  Every insert of the current checkpoint applies
-//          atomicMin to it, so the value left behind is the one the reference's sequential
-//          execution order inserts first (leaves by index, then first-occurrence parents by
-//          level and index, then the baseline's per-level inserts).  node = low 32 bits.
-//   tree : checkpoint id of the first insert; UINT32_MAX while the inserting thread has
-//          claimed the key but not yet stored it (readers treat that as "this checkpoint").
+//   val  : u64 = priority << 45 | checkpoint << 32 | node.  Every insert of the current
+//          checkpoint applies atomicMin to it; within one checkpoint the checkpoint field is
+//          the same, so the value left behind is the one the reference's sequential execution
+//          order inserts first (leaves by index, then first-occurrence parents by level and
+//          index, then the baseline's per-level inserts).  One atomic sets the owner and its
+//          checkpoint together.  All ones (checkpoint field MAP_TREE_PENDING) while the
+//          inserting thread has claimed the key but not yet merged its value: readers treat
+//          that as "this checkpoint".  Checkpoint ids are below MAP_TREE_PENDING.
 // The digest equal to the EMPTY pattern is kept in one extra slot at index `cap`.
 #pragma once
 #include "common.cuh"
@@ -23,8 +25,8 @@ struct __align__(32) MapSlot {
   unsigned long long key_lo;
   unsigned long long key_hi;
   unsigned long long val;
-  uint32_t tree;
-  uint32_t pad;
+  uint32_t spare;
+  uint32_t pad;        // special slot only: 1 once occupied
 };
 static_assert(sizeof(MapSlot) == 32, "slot must be 32 bytes");
 
@@ -33,7 +35,17 @@ struct __align__(16) Key128 {
 };
 
 constexpr unsigned long long MAP_EMPTY = ~0ull;
-constexpr uint32_t MAP_TREE_PENDING = 0xffffffffu;
+constexpr uint32_t MAP_TREE_BITS = 13;
+constexpr uint32_t MAP_TREE_PENDING = (1u << MAP_TREE_BITS) - 1u;   // 8191
+
+// (priority << 32 | node) of the inserting order + the checkpoint id -> the stored value
+__device__ __forceinline__ unsigned long long map_pack(unsigned long long val, uint32_t cur) {
+  return ((val >> 32) << (32 + MAP_TREE_BITS)) | ((unsigned long long)(cur & MAP_TREE_PENDING) << 32) |
+         (val & 0xffffffffull);
+}
+__device__ __forceinline__ uint32_t map_val_tree(unsigned long long v) {
+  return (uint32_t)(v >> 32) & MAP_TREE_PENDING;
+}
 
 struct MapView {
   MapSlot* slots;      // cap + 1 slots
@@ -99,11 +111,11 @@ __device__ __forceinline__ Key128 atomic_cas_key(MapSlot* s, Key128 cmp, Key128 
   return atomicCAS(reinterpret_cast<Key128*>(&s->key_lo), cmp, val);
 }
 
-// Insert-if-absent.  On success the caller's value is merged with atomicMin and the
-// checkpoint id stored.  On an existing key nothing is written here; the caller decides
-// (through map_merge_current) whether the entry belongs to the current checkpoint.
-__device__ __forceinline__ MapRef map_insert(const MapView& m, const Digest& d, unsigned long long val,
-                                             uint32_t cur, DevStatus* st) {
+// Insert-if-absent of an already packed value (map_pack).  On success the value is merged
+// with atomicMin.  On an existing key nothing is written here; the caller decides (through
+// map_merge_current) whether the entry belongs to the current checkpoint.
+__device__ __forceinline__ MapRef map_insert_packed(const MapView& m, const Digest& d, unsigned long long val,
+                                                    DevStatus* st) {
   const Key128 k = digest_key(d);
   MapRef r{0, false, false, ~0ull};
   if (key_is_empty_pattern(k)) {
@@ -113,10 +125,7 @@ __device__ __forceinline__ MapRef map_insert(const MapView& m, const Digest& d, 
     r.slot = m.cap;
     r.found = true;
     r.inserted = (old == 0u);
-    if (r.inserted) {
-      atomicExch(&s->tree, cur);
-      atomicAdd(m.size, 1ull);   // one slot, rare: no aggregation needed
-    }
+    if (r.inserted) atomicAdd(m.size, 1ull);   // one slot, rare: no aggregation needed
     return r;
   }
   // a key with an all-ones half could be confused with a half-written slot: always CAS
@@ -141,7 +150,6 @@ __device__ __forceinline__ MapRef map_insert(const MapView& m, const Digest& d, 
       const Key128 old = atomic_cas_key(s, empty, k);
       if (old.lo == MAP_EMPTY && old.hi == MAP_EMPTY) {
         r.prev = atomicMin(&s->val, val);
-        atomicExch(&s->tree, cur);
         count_insert(m.size);
         r.slot = i; r.found = true; r.inserted = true;
         return r;
@@ -157,15 +165,22 @@ __device__ __forceinline__ MapRef map_insert(const MapView& m, const Digest& d, 
   return r;
 }
 
+// insert with `val` = priority << 32 | node, stored for checkpoint `cur`
+__device__ __forceinline__ MapRef map_insert(const MapView& m, const Digest& d, unsigned long long val,
+                                             uint32_t cur, DevStatus* st) {
+  return map_insert_packed(m, d, map_pack(val, cur), st);
+}
+
 // An existing entry belongs to the current checkpoint when its id is `cur` or still
 // pending (claimed by a concurrent inserter of this launch).  In that case the lower
-// (priority, node) value wins, matching "first insert in sequential order".
+// (priority, node) value wins, matching "first insert in sequential order".  An entry of an
+// older checkpoint is never changed by this one, so its id cannot change under the test.
 __device__ __forceinline__ bool map_merge_current(const MapView& m, uint64_t slot, unsigned long long val,
                                                   uint32_t cur, unsigned long long* prev = nullptr) {
   MapSlot* s = &m.slots[slot];
-  const uint32_t t = *reinterpret_cast<volatile uint32_t*>(&s->tree);
-  if (t == cur || t == MAP_TREE_PENDING) {
-    const unsigned long long p = atomicMin(&s->val, val);
+  const uint32_t t = map_val_tree(*reinterpret_cast<volatile unsigned long long*>(&s->val));
+  if (t == (cur & MAP_TREE_PENDING) || t == MAP_TREE_PENDING) {
+    const unsigned long long p = atomicMin(&s->val, map_pack(val, cur));
     if (prev) *prev = p;
     return true;
   }
@@ -175,6 +190,8 @@ __device__ __forceinline__ bool map_merge_current(const MapView& m, uint64_t slo
 __device__ __forceinline__ uint32_t map_node(const MapView& m, uint64_t slot) {
   return (uint32_t)(m.slots[slot].val & 0xffffffffull);
 }
-__device__ __forceinline__ uint32_t map_tree(const MapView& m, uint64_t slot) { return m.slots[slot].tree; }
+__device__ __forceinline__ uint32_t map_tree(const MapView& m, uint64_t slot) {
+  return map_val_tree(m.slots[slot].val);
+}
 
 }  // namespace b2d

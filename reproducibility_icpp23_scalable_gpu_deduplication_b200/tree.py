@@ -158,6 +158,19 @@ class TreeDeduplicator:
             check(rc, "b2d_restart")
         return rc
 
+    def restart_device(self, out, chkpts, chkpt_id, check_status=True):
+        """restart from diffs already in device memory (CUDA uint8 tensors, e.g. diffs copied
+        with diff_device or kept on the GPU); same result as ``restart``."""
+        self._sync_stream()
+        p, n = _dev_ptr(out)
+        ds = [_dev_ptr(c) for c in chkpts]
+        ptrs = (ctypes.c_void_p * len(ds))(*[q.value for q, _ in ds])
+        sizes = (ctypes.c_uint64 * len(ds))(*[m for _, m in ds])
+        rc = lib().b2d_restart_device(self._h, p, n, ptrs, sizes, len(ds), int(chkpt_id))
+        if check_status:
+            check(rc, "b2d_restart_device")
+        return rc
+
     def restart_files(self, out, filenames, chkpt_id, logname=None, check_status=True):
         self._sync_stream()
         p, n = _dev_ptr(out)

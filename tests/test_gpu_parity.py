@@ -49,11 +49,17 @@ def run_both(bufs, cs, kind=HASH_MURMUR3, baselines=None, restart=True, tma=True
         assert gd[-1] == od[-1], (i, parse_header(gd[-1]))
         assert (g.num_first_ocur(), g.num_shift_dupl()) == (o.num_first_ocur(), o.num_shift_dupl())
     if restart:
+        dev_diffs = [to_dev(np.frombuffer(x, np.uint8)) for x in gd]
         for i, b in enumerate(bufs):
             want, rc = O.restart(od, i)
             out = torch.zeros(len(b), dtype=torch.uint8, device="cuda")
             grc = g.restart(out, gd, i, check_status=False)
             assert (grc == 0) == (rc == 0), (i, grc, rc)
+            assert out.cpu().numpy().tobytes() == want.tobytes(), i
+            # the same chain from device-resident diffs
+            out.zero_()
+            drc = g.restart_device(out, dev_diffs, i, check_status=False)
+            assert drc == grc, (i, drc, grc)
             assert out.cpu().numpy().tobytes() == want.tobytes(), i
     run_both.map_stats = g.map_stats()
     g.close()
