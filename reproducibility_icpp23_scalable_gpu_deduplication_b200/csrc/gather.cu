@@ -18,6 +18,11 @@
 
 namespace b2d {
 
+// chunk groups each lane keeps in flight in the data gather
+#ifndef B2D_GATHER_UNROLL
+#define B2D_GATHER_UNROLL 4
+#endif
+
 constexpr uint32_t COMPACT_THREADS = 512;
 
 // Every kernel below is a body over a virtual grid (bid of nb CTAs) with two launchers: one
@@ -515,7 +520,7 @@ __device__ __forceinline__ void gather_vec_body(const DiffArgs& a, uint32_t bid,
   if (units == LPC) {
     // one 16-byte unit per lane per chunk: GATHER_UNROLL chunk groups per iteration, loads
     // first then stores, so each lane keeps several loads in flight (large diffs, baselines)
-    constexpr uint32_t U = 4;
+    constexpr uint32_t U = B2D_GATHER_UNROLL;
     const uint32_t sub = lane % LPC;
     for (; k0 + (uint64_t)CPW * U <= k1; k0 += (uint64_t)CPW * U) {
       uint4 val[U];
