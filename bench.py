@@ -213,7 +213,7 @@ def run_batched(args, rank, world, dev):
     """256 buffers of log-uniform sizes: the batch API against the same buffers one at a time."""
     import torch
 
-    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import CheckpointBatch, TreeDeduplicator, synth
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import CheckpointBatch, TreeDeduplicator, replicas, synth
 
     sizes = synth.batched_sizes(count=args.buffers, hi=args.max_buffer)
     total = sum(sizes)
@@ -280,14 +280,10 @@ def run_batched(args, rank, world, dev):
         t_batch, s_batch, l_batch = series_pass(batch_step)
     same = s_plain == s_batch or args.no_plain
     ms_b, ms_p = statistics.mean(t_batch), statistics.mean(t_plain)
-    tt = torch.tensor([ms_b, ms_p], device=dev)
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-    ms_b, ms_p = float(tt[0]), float(tt[1])
-    value = world * total / (ms_b * 1e-3) / GB
-    plain = world * total / (ms_p * 1e-3) / GB
+    rate_b, ms_b = replicas.throughput(ms_b, total, dev)
+    rate_p, ms_p = replicas.throughput(ms_p, total, dev) if not args.no_plain else (float("nan"), ms_p)
+    value = rate_b / GB
+    plain = rate_p / GB
     peak, peak_kind = measured_peak()
     alg = total + 32 * chunks
     line = {
@@ -493,7 +489,8 @@ def main():
     import torch
     import torch.distributed as dist
 
-    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import HASH_MD5, HASH_MURMUR3, TreeDeduplicator, synth
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import (HASH_MD5, HASH_MURMUR3, TreeDeduplicator,
+                                                                        replicas, synth)
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -554,11 +551,9 @@ def main():
         dist.barrier()
     ms = start.elapsed_time(stop) if flush is None else sum(step_ms)
     del flush
-    t = torch.tensor([ms], device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * args.steps * nbytes / (ms_max * 1e-3) / GB
+    # replicas: the slowest rank's time, every rank's bytes
+    rate, ms_max = replicas.throughput(ms, args.steps * nbytes, dev)
+    value = rate / GB
     leaf_ms = 1e3 * statistics.mean(leaf_s)   # 0 when the graph runs without timing events
     del bufs
 
@@ -579,10 +574,7 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize()
     e_ms = e0.elapsed_time(e1)
-    te = torch.tensor([e_ms], device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * len(e2e_bufs) * nbytes / (float(te.item()) * 1e-3) / GB if e2e_bufs else None
+    e2e_value = replicas.throughput(e_ms, len(e2e_bufs) * nbytes, dev)[0] / GB if e2e_bufs else None
     del e2e_bufs
 
     # restart: rebuild the last checkpoint of a fresh 4-checkpoint series from its diffs held in

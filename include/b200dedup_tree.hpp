@@ -137,6 +137,52 @@ class TreeDeduplicator {
   b2d_dedup* h_ = nullptr;
 };
 
+// Batched checkpoints (b2d_batch_*): one checkpoint of each of many TreeDeduplicators' buffers
+// per call, sharing launches; each deduplicator's result is what its own checkpoint gives.
+// No reference counterpart.
+class CheckpointBatch {
+ public:
+  CheckpointBatch() { check(b2d_batch_create(&b_), "CheckpointBatch"); }
+  ~CheckpointBatch() {
+    if (b_) b2d_batch_destroy(b_);
+  }
+  CheckpointBatch(const CheckpointBatch&) = delete;
+  CheckpointBatch& operator=(const CheckpointBatch&) = delete;
+
+  void set_param(const char* name, int64_t value) { check(b2d_batch_set_param(b_, name, value), name); }
+  // checkpoint device buffers data[i] (len[i] bytes) through dedups[i]; make_baseline may be
+  // empty (no forced baselines).  Diffs are then read per deduplicator (diff()).
+  void checkpoint(std::vector<TreeDeduplicator*>& dedups, const std::vector<uint8_t*>& data,
+                  const std::vector<size_t>& len, const std::vector<int>& make_baseline = {}) {
+    std::vector<b2d_dedup*> hs;
+    std::vector<const void*> ptrs;
+    std::vector<uint64_t> lens;
+    for (size_t i = 0; i < dedups.size(); i++) {
+      hs.push_back(dedups[i]->handle());
+      ptrs.push_back(data[i]);
+      lens.push_back(len[i]);
+    }
+    std::vector<int> rcs(dedups.size(), 0);
+    check(b2d_batch_checkpoint(b_, hs.data(), ptrs.data(), lens.data(),
+                               make_baseline.empty() ? nullptr : make_baseline.data(), (uint32_t)hs.size(),
+                               rcs.data()),
+          "batch checkpoint");
+  }
+
+ private:
+  b2d_batch* b_ = nullptr;
+};
+
+// the last diff of a deduplicator, copied to the host
+inline std::vector<uint8_t> diff(TreeDeduplicator& d) {
+  const void* p = nullptr;
+  uint64_t n = 0;
+  check(b2d_diff_device(d.handle(), &p, &n), "diff");
+  std::vector<uint8_t> out(n);
+  check(b2d_copy_diff(d.handle(), out.data(), n), "diff");
+  return out;
+}
+
 }  // namespace b2d
 
 #endif  // B200DEDUP_TREE_HPP

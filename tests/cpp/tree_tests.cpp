@@ -3,6 +3,7 @@
 //        one incremental checkpoint, restart both, check num_first_ocur()/num_shift_dupl()
 //   tree_chkpt <chunk_size> <num_chkpts>  : test/tree_chkpt.cpp -- 1 MiB of fresh random bytes
 //        per checkpoint, restart every checkpoint and compare
+//   batch <count>                         : CheckpointBatch against one-at-a-time checkpoints
 // Exit status 0 = pass, like the reference's ctest executables.
 #include <cuda_runtime.h>
 
@@ -87,12 +88,58 @@ static int run_tree_chkpt(uint32_t chunk_size, uint32_t num_chkpts) {
   return 0;
 }
 
+// batch <count> : `count` buffers of uneven sizes, 3 checkpoints through a CheckpointBatch and
+// through separate deduplicators one at a time; every diff must be equal
+static int run_batch(uint32_t count) {
+  std::mt19937_64 rng(7);
+  std::vector<size_t> len;
+  std::vector<std::vector<uint8_t>> host;
+  std::vector<uint8_t*> dev;
+  for (uint32_t i = 0; i < count; i++) {
+    len.push_back(4096 + (size_t)(rng() % (1u << 20)));
+    host.emplace_back(len.back());
+    for (auto& x : host.back()) x = (uint8_t)(rng() & 0xff);
+    dev.push_back(dev_copy(host.back()));
+  }
+  std::vector<b2d::TreeDeduplicator*> batched, alone;
+  for (uint32_t i = 0; i < count; i++) {
+    batched.push_back(new b2d::TreeDeduplicator(128));
+    alone.push_back(new b2d::TreeDeduplicator(128));
+  }
+  b2d::CheckpointBatch batch;
+  int rc = 0;
+  for (int c = 0; c < 3 && rc == 0; c++) {
+    if (c > 0)
+      for (uint32_t i = 0; i < count; i++) {   // rewrite a few chunks of every buffer
+        for (size_t k = 0; k < 64 && k < host[i].size(); k++) host[i][(rng() % host[i].size())] ^= 0x5a;
+        cudaMemcpy(dev[i], host[i].data(), len[i], cudaMemcpyHostToDevice);
+      }
+    batch.checkpoint(batched, dev, len);
+    for (uint32_t i = 0; i < count; i++) {
+      std::vector<uint8_t> want;
+      alone[i]->checkpoint(dev[i], len[i], want, c == 0);
+      if (b2d::diff(*batched[i]) != want) {
+        printf("batch checkpoint %d buffer %u differs\n", c, i);
+        rc = 1;
+      }
+    }
+  }
+  for (uint32_t i = 0; i < count; i++) {
+    delete batched[i];
+    delete alone[i];
+    cudaFree(dev[i]);
+  }
+  if (rc == 0) printf("batch of %u: all diffs equal\n", count);
+  return rc;
+}
+
 int main(int argc, char** argv) {
   try {
     if (argc == 6 && std::string(argv[1]) == "case")
       return run_case(argv[2], argv[3], strtoull(argv[4], nullptr, 10), strtoull(argv[5], nullptr, 10));
     if (argc == 4 && std::string(argv[1]) == "tree_chkpt")
       return run_tree_chkpt((uint32_t)atoi(argv[2]), (uint32_t)atoi(argv[3]));
+    if (argc == 3 && std::string(argv[1]) == "batch") return run_batch((uint32_t)atoi(argv[2]));
   } catch (const b2d::Error& e) {
     printf("error: %s\n", e.what());
     return 2;

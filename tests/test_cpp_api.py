@@ -43,3 +43,9 @@ def test_cpp_reference_test_cases(cuda):
 def test_cpp_tree_chkpt(cuda, cs):
     r = subprocess.run([build_cpp(), "tree_chkpt", str(cs), "10"], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
+
+
+@pytest.mark.gpu
+def test_cpp_checkpoint_batch(cuda):
+    r = subprocess.run([build_cpp(), "batch", "9"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
