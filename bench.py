@@ -269,7 +269,7 @@ def run_batched(args, rank, world, dev):
             h.close()
         del ss
         torch.cuda.empty_cache()
-    tuned = {k: batch.get_param(k) for k in ("leaf_stages", "leaf_ctas_per_sm", "tiles_per_pop", "streams")}
+    tuned = {k: batch.get_param(k) for k in ("shared", "leaf_stages", "leaf_ctas_per_sm", "tiles_per_pop")}
 
     def batch_step(hs, bufs, base):
         batch.checkpoint(hs, bufs)

@@ -205,8 +205,10 @@ int b2d_batch_destroy(b2d_batch* b);
 int b2d_batch_set_stream(b2d_batch* b, void* cuda_stream);
 /* Tuning: "leaf_stages" (staging ring depth, 0 = 64 KB ring), "leaf_ctas_per_sm" (0 = 3),
  * "tiles_per_pop" (work-queue granule, tiles of 256 chunks), "streams" (graph branches for the
- * per-handle work), "autotune" (1: coordinate descent over those knobs, one setting per
- * incremental batch -- six batches -- measured by device time; "tuned" reads 1 once it has
+ * per-handle work when "shared" is 0), "shared" (1 = the shared segmented forest/diff launches,
+ * default; 0 = per-handle launches on "streams" branches), "autotune" (1: coordinate descent over
+ * shared, tiles_per_pop and staging, one setting per incremental batch -- five batches --
+ * measured by device time; "tuned" reads 1 once it has
  * settled and the knobs then read the chosen values), "graph" (2 = launch a composition directly
  * the first time and as a captured graph from its second batch on, default; 1 = always a graph;
  * 0 = never), "graph_cache" (instantiated graphs kept, one per batch composition, default 16),

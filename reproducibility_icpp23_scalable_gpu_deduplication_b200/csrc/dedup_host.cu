@@ -931,28 +931,29 @@ __global__ void batch_collect_kernel(DevState* const* states, uint32_t count, De
 }
 
 struct BatchCand {
-  int stages, ctas, tiles_per_pop, streams;
+  int stages, ctas, tiles_per_pop, streams, shared;
 };
 
 // Online coordinate-descent tuner.  Each incremental batch (same bytes every time) measures one
 // setting by its graph's device time: first the current setting, then, one knob at a time,
-// each other value of that knob, keeping a value whenever it is faster.  Knobs: graph branches
-// for the per-buffer work, tiles (of 256 chunks) per work-queue pop, and staging (ring depth x
-// CTAs per SM) of the hashing kernel.  1 + 2 + 2 + 1 = 6 measured batches.
+// each other value of that knob, keeping a value whenever it is faster.  Knobs: shared
+// segmented forest/diff launches for all handles or per-handle launches on 32 graph branches,
+// tiles (of 256 chunks) per work-queue pop, and staging (ring depth x CTAs per SM) of the
+// hashing kernel.  1 + 1 + 2 + 1 = 5 measured batches.
 struct BatchTuner {
   static constexpr int KNOBS = 3;
-  BatchCand base{0, 3, 4, 8};
+  BatchCand base{0, 3, 4, 32, 1};
   double base_score = 0;
   bool have_base = false, done = false;
   int knob = 0;
   size_t idx = 0;
-  BatchCand pending{0, 3, 4, 8};
+  BatchCand pending{0, 3, 4, 32, 1};
 
-  static size_t nvalues(int k) { return k == 2 ? 2 : 3; }
+  static size_t nvalues(int k) { return k == 1 ? 3 : 2; }
   static BatchCand with_value(BatchCand c, int k, size_t i) {
-    static const int streams[3] = {8, 32, 2}, tpp[3] = {4, 1, 16};
+    static const int tpp[3] = {4, 1, 16};
     static const int stages[2] = {0, 3}, ctas[2] = {3, 2};
-    if (k == 0) c.streams = streams[i];
+    if (k == 0) c.shared = i == 0 ? 1 : 0;
     else if (k == 1) c.tiles_per_pop = tpp[i];
     else {
       c.stages = stages[i];
@@ -961,7 +962,8 @@ struct BatchTuner {
     return c;
   }
   static bool same(const BatchCand& a, const BatchCand& b) {
-    return a.stages == b.stages && a.ctas == b.ctas && a.tiles_per_pop == b.tiles_per_pop && a.streams == b.streams;
+    return a.stages == b.stages && a.ctas == b.ctas && a.tiles_per_pop == b.tiles_per_pop &&
+           a.streams == b.streams && a.shared == b.shared;
   }
   void reset(const BatchCand& start) {
     *this = BatchTuner();
@@ -1042,7 +1044,7 @@ struct b2d_batch {
   bool fl_scoring = false, fl_any_baseline = false;
   std::chrono::high_resolution_clock::time_point fl_t0;
   // tuning: current values, and the online tuner
-  BatchCand cur{0, 3, 4, 8};
+  BatchCand cur{0, 3, 4, 32, 1};
   bool autotune = false;
   BatchTuner tuner;
   // last batch
@@ -1169,11 +1171,12 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
   L.queues = align_up(L.states + sizeof(DevState*) * count, 64);
   L.bstatus = align_up(L.queues + sizeof(unsigned int) * (groups.size() + 1), 64);
   L.dargs = align_up(L.bstatus + sizeof(DevStatus), 64);
-  L.dtab = align_up(L.dargs + (b->batch_diff ? sizeof(DiffArgs) * count : 0), 64);
+  const bool seg_diff = b->batch_diff && cand.shared;
+  L.dtab = align_up(L.dargs + (seg_diff ? sizeof(DiffArgs) * count : 0), 64);
   const size_t tab_len = (size_t)count + 1;   // entries per table
   // shared forest phases: every handle's launch steps, one segmented launch per (phase, step,
   // kind) with three tables (CTA offsets, p0, p1)
-  const bool seg_forest = b->batch_forest && b->batch_diff;
+  const bool seg_forest = b->batch_forest && seg_diff;
   std::vector<std::vector<ForestStep>> fsteps[2];
   struct FLaunch {
     int phase, kind;
@@ -1198,7 +1201,7 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
         }
     }
   }
-  L.fargs = align_up(L.dtab + (b->batch_diff ? sizeof(uint32_t) * tab_len * DIFF_TABLES : 0), 64);
+  L.fargs = align_up(L.dtab + (seg_diff ? sizeof(uint32_t) * tab_len * DIFF_TABLES : 0), 64);
   L.ftab = align_up(L.fargs + (seg_forest ? sizeof(ForestArgs) * count : 0), 64);
   for (size_t q = 0; q < flaunch.size(); q++) flaunch[q].off = L.ftab + sizeof(uint32_t) * 3 * tab_len * q;
   L.total = align_up(L.ftab + sizeof(uint32_t) * 3 * tab_len * flaunch.size(), 256);
@@ -1216,7 +1219,7 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
   uint8_t* B = b->blob.p;
   // shared diff assembly: every handle's DiffArgs, grid sizes and the CTA offset tables
   DiffBatch dplan{};
-  if (b->batch_diff) {
+  if (seg_diff) {
     auto tab = [&](int t) { return reinterpret_cast<uint32_t*>(H + L.dtab) + (size_t)t * tab_len; };
     auto dtab = [&](int t) { return reinterpret_cast<const uint32_t*>(B + L.dtab) + (size_t)t * tab_len; };
     uint32_t tot_g = 0, tot_gl = 0, tot_gp = 0, tot_gs = 0, tot_v[GATHER_VARIANTS] = {0};
@@ -1310,7 +1313,7 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
     key.push_back((uint64_t)(int64_t)item_of[i]);
   }
   for (auto& g : groups) key.insert(key.end(), {(uint64_t)g.U, (uint64_t)g.kind, g.beg, g.end, g.tiles});
-  key.insert(key.end(), {(uint64_t)B, (uint64_t)H, L.total, (uint64_t)b->batch_diff, (uint64_t)seg_forest,
+  key.insert(key.end(), {(uint64_t)B, (uint64_t)H, L.total, (uint64_t)seg_diff, (uint64_t)seg_forest,
                          (uint64_t)b->coll.p,
                          (uint64_t)b->coll_h.p, (uint64_t)cand.stages,
                          (uint64_t)cand.ctas, (uint64_t)cand.tiles_per_pop, (uint64_t)cand.streams});
@@ -1365,7 +1368,7 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
         b2d_dedup* d = hs[i];
         const bool skip_leaves = item_of[i] >= 0;
         if (seg_forest && skip_leaves) continue;   // nothing of this handle runs in a branch
-        const int r = enqueue_checkpoint(d, s, &d->state.p->round, false, false, skip_leaves, true, b->batch_diff,
+        const int r = enqueue_checkpoint(d, s, &d->state.p->round, false, false, skip_leaves, true, seg_diff,
                                          seg_forest);
         if (r != B2D_OK) erc = r;
         launches += d->launches;
@@ -1388,7 +1391,7 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
         launches++;
       }
     }
-    if (b->batch_diff && erc == B2D_OK) {
+    if (seg_diff && erc == B2D_OK) {
       uint32_t dl = 0;
       cap_err(launch_collect_diff_batch(dplan, main, &dl));
       launches += dl;
@@ -1885,6 +1888,7 @@ int b2d_batch_set_param(b2d_batch* b, const char* name, int64_t value) {
   else if (k == "leaf_ctas_per_sm" && value >= 0 && value <= 8) b->cur.ctas = (int)value;
   else if (k == "tiles_per_pop" && value >= 1 && value <= 1024) b->cur.tiles_per_pop = (int)value;
   else if (k == "streams" && value >= 1 && value <= 64) b->cur.streams = (int)value;
+  else if (k == "shared" && (value == 0 || value == 1)) b->cur.shared = (int)value;
   else if (k == "graph_cache" && value >= 1 && value <= 4096) b->graph_cap = (size_t)value;
   else if (k == "graph" && value >= 0 && value <= 2) b->graph_mode = (int)value;
   else if (k == "batch_diff" && (value == 0 || value == 1)) b->batch_diff = value != 0;
@@ -1903,6 +1907,7 @@ int b2d_batch_get_param(b2d_batch* b, const char* name, int64_t* value) {
   else if (k == "leaf_ctas_per_sm") *value = b->cur.ctas;
   else if (k == "tiles_per_pop") *value = b->cur.tiles_per_pop;
   else if (k == "streams") *value = b->cur.streams;
+  else if (k == "shared") *value = b->cur.shared;
   else if (k == "autotune") *value = b->autotune ? 1 : 0;
   else if (k == "tuned") *value = b->tuner.done ? 1 : 0;
   else if (k == "graph_cache") *value = (int64_t)b->graph_cap;

@@ -127,12 +127,12 @@ def test_batch_autotune_keeps_output(cuda):
     """the tuner measures one setting per incremental round; output never changes"""
     specs = SPECS[:3] + SPECS[5:7]
     with CheckpointBatch(autotune=True) as b:
-        # one baseline round (not scored), six scored incremental rounds, one with the result
+        # one baseline round (not scored), five scored incremental rounds, then the result
         rounds = 8
         baselines = [[True] * len(specs)] + [[False] * len(specs) for _ in range(rounds - 1)]
         got, _, _ = run_batch(specs, rounds, baselines, b)
         assert b.get_param("tuned") == 1
-        for k in ("leaf_stages", "leaf_ctas_per_sm", "tiles_per_pop", "streams"):
+        for k in ("shared", "leaf_stages", "leaf_ctas_per_sm", "tiles_per_pop", "streams"):
             b.get_param(k)
     want = diffs_alone(specs, rounds, baselines)
     assert got == want
