@@ -80,6 +80,13 @@ struct PinnedBuf {
     else p = nullptr;
     return e;
   }
+  // for buffers whose size drifts from call to call (diffs): grow by a quarter plus slack, so a
+  // diff a few bytes longer than the last one does not free and re-pin tens of megabytes
+  cudaError_t grow(size_t count) {
+    if (count <= n && p) return cudaSuccess;
+    const size_t unit = (1u << 20) / sizeof(T) + 1;
+    return reserve((count + count / 4 + unit - 1) / unit * unit);
+  }
 };
 
 __global__ void map_special_init_kernel(MapSlot* special) {
@@ -634,7 +641,7 @@ int checkpoint_to_pinned(b2d_dedup* d, const void* d_data, uint64_t len, bool ma
                          const uint8_t** diff, uint64_t* diff_len) {
   int rc = do_checkpoint(d, d_data, len, make_baseline, advance);
   if (rc) return rc;
-  B2D_CU(d->diff_h.reserve(d->diff_len));
+  B2D_CU(d->diff_h.grow(d->diff_len));
   rc = copy_diff(d, d->diff_h.p, d->diff_h.n);
   if (rc) return rc;
   if (diff) *diff = d->diff_h.p;
@@ -795,7 +802,7 @@ int do_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* di
   B2D_CU(d->r_diff.reserve(max_size + 16));
   B2D_CU(d->state.reserve(1));
   B2D_CU(d->state_h.reserve(1));
-  if (!ddiffs) B2D_CU(d->r_stage.reserve(max_size + 16 + 8 * max_ids));
+  if (!ddiffs) B2D_CU(d->r_stage.grow(max_size + 16 + 8 * max_ids));
   B2D_CU(cudaMemsetAsync(d->state.p, 0, sizeof(DevState), d->stream));
   d->launches = 0;
   double copy_time = 0;

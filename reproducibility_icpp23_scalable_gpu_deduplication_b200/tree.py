@@ -125,10 +125,12 @@ class TreeDeduplicator:
         check(lib().b2d_copy_diff_async(self._h, ctypes.c_void_p(ptr), cap, sh), "b2d_copy_diff_async")
         return n
 
-    def checkpoint(self, data, make_baseline=False, filename=None, logname=None):
+    def checkpoint(self, data, make_baseline=False, filename=None, logname=None, copy=True):
         """checkpoint(data_ptr, len, diff_h[, logname], make_baseline) / (.., filename, logname, ..).
 
-        Returns the diff as bytes (None for the file overload, which writes `filename`)."""
+        Returns the diff as bytes (None for the file overload, which writes `filename`).  With
+        ``copy=False`` it returns a read-only uint8 numpy view of the library's pinned host copy
+        of the diff instead: no host-side copy, valid until this deduplicator's next call."""
         self._sync_stream()
         p, n = _dev_ptr(data)
         if filename is not None:
@@ -143,7 +145,11 @@ class TreeDeduplicator:
         else:
             check(lib().b2d_checkpoint(self._h, p, n, int(bool(make_baseline)), ctypes.byref(dptr),
                                        ctypes.byref(dlen)), "b2d_checkpoint")
-        return ctypes.string_at(dptr, dlen.value)
+        if copy:
+            return ctypes.string_at(dptr, dlen.value)
+        view = np.ctypeslib.as_array(dptr, shape=(dlen.value,)) if dlen.value else np.empty(0, np.uint8)
+        view.flags.writeable = False
+        return view
 
     # -- restart overloads (src/tree_approach.cpp:1786-1838)
     def restart(self, out, chkpts, chkpt_id, logname=None, check_status=True):

@@ -190,6 +190,24 @@ def test_map_growth_keeps_output(cuda):
         assert grows >= 1 and entries <= 0.3 * slots
 
 
+def test_diff_views_without_host_copy(cuda):
+    """checkpoint(copy=False) returns a read-only view of the pinned host diff; the bytes equal
+    the oracle's while that staging grows (a tiny all-zero baseline first, then a full one)"""
+    s = synth.plain_64m(nbytes=4 << 20)
+    bufs = [np.zeros(4 << 20, np.uint8)] + [s.next().copy() for _ in range(3)]
+    g = TreeDeduplicator(128, HASH_MURMUR3)
+    o = O.OracleTreeDeduplicator(128, HASH_MURMUR3)
+    sizes = []
+    for i, (b, mb) in enumerate(zip(bufs, [True, True, False, False])):
+        v = g.checkpoint(to_dev(b), mb, copy=False)
+        want = o.checkpoint(b, mb)
+        assert isinstance(v, np.ndarray) and v.dtype == np.uint8 and not v.flags.writeable
+        assert v.tobytes() == want, i
+        sizes.append(v.size)
+    assert sizes[0] < sizes[1] // 8
+    g.close()
+
+
 @pytest.mark.parametrize("unit", [16, 32, 64])
 def test_narrow_staging_units(cuda, unit):
     """the staged hashing kernel with segments narrower than the chunk allows"""
