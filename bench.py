@@ -491,6 +491,7 @@ def main():
 
     from reproducibility_icpp23_scalable_gpu_deduplication_b200 import (HASH_MD5, HASH_MURMUR3, TreeDeduplicator,
                                                                         replicas, synth)
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200.tree import parse_header
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -618,10 +619,20 @@ def main():
         torch.cuda.synchronize()
         rd_ms = r0.elapsed_time(r1)
         ok_d = bool(torch.equal(out, x.view(torch.uint8).reshape(-1)[:nbytes]))
+        # restart roofline: the output written once, every output chunk read once from some
+        # diff's data section, and every diff's header and region lists read
+        hdrs = [parse_header(dh) for dh in diffs]
+        meta = sum(32 + 4 * h["num_first_ocur"] + 8 * (h["num_prior_chkpts"] + h["num_shift_dupl"]) for h in hdrs)
+        alg = 2 * nbytes + meta
+        peak_r, peak_kind_r = measured_peak()
         restart = {"value": round(nbytes / (r_ms * 1e-3) / GB, 2), "unit": "GB/s", "ms": round(r_ms, 3),
                    "diffs": 4, "h2d_bytes": int(sum(d.nbytes for d in diffs)), "identical": ok,
                    "device_diffs": {"value": round(nbytes / (rd_ms * 1e-3) / GB, 2), "unit": "GB/s",
-                                    "ms": round(rd_ms, 3), "identical": ok_d}}
+                                    "ms": round(rd_ms, 3), "identical": ok_d,
+                                    "roofline": {"bound": "hbm", "algorithmic_bytes": alg,
+                                                 "achieved": round(alg / (rd_ms * 1e-3) / GB, 1), "peak": peak_r,
+                                                 "peak_kind": peak_kind_r, "unit": "GB/s",
+                                                 "frac": round(alg / (rd_ms * 1e-3) / GB / peak_r, 4)}}}
         del ddiffs
         rd.close()
         del rs, diffs, out, x

@@ -135,7 +135,7 @@ int b2d_restart_device(b2d_dedup* d, void* d_out, uint64_t len, const void* cons
  * runtime whose device memory is all owned by its own pool and budget.  Same result as
  * b2d_restart, but the diffs are device-resident (d_diffs[i]: device pointer, sizes[i]: bytes)
  * and no handle is needed.  The scratch is one fixed __device__ array in the library (about
- * 7.4 MB on every GPU that loads it, held until exit): at most 2^18 chunks per checkpoint and
+ * 10.0 MB on every GPU that loads it, held until exit): at most 2^18 chunks per checkpoint and
  * checkpoint ids below 4096, else B2D_ERR_UNSUPPORTED.  The first call on a device looks up
  * that array's address and should come before any stream capture.  All calls share the array:
  * calls that overlap on the GPU race and must be serialised by the caller.  Work runs on

@@ -198,9 +198,10 @@ struct b2d_dedup {
   bool diff_valid = false;
 
   // restart scratch
-  DevBuf<uint2> r_node_list, r_rep;
-  DevBuf<unsigned long long> r_dist;
-  DevBuf<uint32_t> r_offs, r_partial;
+  DevBuf<uint2> r_node_list, r_rep;      // restart: NodeIDs of the main diff's chunks; slots' rep
+  DevBuf<uint32_t> r_dist;                 // slots' data offsets
+  DevBuf<uint8_t> r_mflag, r_flag;
+  DevBuf<uint32_t> r_offs, r_partial;      // r_offs: offsets, region starts, source starts, trees
   DevBuf<unsigned long long> r_cum, r_total;
   DevBuf<uint8_t> r_diff;
   PinnedBuf<uint8_t> r_stage;
@@ -301,6 +302,7 @@ uint64_t handle_bytes(const b2d_dedup* d) {
          buf_bytes(d->region_off) + buf_bytes(d->sprev) + buf_bytes(d->skey) + buf_bytes(d->hist) +
          buf_bytes(d->bucket_start) + buf_bytes(d->partial) + buf_bytes(d->partial2) + buf_bytes(d->diff) +
          buf_bytes(d->state) + buf_bytes(d->r_node_list) + buf_bytes(d->r_rep) + buf_bytes(d->r_dist) +
+         buf_bytes(d->r_mflag) + buf_bytes(d->r_flag) +
          buf_bytes(d->r_offs) + buf_bytes(d->r_partial) + buf_bytes(d->r_cum) + buf_bytes(d->r_total) +
          buf_bytes(d->r_diff);
 }
@@ -779,7 +781,9 @@ int do_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* di
   uint64_t nc = (h.datalen + h.cs - 1) / h.cs;
   if (nc > 0x7fffffffull) return B2D_ERR_FORMAT;
   const uint32_t n = (uint32_t)nc, N = 2u * n - 1u;
-  // scratch sized for the whole chain
+  // the chain, newest first: from `id` down while the index is not below the last ref_id
+  std::vector<int> chain;
+  std::vector<HostHdr> hdrs;
   uint64_t max_size = 0, max_list = 0, max_ids = 0;
   {
     uint32_t ref = h.ref_id;
@@ -787,25 +791,46 @@ int do_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* di
       HostHdr hh;
       if (!parse_hdr(diffs[idx], sizes[idx], hh)) return B2D_ERR_FORMAT;
       if (idx != (int)id) ref = hh.ref_id;
+      chain.push_back(idx);
+      hdrs.push_back(hh);
       max_size = std::max<uint64_t>(max_size, sizes[idx]);
       max_list = std::max<uint64_t>(max_list, std::max<uint64_t>(hh.F, hh.S));
       max_ids = std::max<uint64_t>(max_ids, (uint64_t)hh.chkpt_id + 1);
     }
   }
+  // window slots: older diffs resolved per walk.  Device diffs are read where they lie, so a
+  // window holds several (bounded by the slots' memory); host diffs pass one at a time through
+  // one device copy.
+  const uint64_t older = chain.size() - 1;
+  uint32_t W = 1;
+  if (ddiffs && older > 1) {
+    const uint64_t per_slot = 13ull * n;   // dist u32 + rep uint2 + a flag byte per chunk
+    W = (uint32_t)std::min<uint64_t>(std::min<uint64_t>(older, RESTART_WINDOW),
+                                     std::max<uint64_t>(1, RESTART_SLOT_BYTES / per_slot));
+  }
   B2D_CU(d->r_node_list.reserve(n));
-  B2D_CU(d->r_rep.reserve(n));
-  B2D_CU(d->r_dist.reserve(n));
-  B2D_CU(d->r_offs.reserve(max_list));
+  B2D_CU(d->r_mflag.reserve(n));
+  B2D_CU(d->r_dist.reserve((uint64_t)n * W));
+  B2D_CU(d->r_rep.reserve((uint64_t)n * W));
+  B2D_CU(d->r_flag.reserve((uint64_t)n * W));
+  B2D_CU(d->r_offs.reserve(4 * std::max<uint64_t>(max_list, 1)));
   B2D_CU(d->r_partial.reserve(SCAN_GRID));
   B2D_CU(d->r_cum.reserve(max_ids));
   B2D_CU(d->r_total.reserve(1));
-  B2D_CU(d->r_diff.reserve(max_size + 16));
+  if (!ddiffs) B2D_CU(d->r_diff.reserve(max_size + 16));   // device diffs are read where they lie
   B2D_CU(d->state.reserve(1));
   B2D_CU(d->state_h.reserve(1));
   if (!ddiffs) B2D_CU(d->r_stage.grow(max_size + 16 + 8 * max_ids));
   B2D_CU(cudaMemsetAsync(d->state.p, 0, sizeof(DevState), d->stream));
   d->launches = 0;
   double copy_time = 0;
+  auto slot = [&](uint32_t k) {
+    RestartSlot sl;
+    sl.dist = d->r_dist.p + (uint64_t)n * k;
+    sl.rep = d->r_rep.p + (uint64_t)n * k;
+    sl.flag = d->r_flag.p + (uint64_t)n * k;
+    return sl;
+  };
 
   RestartArgs a{};
   a.n = n;
@@ -813,24 +838,46 @@ int do_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* di
   a.out = static_cast<uint8_t*>(d_out);
   a.out_len = h.datalen;
   a.node_list = d->r_node_list.p;
-  a.dist = d->r_dist.p;
-  a.rep = d->r_rep.p;
+  a.mflag = d->r_mflag.p;
+  const uint64_t lcap = std::max<uint64_t>(max_list, 1);
   a.offs = d->r_offs.p;
+  a.rstart = d->r_offs.p + lcap;
+  a.pstart = d->r_offs.p + 2 * lcap;
+  a.rtree = d->r_offs.p + 3 * lcap;
   a.partial = d->r_partial.p;
   a.total = d->r_total.p;
   a.st = &d->state.p->status;
-  B2D_CU(launch_restart_init(a, d->sm_count, d->stream));
+  RestartWalk w{};
+  w.main_cur = h.chkpt_id;
+  w.n = n;
+  w.N = N;
+  w.out = a.out;
+  w.out_len = h.datalen;
+  w.node_list = a.node_list;
+  w.mflag = a.mflag;
+  w.st = a.st;
+  uint32_t wcount = 0;
+  auto flush = [&](bool last) -> cudaError_t {
+    if (wcount == 0) return cudaSuccess;
+    w.count = wcount;
+    w.last = last;
+    cudaError_t e = launch_restart_walk(w, d->sm_count, d->stream);
+    d->launches += 1;
+    w.dense = 1;   // a walk that is not the last wrote every chunk's NodeID
+    wcount = 0;
+    return e;
+  };
 
-  uint32_t ref = h.ref_id;
-  for (int idx = (int)id; idx >= 0 && idx >= (int)ref; idx--) {
-    HostHdr hh;
-    parse_hdr(diffs[idx], sizes[idx], hh);
-    if (idx != (int)id) ref = hh.ref_id;
-    // stage the diff (plus its repeat-table running counts) in pinned memory, then one copy
+  for (size_t k = 0; k < chain.size(); k++) {
+    const int idx = chain[k];
+    const HostHdr& hh = hdrs[k];
+    const bool is_main = k == 0;
+    // host diffs: one copy into the device scratch, placed so the data section is 16-byte
+    // aligned; pinned (page-locked) host diffs are copied straight from where they are, others
+    // go through the handle's pinned staging buffer.  The repeat table's running counts are
+    // uploaded beside them.
     const uint32_t delta = (uint32_t)((16u - (hh.data_off & 15u)) & 15u);
     const uint64_t ncum = (uint64_t)hh.chkpt_id + 1;
-    // device diffs and pinned (page-locked) host diffs are copied straight to the scratch;
-    // other host diffs go through the handle's pinned staging buffer, reused per diff
     bool pinned = ddiffs != nullptr;
     if (!ddiffs) {
       cudaPointerAttributes pa;
@@ -853,15 +900,15 @@ int do_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* di
       if (ck < ncum) cum[ck] = cnt; else bad_row = true;
     }
     for (uint64_t t = 1; t < ncum; t++) cum[t] += cum[t - 1];
-    B2D_CU(cudaMemcpyAsync(d->r_diff.p + delta, src, sizes[idx],
-                           ddiffs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, d->stream));
+    if (!ddiffs)
+      B2D_CU(cudaMemcpyAsync(d->r_diff.p + delta, src, sizes[idx], cudaMemcpyHostToDevice, d->stream));
     B2D_CU(cudaMemcpyAsync(d->r_cum.p, cum.data(), sizeof(unsigned long long) * ncum, cudaMemcpyHostToDevice,
                            d->stream));
-    if (idx == (int)id) {
+    if (is_main && !ddiffs) {
       B2D_CU(cudaStreamSynchronize(d->stream));
       copy_time = secs(c0, clk::now());
     }
-    a.diff = d->r_diff.p + delta;
+    a.diff = ddiffs ? src : d->r_diff.p + delta;
     a.diff_size = sizes[idx];
     a.first_off = hh.first_off;
     a.count_off = hh.count_off;
@@ -873,11 +920,24 @@ int do_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* di
     a.cur_id = hh.chkpt_id;
     a.datalen = hh.datalen;
     a.cs = hh.cs;
-    a.is_main = idx == (int)id;
+    a.is_main = is_main;
     a.cum = d->r_cum.p;
     a.ncum = (uint32_t)ncum;
+    a.slot = slot(is_main ? 0 : wcount);
     B2D_CU(launch_restart_diff(a, &d->state.p->straddle, d->sm_count, d->stream));
-    d->launches += 9 + (straddle_query(n).count ? 2 : 0);
+    d->launches += restart_diff_launches(n);
+    if (!is_main) {
+      // the window's walk copies from every diff in it, which share one chunk size
+      if (wcount == 0) w.cs = hh.cs;
+      w.data[wcount] = a.diff + hh.data_off;
+      w.data_len[wcount] = sizes[idx] - hh.data_off;
+      w.datalen[wcount] = hh.datalen;
+      w.cur[wcount] = hh.chkpt_id;
+      w.slot[wcount] = a.slot;
+      wcount++;
+      const bool end = k + 1 == chain.size();
+      if (bad_row || end || wcount == W || hdrs[k + 1].cs != hh.cs) B2D_CU(flush(bad_row || end));
+    }
     if (bad_row) {
       B2D_CU(cudaStreamSynchronize(d->stream));
       d->restart_timers[0] = copy_time;

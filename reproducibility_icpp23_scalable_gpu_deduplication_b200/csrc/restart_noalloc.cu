@@ -32,15 +32,17 @@ constexpr uint64_t NOALLOC_MAX_IDS = 4096;
 
 constexpr size_t na_align(size_t x) { return (x + 255) & ~size_t(255); }
 constexpr size_t NA_NODE_LIST = 0;
-constexpr size_t NA_REP = na_align(NA_NODE_LIST + sizeof(uint2) * NOALLOC_MAX_CHUNKS);
-constexpr size_t NA_DIST = na_align(NA_REP + sizeof(uint2) * NOALLOC_MAX_CHUNKS);
-constexpr size_t NA_OFFS = na_align(NA_DIST + sizeof(unsigned long long) * NOALLOC_MAX_CHUNKS);
-constexpr size_t NA_CUM = na_align(NA_OFFS + sizeof(uint32_t) * NOALLOC_MAX_CHUNKS);
+constexpr size_t NA_MFLAG = na_align(NA_NODE_LIST + sizeof(uint2) * NOALLOC_MAX_CHUNKS);
+constexpr size_t NA_DIST = na_align(NA_MFLAG + NOALLOC_MAX_CHUNKS);
+constexpr size_t NA_REP = na_align(NA_DIST + sizeof(uint32_t) * NOALLOC_MAX_CHUNKS);
+constexpr size_t NA_FLAG = na_align(NA_REP + sizeof(uint2) * NOALLOC_MAX_CHUNKS);
+constexpr size_t NA_OFFS = na_align(NA_FLAG + NOALLOC_MAX_CHUNKS);   // offsets, starts, sources, trees
+constexpr size_t NA_CUM = na_align(NA_OFFS + 4 * sizeof(uint32_t) * NOALLOC_MAX_CHUNKS);
 constexpr size_t NA_PARTIAL = na_align(NA_CUM + sizeof(unsigned long long) * NOALLOC_MAX_IDS);
 constexpr size_t NA_TOTAL = na_align(NA_PARTIAL + sizeof(uint32_t) * SCAN_GRID);
 constexpr size_t NA_STATUS = na_align(NA_TOTAL + sizeof(unsigned long long));
 constexpr size_t NA_STRADDLE = na_align(NA_STATUS + sizeof(DevStatus));
-constexpr size_t NA_BYTES = na_align(NA_STRADDLE + sizeof(StraddleInfo));   // 7,374,848 bytes (about 7.4 MB)
+constexpr size_t NA_BYTES = na_align(NA_STRADDLE + sizeof(StraddleInfo));   // 9,996,288 bytes (about 10.0 MB)
 
 static __device__ __align__(256) unsigned char g_restart_scratch[NA_BYTES];
 
@@ -122,16 +124,30 @@ extern "C" int b2d_restart_noalloc(void* d_out, uint64_t len, const void* const*
   a.out = static_cast<uint8_t*>(d_out);
   a.out_len = h.datalen;
   a.node_list = reinterpret_cast<uint2*>(base + NA_NODE_LIST);
-  a.rep = reinterpret_cast<uint2*>(base + NA_REP);
-  a.dist = reinterpret_cast<unsigned long long*>(base + NA_DIST);
+  a.mflag = base + NA_MFLAG;
+  a.slot.dist = reinterpret_cast<uint32_t*>(base + NA_DIST);
+  a.slot.rep = reinterpret_cast<uint2*>(base + NA_REP);
+  a.slot.flag = base + NA_FLAG;
   a.offs = reinterpret_cast<uint32_t*>(base + NA_OFFS);
+  a.rstart = a.offs + NOALLOC_MAX_CHUNKS;
+  a.pstart = a.offs + 2 * NOALLOC_MAX_CHUNKS;
+  a.rtree = a.offs + 3 * NOALLOC_MAX_CHUNKS;
   a.cum = reinterpret_cast<unsigned long long*>(base + NA_CUM);
   a.partial = reinterpret_cast<uint32_t*>(base + NA_PARTIAL);
   a.total = reinterpret_cast<unsigned long long*>(base + NA_TOTAL);
   a.st = reinterpret_cast<DevStatus*>(base + NA_STATUS);
   StraddleInfo* sd = reinterpret_cast<StraddleInfo*>(base + NA_STRADDLE);
   if (cudaMemsetAsync(a.st, 0, sizeof(DevStatus), s) != cudaSuccess) return B2D_ERR_CUDA;
-  if (launch_restart_init(a, sm_count, s) != cudaSuccess) return B2D_ERR_CUDA;
+  // older diffs go through the one slot: each is expanded, then walked on its own
+  RestartWalk w{};
+  w.main_cur = h.chkpt_id;
+  w.n = n;
+  w.N = N;
+  w.out = a.out;
+  w.out_len = h.datalen;
+  w.node_list = a.node_list;
+  w.mflag = a.mflag;
+  w.st = a.st;
 
   uint32_t ref = h.ref_id;
   for (int idx = (int)chkpt_id; idx >= 0 && idx >= (int)ref; idx--) {
@@ -156,6 +172,18 @@ extern "C" int b2d_restart_noalloc(void* d_out, uint64_t len, const void* const*
     a.ncum = hh.chkpt_id + 1u;
     if (launch_restart_cum(a, s) != cudaSuccess) return B2D_ERR_CUDA;
     if (launch_restart_diff(a, sd, sm_count, s) != cudaSuccess) return B2D_ERR_CUDA;
+    if (!a.is_main) {
+      w.count = 1;
+      w.cs = hh.cs;
+      w.data[0] = a.diff + hh.data_off;
+      w.data_len[0] = sizes[idx] - hh.data_off;
+      w.datalen[0] = hh.datalen;
+      w.cur[0] = hh.chkpt_id;
+      w.slot[0] = a.slot;
+      w.last = idx - 1 < 0 || idx - 1 < (int)ref;
+      if (launch_restart_walk(w, sm_count, s) != cudaSuccess) return B2D_ERR_CUDA;
+      w.dense = 1;
+    }
   }
   DevStatus st;
   if (cudaMemcpyAsync(&st, a.st, sizeof(DevStatus), cudaMemcpyDeviceToHost, s) != cudaSuccess) return B2D_ERR_CUDA;
