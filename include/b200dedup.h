@@ -57,7 +57,14 @@ enum b2d_hash_kind {
 /* TreeDeduplicator(uint32_t bytes_per_chunk) -- src/tree_approach.cpp:5-9.  The hash is a
  * compile-time choice in the reference (include/hash_functions.hpp:16-20); here a parameter. */
 int b2d_create(uint32_t chunk_size, int hash_kind, b2d_dedup** out);
-/* ~TreeDeduplicator() -- src/tree_approach.cpp:11 */
+/* ListDeduplicator(uint32_t bytes_per_chunk) -- src/list_approach.cpp:5-9: the list approach
+ * (one digest per chunk, a changed chunk is a first occurrence or a shifted duplicate,
+ * src/list_approach.cpp:23-257) behind the same handle.  Every call below takes it: checkpoint
+ * overloads (:843-974, diffs naming chunk indices), host and device restarts (:259-586), file
+ * and log forms ("List" rows).  Not accepted by the batched form (B2D_ERR_UNSUPPORTED) nor by
+ * b2d_restart_noalloc, which restarts tree diffs. */
+int b2d_create_list(uint32_t chunk_size, int hash_kind, b2d_dedup** out);
+/* ~TreeDeduplicator() -- src/tree_approach.cpp:11 (~ListDeduplicator(), src/list_approach.cpp:11) */
 int b2d_destroy(b2d_dedup* d);
 /* Run all device work of this handle on `cuda_stream` (a cudaStream_t; NULL = the handle's
  * own stream).  No reference counterpart (Kokkos uses its default execution space). */

@@ -53,7 +53,7 @@ class TreeDeduplicator {
   explicit TreeDeduplicator(uint32_t bytes_per_chunk, int hash_kind = B2D_HASH_MURMUR3) {
     check(b2d_create(bytes_per_chunk, hash_kind, &h_), "TreeDeduplicator");
   }
-  ~TreeDeduplicator() {
+  virtual ~TreeDeduplicator() {
     if (h_) b2d_destroy(h_);
   }
   TreeDeduplicator(const TreeDeduplicator&) = delete;
@@ -133,8 +133,23 @@ class TreeDeduplicator {
   }
   b2d_dedup* handle() { return h_; }
 
+ protected:
+  struct ListTag {};
+  TreeDeduplicator(uint32_t bytes_per_chunk, int hash_kind, ListTag) {
+    check(b2d_create_list(bytes_per_chunk, hash_kind, &h_), "ListDeduplicator");
+  }
+
  private:
   b2d_dedup* h_ = nullptr;
+};
+
+// ListDeduplicator(uint32_t bytes_per_chunk) -- src/list_approach.cpp:5-9, with the same method
+// set (include/list_approach.hpp): checkpoint overloads write list diffs naming chunk indices,
+// restarts take list diffs.  Not accepted by CheckpointBatch.
+class ListDeduplicator : public TreeDeduplicator {
+ public:
+  explicit ListDeduplicator(uint32_t bytes_per_chunk, int hash_kind = B2D_HASH_MURMUR3)
+      : TreeDeduplicator(bytes_per_chunk, hash_kind, ListTag{}) {}
 };
 
 // Batched checkpoints (b2d_batch_*): one checkpoint of each of many TreeDeduplicators' buffers

@@ -1,8 +1,9 @@
-"""ctypes bindings for the CPU oracle (oracle/tree_oracle.c).
+"""ctypes bindings for the CPU oracle (oracle/tree_oracle.c, oracle/list_oracle.c).
 
 TEST INFRASTRUCTURE ONLY -- imported by tests/, ``__graft_entry__.smoke()`` and bench.py's
-CPU baseline.  The oracle restates the reference tree approach sequentially
-(src/tree_approach.cpp:13-1128 of TauferLab/Reproducibility_ICPP23_Scalable_GPU_Deduplication).
+CPU baseline.  The oracle restates the reference tree approach (src/tree_approach.cpp:13-1128)
+and list approach (src/list_approach.cpp:23-586) of
+TauferLab/Reproducibility_ICPP23_Scalable_GPU_Deduplication sequentially.
 """
 import ctypes
 import os
@@ -60,6 +61,21 @@ def lib():
         L.oracle_num_leaf_descendents.argtypes = [u32, u32]
         L.oracle_leftmost_leaf.restype = u32
         L.oracle_leftmost_leaf.argtypes = [u32, u32]
+        L.oracle_list_create.restype = vp
+        L.oracle_list_create.argtypes = [u32, ctypes.c_int]
+        L.oracle_list_destroy.argtypes = [vp]
+        L.oracle_list_set_threads.argtypes = [vp, ctypes.c_int]
+        L.oracle_list_checkpoint.restype = ctypes.c_int
+        L.oracle_list_checkpoint.argtypes = [vp, vp, u64, ctypes.c_int, ctypes.POINTER(u8p), ctypes.POINTER(u64)]
+        L.oracle_list_num_first_ocur.restype = u64
+        L.oracle_list_num_first_ocur.argtypes = [vp]
+        L.oracle_list_num_shift_dupl.restype = u64
+        L.oracle_list_num_shift_dupl.argtypes = [vp]
+        L.oracle_list_current_id.restype = u32
+        L.oracle_list_current_id.argtypes = [vp]
+        L.oracle_list_datasizes.argtypes = [vp, ctypes.POINTER(u64)]
+        L.oracle_list_restart.restype = ctypes.c_int
+        L.oracle_list_restart.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(u64), u32, u32, vp, u64]
         _lib = L
     return _lib
 
@@ -150,6 +166,76 @@ class OracleTreeDeduplicator:
 
     def map_size(self):
         return lib().oracle_map_size(self._h)
+
+
+class OracleListDeduplicator:
+    """Sequential restatement of the reference ``ListDeduplicator`` (host buffers)."""
+
+    def __init__(self, chunk_size, hash_kind=HASH_MURMUR3, threads=1):
+        L = lib()
+        self._h = L.oracle_list_create(chunk_size, hash_kind)
+        if not self._h:
+            raise ValueError("bad chunk size")
+        L.oracle_list_set_threads(self._h, threads)
+        self.chunk_size = chunk_size
+        self.hash_kind = hash_kind
+
+    def close(self):
+        if self._h:
+            lib().oracle_list_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def checkpoint(self, data, make_baseline=False):
+        a = np.ascontiguousarray(data, dtype=np.uint8).reshape(-1)
+        out = ctypes.POINTER(ctypes.c_uint8)()
+        n = ctypes.c_uint64(0)
+        rc = lib().oracle_list_checkpoint(self._h, _ptr(a), a.size, int(bool(make_baseline)), ctypes.byref(out),
+                                          ctypes.byref(n))
+        if rc < 0:
+            raise RuntimeError(f"oracle list checkpoint failed: {rc}")
+        diff = ctypes.string_at(out, n.value)
+        lib().oracle_free(out)
+        self.last_rc = rc
+        return diff
+
+    def num_first_ocur(self):
+        return lib().oracle_list_num_first_ocur(self._h)
+
+    def num_shift_dupl(self):
+        return lib().oracle_list_num_shift_dupl(self._h)
+
+    @property
+    def current_id(self):
+        return lib().oracle_list_current_id(self._h)
+
+    def datasizes(self):
+        out = (ctypes.c_uint64 * 2)()
+        lib().oracle_list_datasizes(self._h, out)
+        return out[0], out[1]
+
+
+def _restart(fn, diffs, chkpt_idx, out_len, init):
+    bufs = [np.frombuffer(bytes(d), dtype=np.uint8).copy() for d in diffs]
+    if out_len is None:
+        out_len = int(np.frombuffer(bufs[chkpt_idx][8:16].tobytes(), np.uint64)[0])
+    out = np.zeros(out_len, np.uint8) if init is None else np.array(init, dtype=np.uint8).copy()
+    ptrs = (ctypes.c_void_p * len(bufs))(*[b.ctypes.data for b in bufs])
+    sizes = (ctypes.c_uint64 * len(bufs))(*[b.size for b in bufs])
+    rc = fn(ptrs, sizes, len(bufs), chkpt_idx, _ptr(out), out_len)
+    if rc < 0:
+        raise RuntimeError(f"oracle restart failed: {rc}")
+    return out, rc
+
+
+def list_restart(diffs, chkpt_idx, out_len=None, init=None):
+    """List host-view restart (src/list_approach.cpp:259-586). Returns (buffer, rc)."""
+    return _restart(lib().oracle_list_restart, diffs, chkpt_idx, out_len, init)
 
 
 def restart(diffs, chkpt_idx, out_len=None, init=None):

@@ -5,8 +5,8 @@ hand-written sm_100a CUDA kernels behind the C ABI in include/b200dedup.h
 (libb200dedup.so, built in this directory), with this Python mirror of its interface.
 """
 from ._lib import HASH_MD5, HASH_MURMUR3, B2DError, lib, lib_path  # noqa: F401
-from .tree import TreeDeduplicator, hash_chunks, parse_header  # noqa: F401
+from .tree import ListDeduplicator, TreeDeduplicator, hash_chunks, parse_header  # noqa: F401
 from .batch import CheckpointBatch  # noqa: F401
 
-__all__ = ["TreeDeduplicator", "CheckpointBatch", "hash_chunks", "parse_header", "HASH_MURMUR3", "HASH_MD5", "B2DError", "lib",
+__all__ = ["TreeDeduplicator", "ListDeduplicator", "CheckpointBatch", "hash_chunks", "parse_header", "HASH_MURMUR3", "HASH_MD5", "B2DError", "lib",
            "lib_path"]

@@ -24,6 +24,7 @@ _vp, _u32, _u64, _int, _cc = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, 
 _u8pp = ctypes.POINTER(ctypes.POINTER(ctypes.c_uint8))
 SIGNATURES = [
     ("b2d_create", _int, [_u32, _int, ctypes.POINTER(_vp)]),
+    ("b2d_create_list", _int, [_u32, _int, ctypes.POINTER(_vp)]),
     ("b2d_destroy", _int, [_vp]),
     ("b2d_set_stream", _int, [_vp, _vp]),
     ("b2d_set_param", _int, [_vp, _cc, ctypes.c_int64]),

@@ -1,17 +1,19 @@
-// dedup_files: deduplicate a sequence of checkpoint files with the B200 tree deduplicator.
+// dedup_files: deduplicate a sequence of checkpoint files with the B200 deduplicators.
 //
 // Command line of the reference's driver (src/dedup_files.cpp:10-21, argv layout :30-48):
-//   dedup_files chunk_size num_chkpts --run-tree-chkpt file_0 ... file_{num_chkpts-1}
+//   dedup_files chunk_size num_chkpts --run-tree-chkpt|--run-list-chkpt file_0 ... file_{num_chkpts-1}
 // Each file is loaded into device memory and checkpointed in order (file_0 as the baseline);
-// the diff is written next to it as <file>.hashtree.incr_chkpt and the reference's per-
-// checkpoint log under the file's base name (src/dedup_files.cpp:88-102).  Only the tree
-// approach is built here; the reference's other approaches (full, basic, list) are rejected.
+// the diff is written next to it as <file>.hashtree.incr_chkpt (tree) or
+// <file>.hashlist.incr_chkpt (list), and the reference's per-checkpoint log under the file's
+// base name (src/dedup_files.cpp:88-102).  The tree and list approaches are built here; the
+// reference's full and basic approaches are rejected.
 #include <cuda_runtime.h>
 
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -28,13 +30,14 @@ static bool read_file(const std::string& path, std::vector<uint8_t>& out) {
 
 int main(int argc, char** argv) {
   if (argc < 5) {
-    std::fprintf(stderr, "usage: %s chunk_size num_chkpts --run-tree-chkpt file...\n", argv[0]);
+    std::fprintf(stderr, "usage: %s chunk_size num_chkpts --run-tree-chkpt|--run-list-chkpt file...\n", argv[0]);
     return 1;
   }
   const uint32_t chunk_size = (uint32_t)std::strtoul(argv[1], nullptr, 10);
   const uint32_t num_chkpts = (uint32_t)std::strtoul(argv[2], nullptr, 10);
-  if (std::strcmp(argv[3], "--run-tree-chkpt") != 0) {
-    std::fprintf(stderr, "error: mode %s is not built here; only --run-tree-chkpt\n", argv[3]);
+  const bool list = std::strcmp(argv[3], "--run-list-chkpt") == 0;
+  if (!list && std::strcmp(argv[3], "--run-tree-chkpt") != 0) {
+    std::fprintf(stderr, "error: mode %s is not built here; only --run-tree-chkpt and --run-list-chkpt\n", argv[3]);
     return 2;
   }
   if (chunk_size == 0 || (uint32_t)argc < 4 + num_chkpts) {
@@ -42,7 +45,9 @@ int main(int argc, char** argv) {
     return 1;
   }
   try {
-    b2d::TreeDeduplicator dedup(chunk_size);
+    std::unique_ptr<b2d::TreeDeduplicator> owner(list ? new b2d::ListDeduplicator(chunk_size)
+                                                      : new b2d::TreeDeduplicator(chunk_size));
+    b2d::TreeDeduplicator& dedup = *owner;
     std::vector<uint8_t> host;
     uint8_t* dev = nullptr;
     size_t cap = 0;
@@ -61,7 +66,7 @@ int main(int argc, char** argv) {
         }
       }
       if (cudaMemcpy(dev, host.data(), host.size(), cudaMemcpyHostToDevice) != cudaSuccess) return 4;
-      std::string filename = path + ".hashtree.incr_chkpt";
+      std::string filename = path + (list ? ".hashlist.incr_chkpt" : ".hashtree.incr_chkpt");
       std::string logname = path.substr(path.rfind('/') + 1);
       dedup.checkpoint(dev, host.size(), filename, logname, idx == 0);
       std::printf("checkpoint %u: %s -> %s (first regions %zu, shifted regions %zu)\n", idx, path.c_str(),

@@ -1,9 +1,11 @@
-// restart_chkpt_files: rebuild one checkpoint from <file>.hashtree.incr_chkpt diffs.
+// restart_chkpt_files: rebuild one checkpoint from <file>.hashtree.incr_chkpt (tree) or
+// <file>.hashlist.incr_chkpt (list) diffs.
 //
 // Command line of the reference's driver (src/restart_chkpt_files.cpp:26-45):
-//   restart_chkpt_files restart_id num_chkpts num_tests chunk_size --run-tree-chkpt file...
+//   restart_chkpt_files restart_id num_chkpts num_tests chunk_size --run-tree-chkpt|--run-list-chkpt file...
 // `file_i` are the original checkpoint files (their sizes give the restart length, :72-77);
-// the diffs are read from file_i.hashtree.incr_chkpt (:57-60, :171-184).  Checkpoint
+// the diffs are read from file_i.hashtree.incr_chkpt (:57-60, :171-184) or
+// file_i.hashlist.incr_chkpt (:53-56, :140-151).  Checkpoint
 // `restart_id` is rebuilt `num_tests` times into device memory and its digest printed the way
 // the reference does (:188-195, include/hash_functions.hpp:47-63: the chunk hash of the whole
 // buffer, upper-case hex, a space after every 4 bytes).
@@ -13,6 +15,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -34,7 +37,8 @@ static long file_size(const std::string& path) {
 
 int main(int argc, char** argv) {
   if (argc < 7) {
-    std::fprintf(stderr, "usage: %s restart_id num_chkpts num_tests chunk_size --run-tree-chkpt file...\n",
+    std::fprintf(stderr,
+                 "usage: %s restart_id num_chkpts num_tests chunk_size --run-tree-chkpt|--run-list-chkpt file...\n",
                  argv[0]);
     return 1;
   }
@@ -42,10 +46,12 @@ int main(int argc, char** argv) {
   const uint32_t num_chkpts = (uint32_t)std::strtoul(argv[2], nullptr, 10);
   const uint32_t num_tests = (uint32_t)std::strtoul(argv[3], nullptr, 10);
   const uint32_t chunk_size = (uint32_t)std::strtoul(argv[4], nullptr, 10);
-  if (std::strcmp(argv[5], "--run-tree-chkpt") != 0) {
-    std::fprintf(stderr, "error: mode %s is not built here; only --run-tree-chkpt\n", argv[5]);
+  const bool list = std::strcmp(argv[5], "--run-list-chkpt") == 0;
+  if (!list && std::strcmp(argv[5], "--run-tree-chkpt") != 0) {
+    std::fprintf(stderr, "error: mode %s is not built here; only --run-tree-chkpt and --run-list-chkpt\n", argv[5]);
     return 2;
   }
+  const std::string suffix = list ? ".hashlist.incr_chkpt" : ".hashtree.incr_chkpt";
   if (chunk_size == 0 || restart_id >= num_chkpts || (uint32_t)argc < 6 + num_chkpts) {
     std::fprintf(stderr, "error: expected chunk_size > 0, restart_id < num_chkpts and %u files\n", num_chkpts);
     return 1;
@@ -59,8 +65,8 @@ int main(int argc, char** argv) {
   }
   std::vector<std::vector<uint8_t>> diffs(num_chkpts);
   for (uint32_t i = 0; i < num_chkpts; i++) {
-    if (!read_file(files[i] + ".hashtree.incr_chkpt", diffs[i])) {
-      std::fprintf(stderr, "error: cannot read %s.hashtree.incr_chkpt\n", files[i].c_str());
+    if (!read_file(files[i] + suffix, diffs[i])) {
+      std::fprintf(stderr, "error: cannot read %s%s\n", files[i].c_str(), suffix.c_str());
       return 3;
     }
   }
@@ -74,7 +80,9 @@ int main(int argc, char** argv) {
   try {
     for (uint32_t t = 0; t < num_tests; t++) {
       cudaMemset(dev, 0, (size_t)len);
-      b2d::TreeDeduplicator dedup(chunk_size);
+      std::unique_ptr<b2d::TreeDeduplicator> owner(list ? new b2d::ListDeduplicator(chunk_size)
+                                                        : new b2d::TreeDeduplicator(chunk_size));
+      b2d::TreeDeduplicator& dedup = *owner;
       std::string logname = files[restart_id].substr(files[restart_id].rfind('/') + 1);
       dedup.restart(dev, (size_t)len, diffs, logname, restart_id);
       if (cudaMemcpy(host.data(), dev, (size_t)len, cudaMemcpyDeviceToHost) != cudaSuccess) {
@@ -90,7 +98,7 @@ int main(int argc, char** argv) {
         s += hexchars[dg[k] & 0xF];
         if (k % 4 == 3) s += ' ';
       }
-      std::printf("Hashtree digest:       %s\n", s.c_str());
+      std::printf(list ? "Hashlist digest:       %s\n" : "Hashtree digest:       %s\n", s.c_str());
     }
   } catch (const b2d::Error& e) {
     std::fprintf(stderr, "error: %s\n", e.what());

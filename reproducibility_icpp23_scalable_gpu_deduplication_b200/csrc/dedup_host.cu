@@ -151,6 +151,7 @@ struct b2d_dedup {
   double timers[4] = {0, 0, 0, 0};
   double restart_timers[2] = {0, 0};
   int kind = HASH_MURMUR3;
+  int list = 0;   // 1: ListDeduplicator (src/list_approach.cpp), 0: TreeDeduplicator
 
   uint32_t n = 0, N = 0, D = 0;
   uint64_t F = 0, S = 0;
@@ -448,6 +449,8 @@ int prepare_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, bool make
     if (rc) return rc;
     d->have_tree = true;
     d->baseline_id = d->current_id;
+    // the list approach starts a baseline from an all-zero digest list (src/list_approach.cpp:865-869)
+    if (d->list) B2D_CU(cudaMemsetAsync(d->tree.p + (d->n - 1u), 0, sizeof(Digest) * (size_t)d->n, d->stream));
   } else {
     int rc = map_ensure(d);
     if (rc) return rc;
@@ -476,7 +479,9 @@ int prepare_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, bool make
   RoundState* r = d->round_h.p;
   r->cur = d->current_id;
   r->baseline_id = d->baseline_id;
-  r->baseline = baseline ? 1u : 0u;
+  // the list approach applies one per-chunk rule to every checkpoint (src/list_approach.cpp:41-71):
+  // the incremental leaf rule against a list that a baseline has zeroed
+  r->baseline = (baseline && !d->list) ? 1u : 0u;
   r->buckets = d->current_id + 1u;
   map_view(d, r->map);
   return B2D_OK;
@@ -494,7 +499,7 @@ void graph_key(const b2d_dedup* d, const RoundState* rs_dev, std::vector<uint64_
             (uint64_t)d->state.p, (uint64_t)d->state_h.p, (uint64_t)d->round_h.p, (uint64_t)rs_dev, d->bcap,
             (uint64_t)d->tune.allow_tma, (uint64_t)d->tune.stages, (uint64_t)d->tune.ctas_per_sm, (uint64_t)d->graph_timing,
             (uint64_t)d->tune.unit,
-            (uint64_t)d->sm_count});
+            (uint64_t)d->sm_count, (uint64_t)d->list});
 }
 
 // Device work of one checkpoint on `s`.  `rs_dev` is where the kernels read this checkpoint's
@@ -535,20 +540,32 @@ int enqueue_checkpoint(b2d_dedup* d, cudaStream_t s, RoundState* rs_dev, bool up
     d->leaf_tma = leaf_path == 1;
   }
   if (timing) B2D_CU(record_timing(d->ev[3], s));
-  if (!skip_forest) {
+  if (d->list) {
+    // list approach: no tree; per-chunk labels and region flags (src/list_approach.cpp:41-71)
+    B2D_CU(launch_list_label(forest_args(d, rs_dev), d->sm_count, s));
+  } else if (!skip_forest) {
     const ForestArgs fa = forest_args(d, rs_dev);
     B2D_CU(launch_forest(fa, 1, s));
     B2D_CU(launch_zero_exists(&ds->zero_exists, rs_dev, s));
     B2D_CU(launch_forest(fa, 2, s));
   }
   if (timing) B2D_CU(record_timing(d->ev[1], s));
-  // collect_diff (:511-710); a batch may assemble all its handles' diffs in shared launches
-  if (!skip_diff) B2D_CU(launch_collect_diff(diff_args(d, rs_dev), d->bcap, d->sm_count, s));
+  // collect_diff (:511-710; list approach src/list_approach.cpp:79-257, single-chunk regions in
+  // chunk order, chunk indices in the diff); a batch may assemble all its handles' diffs in
+  // shared launches
+  if (!skip_diff) {
+    DiffArgs da = diff_args(d, rs_dev);
+    if (d->list) da.id_bias = d->n - 1u;
+    B2D_CU(launch_collect_diff(da, d->bcap, d->sm_count, s, d->list != 0));
+  }
   if (timing) B2D_CU(record_timing(d->ev[2], s));
   if (!managed) B2D_CU(cudaMemcpyAsync(d->state_h.p, d->state.p, sizeof(DevState), cudaMemcpyDeviceToHost, s));
-  d->launches = (skip_leaves ? 0 : 1) +
-                (skip_forest ? 0 : forest_launch_count(d->D, 1) + forest_launch_count(d->D, 2) + 1) +
-                (skip_diff ? 0 : 14);
+  if (d->list)
+    d->launches = (skip_leaves ? 0 : 1) + 1 + (skip_diff ? 0 : 12);
+  else
+    d->launches = (skip_leaves ? 0 : 1) +
+                  (skip_forest ? 0 : forest_launch_count(d->D, 1) + forest_launch_count(d->D, 2) + 1) +
+                  (skip_diff ? 0 : 14);
   return B2D_OK;
 }
 
@@ -674,13 +691,14 @@ int write_chkpt_log(b2d_dedup* d, const uint8_t* diff, uint64_t diff_len, const 
     snprintf(b, sizeof b, "%g", v);
     return std::string(b);
   };
-  fprintf(result, "Tree,%u,%u,%llu,%llu,%llu,%llu,%s,%s,%s,%s\n", id, d->chunk_size,
+  const char* approach = d->list ? "List" : "Tree";
+  fprintf(result, "%s,%u,%u,%llu,%llu,%llu,%llu,%s,%s,%s,%s\n", approach, id, d->chunk_size,
           (unsigned long long)d->data_len, (unsigned long long)(d->datasizes[0] + d->datasizes[1]),
           (unsigned long long)d->datasizes[0], (unsigned long long)d->datasizes[1], g(d->timers[0]).c_str(),
           g(d->timers[1]).c_str(), g(d->timers[2]).c_str(), g(d->timers[3]).c_str());
-  fprintf(timing, "Tree,%u,%u,%s,%s,%s\n", id, d->chunk_size, g(d->timers[1]).c_str(), g(d->timers[2]).c_str(),
+  fprintf(timing, "%s,%u,%u,%s,%s,%s\n", approach, id, d->chunk_size, g(d->timers[1]).c_str(), g(d->timers[2]).c_str(),
           g(d->timers[3]).c_str());
-  fprintf(size, "Tree,%u,%u,%llu,%llu,", id, d->chunk_size, (unsigned long long)d->datasizes[0],
+  fprintf(size, "%s,%u,%u,%llu,%llu,", approach, id, d->chunk_size, (unsigned long long)d->datasizes[0],
           (unsigned long long)d->datasizes[1]);
   // write_metadata_breakdown (src/utils.cpp:38-124)
   uint32_t h[8];
@@ -719,7 +737,8 @@ int write_chkpt_log(b2d_dedup* d, const uint8_t* diff, uint64_t diff_len, const 
 int write_restart_log(b2d_dedup* d, uint32_t id, const std::string& logname) {
   FILE* f = fopen(logname.c_str(), "a");
   if (!f) return B2D_OK;   // the reference ignores an unopenable restart log ("/dev/null/")
-  fprintf(f, "Tree,%u,%u,%g,%g\n", id, d->chunk_size, d->restart_timers[0], d->restart_timers[1]);
+  fprintf(f, "%s,%u,%u,%g,%g\n", d->list ? "List" : "Tree", id, d->chunk_size, d->restart_timers[0],
+          d->restart_timers[1]);
   fclose(f);
   return B2D_OK;
 }
@@ -847,6 +866,8 @@ int do_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* di
   a.partial = d->r_partial.p;
   a.total = d->r_total.p;
   a.st = &d->state.p->status;
+  // list diffs name chunks; the restart kernels work on leaf heap indices (leaf of chunk c = n-1+c)
+  a.id_bias = d->list ? n - 1u : 0u;
   RestartWalk w{};
   w.main_cur = h.chkpt_id;
   w.n = n;
@@ -925,7 +946,7 @@ int do_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* di
     a.ncum = (uint32_t)ncum;
     a.slot = slot(is_main ? 0 : wcount);
     B2D_CU(launch_restart_diff(a, &d->state.p->straddle, d->sm_count, d->stream));
-    d->launches += restart_diff_launches(n);
+    d->launches += restart_diff_launches(n, d->list != 0);
     if (!is_main) {
       // the window's walk copies from every diff in it, which share one chunk size
       if (wcount == 0) w.cs = hh.cs;
@@ -1168,6 +1189,7 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
   if (count == 0) return B2D_OK;
   for (uint32_t i = 0; i < count; i++) {
     if (!hs[i]) return B2D_ERR_ARG;
+    if (hs[i]->list) return B2D_ERR_UNSUPPORTED;   // the batched form runs tree handles
     for (uint32_t j = 0; j < i; j++)
       if (hs[j] == hs[i]) return B2D_ERR_ARG;   // one checkpoint per handle per batch
   }
@@ -1596,6 +1618,12 @@ int batch_finish(b2d_batch* b, int* rcs) {
   }
 
 extern "C" {
+
+int b2d_create_list(uint32_t chunk_size, int hash_kind, b2d_dedup** out) {
+  const int rc = b2d_create(chunk_size, hash_kind, out);
+  if (rc == B2D_OK) (*out)->list = 1;
+  return rc;
+}
 
 int b2d_create(uint32_t chunk_size, int hash_kind, b2d_dedup** out) {
   B2D_GUARD({

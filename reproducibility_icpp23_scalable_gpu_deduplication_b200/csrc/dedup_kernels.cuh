@@ -92,6 +92,8 @@ struct DiffArgs {
   uint32_t* partial2;     // SCAN_GRID * 2 scratch
   uint8_t* diff;          // device diff buffer
   const RoundState* rs;
+  uint32_t id_bias;       // subtracted from every node id written into the diff (list approach:
+                          // n - 1, so leaf heap indices become chunk indices; tree: 0)
 };
 
 // launch parameters carry the buffer geometry; the per-checkpoint values come from *rs
@@ -175,8 +177,15 @@ cudaError_t launch_forest_seg(const ForestSeg& s, int phase, int kind, uint32_t 
 cudaError_t launch_zero_exists_seg(const ForestArgs* args, uint32_t n, cudaStream_t stream);
 int forest_launch_count(uint32_t D, int phase);
 cudaError_t launch_zero_exists(int* flag, const RoundState* rs, cudaStream_t stream);
-// bcap: bucket capacity the scratch was sized for (>= rs->buckets of every checkpoint run)
-cudaError_t launch_collect_diff(const DiffArgs& a, uint32_t bcap, int sm_count, cudaStream_t stream);
+// bcap: bucket capacity the scratch was sized for (>= rs->buckets of every checkpoint run).
+// node_order: the region lists stay in node order (the list approach's order, whose regions
+// are single leaves) instead of the tree's level-descending order.
+cudaError_t launch_collect_diff(const DiffArgs& a, uint32_t bcap, int sm_count, cudaStream_t stream,
+                                bool node_order = false);
+// the list approach's labels: the lowest-index owner of a digest shared by several changed
+// chunks stays the first occurrence, the others become shifted duplicates; region flags are
+// set for both (src/list_approach.cpp:41-71)
+cudaError_t launch_list_label(const ForestArgs& a, int sm_count, cudaStream_t stream);
 
 // Diff assembly of many handles in one launch per step (batched form).  A segmented launch
 // gives handle h the CTAs beg[h] .. beg[h+1]-1 and runs its kernels as if launched alone on

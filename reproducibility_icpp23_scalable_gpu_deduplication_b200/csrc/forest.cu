@@ -580,6 +580,44 @@ cudaError_t launch_zero_exists(int* flag, const RoundState* rs, cudaStream_t str
   return cudaGetLastError();
 }
 
+// List approach (src/list_approach.cpp:41-71): a changed chunk whose digest was new is a first
+// occurrence, one whose digest existed is a shifted duplicate.  The leaf stage labelled every
+// changed chunk of a digest shared within this checkpoint a first occurrence and flagged it;
+// in the reference's sequential order the lowest chunk index inserts first, which is the map
+// entry's owner after the leaf stage's minimum, so the others become shifted duplicates.  The
+// region flags for the diff are set per chunk (its leaf), and the duplicate flags are cleared.
+__global__ void list_label_kernel(ForestArgs a0) {
+  const ForestArgs a = with_round(a0);
+  for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < a.n; c += (uint64_t)gridDim.x * blockDim.x) {
+    uint8_t lab = a.leaflab[c];
+    const uint32_t leaf = a.n - 1u + (uint32_t)c;
+    if (a.dupflag[c]) {
+      a.dupflag[c] = 0;
+      if (lab == FIRST_OCUR) {
+        const uint64_t slot = map_find(a.map, a.tree[leaf]);
+        if (slot <= a.map.cap) {
+          if (map_tree(a.map, slot) == a.cur && map_node(a.map, slot) != leaf) {
+            lab = SHIFT_DUPL;
+            a.leaflab[c] = lab;
+          }
+        } else {
+          set_error(a.st, DERR_INTERNAL, 11);
+        }
+      }
+    }
+    if (lab == FIRST_OCUR) a.push[leaf] = PUSH_FIRST;
+    else if (lab == SHIFT_DUPL) a.push[leaf] = PUSH_SHIFT;
+  }
+}
+
+cudaError_t launch_list_label(const ForestArgs& a, int sm_count, cudaStream_t stream) {
+  const uint64_t want = ((uint64_t)a.n + 255u) / 256u;
+  const uint64_t cap = (uint64_t)sm_count * 8u;
+  const uint32_t grid = (uint32_t)(want < cap ? (want ? want : 1) : cap);
+  list_label_kernel<<<grid, 256, 0, stream>>>(a);
+  return cudaGetLastError();
+}
+
 
 
 }  // namespace b2d

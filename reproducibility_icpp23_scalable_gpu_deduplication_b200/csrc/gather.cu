@@ -472,8 +472,8 @@ __device__ __forceinline__ void shift_write_body(const DiffArgs& a, uint32_t bid
     __syncwarp();
     if (act) {
       uint32_t* e = reinterpret_cast<uint32_t*>(a.diff + shift_off + 8ull * pos);
-      e[0] = a.shift_list[i];
-      e[1] = a.sprev[i];
+      e[0] = a.shift_list[i] - a.id_bias;
+      e[1] = a.sprev[i] - a.id_bias;
     }
   }
 }
@@ -507,7 +507,7 @@ __device__ __forceinline__ void gather_vec_body(const DiffArgs& a, uint32_t bid,
   uint32_t* first_meta = reinterpret_cast<uint32_t*>(a.diff + m.first_off);
   const uint64_t gtid = bid * (uint64_t)blockDim.x + threadIdx.x;
   const uint64_t nthr = (uint64_t)nb * blockDim.x;
-  for (uint64_t i = gtid; i < m.F; i += nthr) first_meta[i] = a.first_list[i];
+  for (uint64_t i = gtid; i < m.F; i += nthr) first_meta[i] = a.first_list[i] - a.id_bias;
   if (m.T == 0) return;
   constexpr uint32_t CPW = 32u / LPC;   // chunks per warp iteration
   const uint32_t lane = threadIdx.x & 31u;
@@ -603,7 +603,7 @@ __device__ __forceinline__ void gather_bytes_body(const DiffArgs& a, uint32_t bi
   const uint64_t gtid = bid * (uint64_t)blockDim.x + threadIdx.x;
   const uint64_t nthr = (uint64_t)nb * blockDim.x;
   for (uint64_t i = gtid; i < m.F; i += nthr) {
-    const uint32_t v = a.first_list[i];
+    const uint32_t v = a.first_list[i] - a.id_bias;
     memcpy(first_meta + 4 * i, &v, 4);
   }
   for (uint64_t k = gtid; k < m.T; k += nthr) {
@@ -684,7 +684,9 @@ cudaError_t launch_collect_diff_batch(const DiffBatch& b, cudaStream_t stream, u
   return cudaGetLastError();
 }
 
-cudaError_t launch_collect_diff(const DiffArgs& a, uint32_t bcap, int sm_count, cudaStream_t stream) {
+cudaError_t launch_collect_diff(const DiffArgs& args, uint32_t bcap, int sm_count, cudaStream_t stream,
+                                bool node_order) {
+  DiffArgs a = args;
   const DiffGrids dg = diff_grids(a, sm_count);
   const uint32_t g = dg.g, gs = dg.gs;
   const uint32_t B = bcap;   // capacity; each kernel reads the checkpoint's bucket count from rs
@@ -692,8 +694,13 @@ cudaError_t launch_collect_diff(const DiffArgs& a, uint32_t bcap, int sm_count, 
   compact_count_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);
   compact_scan_kernel<<<1, 1024, 0, stream>>>(a, g);
   compact_write_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);
-  compact_levels_kernel<<<dg.gl, 256, 0, stream>>>(a);
-  compact_permute_kernel<<<dg.gp, 256, 0, stream>>>(a);
+  if (node_order) {
+    a.first_list = a.tmp_first;
+    a.shift_list = a.tmp_shift;
+  } else {
+    compact_levels_kernel<<<dg.gl, 256, 0, stream>>>(a);
+    compact_permute_kernel<<<dg.gp, 256, 0, stream>>>(a);
+  }
   region_count_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);
   region_scan_kernel<<<1, 1024, 0, stream>>>(a, g);
   region_write_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);

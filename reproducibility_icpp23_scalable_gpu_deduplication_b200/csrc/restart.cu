@@ -48,6 +48,13 @@ __device__ __forceinline__ uint32_t rd_u32(const uint8_t* p) {
   memcpy(&v, p, 4);
   return v;
 }
+// a node id of the diff as a heap index: list diffs name chunk c, whose leaf is n-1+c; a chunk
+// id outside the checkpoint maps to N, one past the last node, which every use rejects
+__device__ __forceinline__ uint32_t rd_node(const RestartArgs& a, const uint8_t* p) {
+  const uint32_t v = rd_u32(p);
+  if (!a.id_bias) return v;
+  return v < a.n ? v + a.id_bias : a.N;
+}
 
 __device__ __forceinline__ void copy_bytes(uint8_t* dst, const uint8_t* src, uint64_t nb) {
   if ((((uintptr_t)dst | (uintptr_t)src) & 15u) == 0) {
@@ -164,12 +171,12 @@ __device__ __forceinline__ uint32_t shift_tree(const RestartArgs& a, uint64_t i)
 __device__ __forceinline__ uint32_t entry_len(const RestartArgs& a, uint64_t i, int which, bool want_meta) {
   if (which == 0) {
     uint32_t lo, hi;
-    leaf_range(rd_u32(a.diff + a.first_off + 4 * i), a.N, lo, hi);
+    leaf_range(rd_node(a, a.diff + a.first_off + 4 * i), a.N, lo, hi);
     if (want_meta) a.rstart[i] = lo;
     return hi - lo + 1u;
   }
-  const uint32_t node = rd_u32(a.diff + a.shift_off + 8 * i);
-  const uint32_t prev = rd_u32(a.diff + a.shift_off + 8 * i + 4);
+  const uint32_t node = rd_node(a, a.diff + a.shift_off + 8 * i);
+  const uint32_t prev = rd_node(a, a.diff + a.shift_off + 8 * i + 4);
   uint32_t nlo, nhi, plo, phi;
   leaf_range(node, a.N, nlo, nhi);
   leaf_range(prev, a.N, plo, phi);
@@ -483,7 +490,7 @@ static void copy_width(uint64_t dst_al, uint64_t src_al, uint32_t cs, uint32_t& 
   if (per && (per & (per - 1u)) == 0) per_log2 = (uint32_t)__builtin_ctz(per);
 }
 
-int restart_diff_launches(uint32_t n) { return 8 + (straddle_query(n).count ? 2 : 0); }
+int restart_diff_launches(uint32_t n, bool list) { return 8 + (!list && straddle_query(n).count ? 2 : 0); }
 
 cudaError_t launch_restart_diff(const RestartArgs& args, StraddleInfo* sd, int sm_count, cudaStream_t s) {
   RestartArgs a = args;
@@ -498,7 +505,7 @@ cudaError_t launch_restart_diff(const RestartArgs& args, StraddleInfo* sd, int s
   r_scan_kernel<<<1, 1024, 0, s>>>(a, g);
   r_write_kernel<<<g, R_THREADS, 0, s>>>(a, 0);
   r_expand_first_kernel<<<grid_for(a.n, sm_count), R_THREADS, 0, s>>>(a);
-  const StraddleQuery q = straddle_query(a.n);
+  const StraddleQuery q = a.id_bias ? StraddleQuery{} : straddle_query(a.n);   // list regions are single leaves
   if (q.count) {
     e = cudaMemsetAsync(sd, 0, sizeof(StraddleInfo), s);
     if (e != cudaSuccess) return e;

@@ -44,6 +44,9 @@ struct RestartArgs {
   uint32_t* partial;       // SCAN_GRID
   unsigned long long* total;
   DevStatus* st;
+  // added to every node id read from the diff: list-approach diffs name chunks, which the
+  // restart handles as the leaves n-1+c of the same heap (0 for tree diffs)
+  uint32_t id_bias;
   // chunk copies (set by launch_restart_diff): piece width in bytes (16/8/4, dividing the chunk
   // size and the alignment of `out` and of the data section; 0: one lane copies a whole chunk),
   // pieces per chunk and its log2 (0xff when not a power of two)
@@ -95,6 +98,6 @@ cudaError_t launch_restart_diff(const RestartArgs& a, StraddleInfo* sd, int sm_c
 // resolves the chunks owed by the window's diffs and copies them
 cudaError_t launch_restart_walk(const RestartWalk& w, int sm_count, cudaStream_t s);
 // kernel launches made by one launch_restart_diff call (a walk is one launch)
-int restart_diff_launches(uint32_t n);
+int restart_diff_launches(uint32_t n, bool list);
 
 }  // namespace b2d

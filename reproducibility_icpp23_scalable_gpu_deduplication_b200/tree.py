@@ -13,7 +13,7 @@ import numpy as np
 from . import _lib
 from ._lib import HASH_MD5, HASH_MURMUR3, check, lib
 
-__all__ = ["TreeDeduplicator", "hash_chunks", "HASH_MURMUR3", "HASH_MD5", "HEADER_BYTES", "parse_header"]
+__all__ = ["TreeDeduplicator", "ListDeduplicator", "hash_chunks", "HASH_MURMUR3", "HASH_MD5", "HEADER_BYTES", "parse_header"]
 
 HEADER_BYTES = 32
 
@@ -59,9 +59,11 @@ def parse_header(diff):
 class TreeDeduplicator:
     """One deduplicated buffer: TreeDeduplicator(uint32_t bytes_per_chunk) (src/tree_approach.cpp:5-9)."""
 
+    _create = "b2d_create"
+
     def __init__(self, chunk_size, hash_kind=HASH_MURMUR3):
         h = ctypes.c_void_p()
-        check(lib().b2d_create(int(chunk_size), int(hash_kind), ctypes.byref(h)), "b2d_create")
+        check(getattr(lib(), self._create)(int(chunk_size), int(hash_kind), ctypes.byref(h)), self._create)
         self._h = h
         self.chunk_size = int(chunk_size)
         self.hash_kind = int(hash_kind)
@@ -289,6 +291,18 @@ def estimate_memory(nbytes, chunk_size, map_max_load_pct=0):
     check(lib().b2d_estimate_memory(int(nbytes), int(chunk_size), int(map_max_load_pct), ctypes.byref(v)),
           "b2d_estimate_memory")
     return v.value
+
+
+
+class ListDeduplicator(TreeDeduplicator):
+    """The list approach: ListDeduplicator(uint32_t bytes_per_chunk) (src/list_approach.cpp:5-9).
+
+    Same methods and argument meaning as ``TreeDeduplicator`` (include/list_approach.hpp): one
+    digest per chunk, a changed chunk is a first occurrence or a shifted duplicate of an earlier
+    one, and the diff names chunk indices (src/list_approach.cpp:23-257).  Restarts take list
+    diffs (:259-586).  Not usable with ``CheckpointBatch``."""
+
+    _create = "b2d_create_list"
 
 
 def hash_chunks(data, chunk_size, hash_kind=HASH_MURMUR3):

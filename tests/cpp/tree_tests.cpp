@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <random>
 #include <string>
 #include <vector>
@@ -60,10 +61,14 @@ static int run_case(const char* s0, const char* s1, size_t first, size_t shift) 
   return (dedup.num_first_ocur() == first && dedup.num_shift_dupl() == shift) ? 0 : 1;
 }
 
-static int run_tree_chkpt(uint32_t chunk_size, uint32_t num_chkpts) {
+// tree_chkpt / list_chkpt (test/tree_chkpt.cpp, test/list_chkpt.cpp): random 1 MiB checkpoints,
+// each restarted from the diffs so far and compared with the data
+static int run_tree_chkpt(uint32_t chunk_size, uint32_t num_chkpts, bool list = false) {
   const size_t len = 1024 * 1024;
   std::mt19937_64 rng(1931);
-  b2d::TreeDeduplicator dedup(chunk_size);
+  std::unique_ptr<b2d::TreeDeduplicator> owner(list ? new b2d::ListDeduplicator(chunk_size)
+                                                    : new b2d::TreeDeduplicator(chunk_size));
+  b2d::TreeDeduplicator& dedup = *owner;
   std::vector<std::vector<uint8_t>> chkpts;
   std::string null("/dev/null/");
   uint8_t* d = nullptr;
@@ -139,6 +144,8 @@ int main(int argc, char** argv) {
       return run_case(argv[2], argv[3], strtoull(argv[4], nullptr, 10), strtoull(argv[5], nullptr, 10));
     if (argc == 4 && std::string(argv[1]) == "tree_chkpt")
       return run_tree_chkpt((uint32_t)atoi(argv[2]), (uint32_t)atoi(argv[3]));
+    if (argc == 4 && std::string(argv[1]) == "list_chkpt")
+      return run_tree_chkpt((uint32_t)atoi(argv[2]), (uint32_t)atoi(argv[3]), true);
     if (argc == 3 && std::string(argv[1]) == "batch") return run_batch((uint32_t)atoi(argv[2]));
   } catch (const b2d::Error& e) {
     printf("error: %s\n", e.what());

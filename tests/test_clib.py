@@ -86,9 +86,9 @@ def test_file_tools_build_and_check_arguments():
         assert os.path.exists(_build.tool_path(name))
     r = subprocess.run([_build.tool_path("dedup_files")], capture_output=True, text=True)
     assert r.returncode == 1 and "usage" in r.stderr
-    r = subprocess.run([_build.tool_path("dedup_files"), "128", "1", "--run-list-chkpt", "x"],
+    r = subprocess.run([_build.tool_path("dedup_files"), "128", "1", "--run-basic-chkpt", "x"],
                        capture_output=True, text=True)
-    assert r.returncode == 2 and "only --run-tree-chkpt" in r.stderr
+    assert r.returncode == 2 and "only --run-tree-chkpt and --run-list-chkpt" in r.stderr
     r = subprocess.run([_build.tool_path("restart_chkpt_files"), "0", "1", "1", "128", "--run-full-chkpt", "x"],
                        capture_output=True, text=True)
     assert r.returncode == 2

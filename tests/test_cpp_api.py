@@ -46,6 +46,14 @@ def test_cpp_tree_chkpt(cuda, cs):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("cs", [128, 64, 4096])
+def test_cpp_list_chkpt(cuda, cs):
+    """test/list_chkpt.cpp of the reference through b2d::ListDeduplicator"""
+    r = subprocess.run([build_cpp(), "list_chkpt", str(cs), "10"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+
+
+@pytest.mark.gpu
 def test_cpp_checkpoint_batch(cuda):
     r = subprocess.run([build_cpp(), "batch", "9"], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
