@@ -47,6 +47,9 @@ def parse():
                    help="plain form: the 4 GiB Murmur3 series (default), the 8 GiB float32 MD5 series, or "
                         "the 64 MiB CPU-runnable series (5% rewritten, 2% shifted, 1% zeroed per checkpoint)")
     p.add_argument("--chunk-size", type=int, default=None, help="default 128 (plain_4g) / 256 (md5_f32_8g)")
+    p.add_argument("--approach", default="tree", choices=["tree", "list"],
+                   help="plain form and reference arm: the tree approach (default) or the list approach "
+                        "(ListDeduplicator); the batched and served forms run the tree approach")
     p.add_argument("--nbytes", type=int, default=None, help="default 4 GiB (plain_4g) / 8 GiB (md5_f32_8g)")
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--cpu-sample-bytes", type=int, default=512 << 20)
@@ -152,13 +155,14 @@ def workload_series(workload, nbytes, cs, device, seed):
     return synth.plain_4g(nbytes=nbytes, chunk_size=cs, device=device, seed=seed)
 
 
-def cpu_baseline_run(nbytes, cs, steps, threads, workload="plain_4g"):
+def cpu_baseline_run(nbytes, cs, steps, threads, workload="plain_4g", approach="tree"):
     """The oracle (sequential restatement of the reference) on the host, all threads hashing."""
     from oracle import oracle as O
     from reproducibility_icpp23_scalable_gpu_deduplication_b200 import synth
 
     s = workload_series(workload, nbytes, cs, None, synth.SEED)
-    o = O.OracleTreeDeduplicator(cs, O.HASH_MD5 if workload == "md5_f32_8g" else O.HASH_MURMUR3, threads=threads)
+    cls = O.OracleListDeduplicator if approach == "list" else O.OracleTreeDeduplicator
+    o = cls(cs, O.HASH_MD5 if workload == "md5_f32_8g" else O.HASH_MURMUR3, threads=threads)
     o.checkpoint(s.next(), True)
     t = 0.0
     for _ in range(steps):
@@ -186,15 +190,15 @@ def run_reference(args, rank):
         return
     threads = os.cpu_count() or 1
     steps = max(1, args.steps)
-    gbps, t = cpu_baseline_run(args.cpu_sample_bytes, args.chunk_size, steps, threads, args.workload)
+    gbps, t = cpu_baseline_run(args.cpu_sample_bytes, args.chunk_size, steps, threads, args.workload, args.approach)
     sample = (f"{args.cpu_sample_bytes >> 20} MiB buffer with the {args.workload} workload's change pattern, "
               f"chunk {args.chunk_size} B, {steps} incremental checkpoints after an untimed baseline")
     line = {
-        "impl": "reference", "metric": "tree-dedup ingest GB/s", "value": round(gbps, 4), "unit": "GB/s",
+        "impl": "reference", "metric": f"{args.approach}-dedup ingest GB/s", "value": round(gbps, 4), "unit": "GB/s",
         "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "ms_per_step": round(1e3 * t / steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
         "config": {"workload": args.workload, "nbytes": args.nbytes, "chunk_size": args.chunk_size,
-                   "hash": "md5" if args.workload == "md5_f32_8g" else "murmur3"},
+                   "hash": "md5" if args.workload == "md5_f32_8g" else "murmur3", "approach": args.approach},
         "cpu_baseline": {"value": round(gbps, 4), "unit": "GB/s", "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": round(gbps, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -468,6 +472,8 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank)
         return
+    if args.form != "plain" and args.approach != "tree":
+        raise SystemExit("--approach list runs the plain form only")
     if args.form != "plain":
         import torch
         import torch.distributed as dist
@@ -489,8 +495,8 @@ def main():
     import torch
     import torch.distributed as dist
 
-    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import (HASH_MD5, HASH_MURMUR3, TreeDeduplicator,
-                                                                        replicas, synth)
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import (HASH_MD5, HASH_MURMUR3, ListDeduplicator,
+                                                                        TreeDeduplicator, replicas, synth)
     from reproducibility_icpp23_scalable_gpu_deduplication_b200.tree import parse_header
 
     torch.cuda.set_device(local)
@@ -505,7 +511,8 @@ def main():
 
     md5 = args.workload == "md5_f32_8g"
     series = workload_series(args.workload, nbytes, cs, dev, synth.SEED + rank)
-    dd = TreeDeduplicator(cs, HASH_MD5 if md5 else HASH_MURMUR3)
+    Dedup = ListDeduplicator if args.approach == "list" else TreeDeduplicator
+    dd = Dedup(cs, HASH_MD5 if md5 else HASH_MURMUR3)
     if args.leaf_stages:
         dd.set_param("leaf_stages", args.leaf_stages)
     if args.leaf_ctas:
@@ -591,7 +598,7 @@ def main():
     restart = None
     if not args.no_restart:
         rs = workload_series(args.workload, nbytes, cs, dev, synth.SEED + rank + 17)
-        rd = TreeDeduplicator(cs, HASH_MD5 if md5 else HASH_MURMUR3)
+        rd = Dedup(cs, HASH_MD5 if md5 else HASH_MURMUR3)
         diffs = []
         for k in range(4):
             x = rs.next()
@@ -649,12 +656,12 @@ def main():
                 "step_frac": round(((nbytes + 32 * n_chunks + statistics.mean(diff_bytes)) /
                                     (ms_max * 1e-3 / args.steps) / GB) / peak, 4)}
     line = {
-        "metric": "tree-dedup ingest GB/s", "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
+        "metric": f"{args.approach}-dedup ingest GB/s", "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic (seeded; reference datasets unavailable)",
         "config": {"workload": args.workload, "nbytes": nbytes, "chunk_size": cs, "hash": "md5" if md5 else "murmur3",
-                   "checkpoints": 1 + args.warmup + args.steps,
+                   "approach": args.approach, "checkpoints": 1 + args.warmup + args.steps,
                    "l2": (f"inputs {nbytes / 2**30:.2f} GiB > L2, no flush" if nbytes >= (256 << 20) else
                           "L2 flushed (512 MiB write) before each step, outside the timed spans"),
                    "parallelism": f"replicas x{world}"},
@@ -670,7 +677,7 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        gbps, _ = cpu_baseline_run(args.cpu_sample_bytes, cs, 2, threads, args.workload)
+        gbps, _ = cpu_baseline_run(args.cpu_sample_bytes, cs, 2, threads, args.workload, args.approach)
         line["cpu_baseline"] = {"value": round(gbps, 4), "unit": "GB/s", "cores": threads, "kind": "port",
                                 "sample": f"{args.cpu_sample_bytes >> 20} MiB buffer with this workload's change "
                                           f"pattern, 2 incremental checkpoints after a baseline"}

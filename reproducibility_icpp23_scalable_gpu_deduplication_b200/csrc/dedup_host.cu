@@ -784,10 +784,12 @@ int do_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* di
       B2D_CU(cudaMemcpy(hdr, ddiffs[idx], 32, cudaMemcpyDeviceToHost));
       HostHdr hh;
       if (!parse_hdr(hdr, sizes[idx], hh)) return B2D_ERR_FORMAT;
+      // header, then the repeat table right behind it (not at its offset in the diff: the
+      // first-occurrence list in between can be tens of megabytes)
       auto& m = hmeta[idx];
-      m.assign(hh.count_off + 8ull * hh.P, 0);
+      m.resize(32 + 8ull * hh.P);
       std::memcpy(m.data(), hdr, 32);
-      if (hh.P) B2D_CU(cudaMemcpy(m.data() + hh.count_off, static_cast<const uint8_t*>(ddiffs[idx]) + hh.count_off,
+      if (hh.P) B2D_CU(cudaMemcpy(m.data() + 32, static_cast<const uint8_t*>(ddiffs[idx]) + hh.count_off,
                                   8ull * hh.P, cudaMemcpyDeviceToHost));
       hptr[idx] = m.data();
       if (idx - 1 < (int)hh.ref_id) break;
@@ -914,10 +916,11 @@ int do_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* di
     }
     std::vector<unsigned long long> cum(ncum, 0ull);
     bool bad_row = false;
+    const uint8_t* ctab = ddiffs ? diffs[idx] + 32 : diffs[idx] + hh.count_off;   // repeat table on the host
     for (uint32_t i = 0; i < hh.P; i++) {
       uint32_t ck, cnt;
-      memcpy(&ck, diffs[idx] + hh.count_off + 8ull * i, 4);
-      memcpy(&cnt, diffs[idx] + hh.count_off + 8ull * i + 4, 4);
+      memcpy(&ck, ctab + 8ull * i, 4);
+      memcpy(&cnt, ctab + 8ull * i + 4, 4);
       if (ck < ncum) cum[ck] = cnt; else bad_row = true;
     }
     for (uint64_t t = 1; t < ncum; t++) cum[t] += cum[t - 1];

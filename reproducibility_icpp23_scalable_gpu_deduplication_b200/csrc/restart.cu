@@ -225,8 +225,8 @@ __global__ void __launch_bounds__(R_THREADS) r_write_kernel(RestartArgs a, int w
   }
 }
 
-__device__ __forceinline__ uint32_t find_entry(const uint32_t* off, uint32_t cnt, uint64_t k) {
-  uint32_t lo = 0, hi = cnt;
+// largest i in [lo, hi) with off[i] <= k (off[lo] <= k)
+__device__ __forceinline__ uint32_t find_entry(const uint32_t* off, uint32_t lo, uint32_t hi, uint64_t k) {
   while (hi - lo > 1) {
     const uint32_t mid = (lo + hi) >> 1;
     if (off[mid] <= k) lo = mid; else hi = mid;
@@ -234,25 +234,62 @@ __device__ __forceinline__ uint32_t find_entry(const uint32_t* off, uint32_t cnt
   return lo;
 }
 
+// Region-list expansion: warp w takes one contiguous range of expanded positions k, in windows
+// of 32 (lane i takes k = base + i).  The entry of the range's first k is searched once; the 32
+// positions of a window lie in at most the 32 entries from the previous window's last one (every
+// entry covers at least one position), so each lane then searches only those -- one cache line
+// for the whole warp.  A list diff, whose entries are single chunks, would otherwise pay a search
+// over millions of entries per chunk.
+// With a.id_bias (list diffs) every entry is one chunk: position k is entry k, no search.
+#define R_EXPAND_LOOP(base, count, off, cnt)                                                      \
+  const uint32_t lane = threadIdx.x & 31u;                                                        \
+  const uint64_t w0_ = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;                    \
+  const uint64_t nw_ = ((uint64_t)gridDim.x * blockDim.x) >> 5;                                   \
+  const uint64_t per_ = ((count) + nw_ * 32u - 1u) / (nw_ * 32u) * 32u;                           \
+  const uint64_t beg_ = w0_ * per_;                                                               \
+  const uint64_t end_ = beg_ + per_ < (count) ? beg_ + per_ : (count);                            \
+  uint32_t ib_ = (!a.id_bias && beg_ < end_) ? find_entry((off), 0u, (cnt), beg_) : 0u;          \
+  for (uint64_t base = beg_; base < end_; base += 32u)
+
+// entry of position k of the current window, whose first position lies in entry ib; an entry
+// covering no position (only a malformed diff has one) sends the search past the window
+__device__ __forceinline__ uint32_t window_entry(const uint32_t* off, uint32_t ib, uint32_t cnt, uint64_t k) {
+  const uint32_t hi = ib + 32u < cnt ? ib + 32u : cnt;
+  uint32_t i = find_entry(off, ib, hi, k);
+  if (i + 1u == hi && hi < cnt && off[hi] <= k) i = find_entry(off, hi, cnt, k);
+  return i;
+}
+#define R_WINDOW_ENTRY(off, cnt, k) window_entry((off), ib_, (cnt), (k))
+
 // first-occurrence regions: dist for every leaf; the main diff also fills node_list and copies
 // the chunk (:822-865 main, :1005-1030 older)
 __global__ void __launch_bounds__(R_THREADS, B2D_RESTART_MINB) r_expand_first_kernel(RestartArgs a) {
-  const uint64_t T = *a.total;
+  const uint64_t T = a.id_bias ? (uint64_t)a.F : *a.total;
   const uint8_t* data = a.diff + a.data_off;
   const uint64_t data_len = a.diff_size - a.data_off;
-  R_WARP_LOOP(kb, T) {
+  R_EXPAND_LOOP(kb, T, a.offs, a.F) {
     const uint64_t k = kb + lane;
     uint64_t dst = 0, nb = 0;
     const uint8_t* src = nullptr;
-    if (k < T) {
-      const uint32_t i = find_entry(a.offs, a.F, k);
-      const uint32_t start = a.rstart[i];
-      const uint32_t j = (uint32_t)(k - a.offs[i]);
+    uint32_t i = ib_;
+    if (k < end_) {
+      uint32_t start, j, off0;
+      if (a.id_bias) {   // one chunk per entry, at data offset k (src/list_approach.cpp:331-351)
+        i = (uint32_t)k;
+        start = rd_node(a, a.diff + a.first_off + 4ull * k);
+        j = 0;
+        off0 = (uint32_t)k;
+      } else {
+        i = R_WINDOW_ENTRY(a.offs, a.F, k);
+        start = a.rstart[i];
+        off0 = a.offs[i];
+        j = (uint32_t)(k - off0);
+      }
       const uint64_t c = (uint64_t)start - (a.n - 1u) + j;
       if (start < a.n - 1u || c >= a.n) {
         set_error(a.st, DERR_RESTART_RANGE, 2);
       } else {
-        const uint32_t off = a.offs[i] + j;   // u32 like the reference (:846, :1018)
+        const uint32_t off = off0 + j;   // u32 like the reference (:846, :1018)
         a.slot.dist[c] = off;
         a.slot.flag[c] = R_HAS_DIST;   // the diff's first writer of this flag
         if (a.is_main) {
@@ -265,6 +302,7 @@ __global__ void __launch_bounds__(R_THREADS, B2D_RESTART_MINB) r_expand_first_ke
       }
     }
     if (a.is_main) warp_copy(a.out, a.cs, a.width, a.per, a.per_log2, dst, src, nb);
+    ib_ = __shfl_sync(R_FULL, i, 31);
   }
 }
 
@@ -329,19 +367,29 @@ __global__ void r_straddle_kernel(RestartArgs a, const StraddleInfo* sd) {
 
 // shifted-duplicate entries (:888-927 main, :1049-1075 older)
 __global__ void __launch_bounds__(R_THREADS, B2D_RESTART_MINB) r_expand_shift_kernel(RestartArgs a) {
-  const uint64_t T = *a.total;
+  const uint64_t T = a.id_bias ? (uint64_t)a.S : *a.total;
   const uint8_t* data = a.diff + a.data_off;
   const uint64_t data_len = a.diff_size - a.data_off;
-  R_WARP_LOOP(kb, T) {
+  R_EXPAND_LOOP(kb, T, a.offs, a.S) {
     const uint64_t k = kb + lane;
     uint64_t dst = 0, nb = 0;
     const uint8_t* src = nullptr;
-    if (k < T) {
-      const uint32_t i = find_entry(a.offs, a.S, k);
-      const uint32_t j = (uint32_t)(k - a.offs[i]);
-      const uint32_t node_start = a.rstart[i];
-      const uint32_t prev_start = a.pstart[i];
-      const uint32_t tree = a.rtree[i];
+    uint32_t i = ib_;
+    if (k < end_) {
+      uint32_t j, node_start, prev_start, tree;
+      if (a.id_bias) {   // one chunk per entry (src/list_approach.cpp:371-408, :501-513)
+        i = (uint32_t)k;
+        j = 0;
+        node_start = rd_node(a, a.diff + a.shift_off + 8ull * k);
+        prev_start = rd_node(a, a.diff + a.shift_off + 8ull * k + 4);
+        tree = shift_tree(a, k);
+      } else {
+        i = R_WINDOW_ENTRY(a.offs, a.S, k);
+        j = (uint32_t)(k - a.offs[i]);
+        node_start = a.rstart[i];
+        prev_start = a.pstart[i];
+        tree = a.rtree[i];
+      }
       const uint64_t c = (uint64_t)node_start + j - (a.n - 1u);
       if (node_start < a.n - 1u || c >= a.n) {
         set_error(a.st, DERR_RESTART_RANGE, 3);
@@ -364,6 +412,7 @@ __global__ void __launch_bounds__(R_THREADS, B2D_RESTART_MINB) r_expand_shift_ke
       }
     }
     if (a.is_main) warp_copy(a.out, a.cs, a.width, a.per, a.per_log2, dst, src, nb);
+    ib_ = __shfl_sync(R_FULL, i, 31);
   }
 }
 
@@ -490,7 +539,7 @@ static void copy_width(uint64_t dst_al, uint64_t src_al, uint32_t cs, uint32_t& 
   if (per && (per & (per - 1u)) == 0) per_log2 = (uint32_t)__builtin_ctz(per);
 }
 
-int restart_diff_launches(uint32_t n, bool list) { return 8 + (!list && straddle_query(n).count ? 2 : 0); }
+int restart_diff_launches(uint32_t n, bool list) { return list ? 2 : 8 + (straddle_query(n).count ? 2 : 0); }
 
 cudaError_t launch_restart_diff(const RestartArgs& args, StraddleInfo* sd, int sm_count, cudaStream_t s) {
   RestartArgs a = args;
@@ -500,10 +549,13 @@ cudaError_t launch_restart_diff(const RestartArgs& args, StraddleInfo* sd, int s
   if (e == cudaSuccess && a.is_main) e = cudaMemsetAsync(a.mflag, 0, a.n, s);
   if (e != cudaSuccess) return e;
   const uint32_t g = SCAN_GRID;
+  const bool scan = !a.id_bias;   // list entries are single chunks: offsets are the entry indices
   // first-occurrence regions
-  r_count_kernel<<<g, R_THREADS, 0, s>>>(a, 0);
-  r_scan_kernel<<<1, 1024, 0, s>>>(a, g);
-  r_write_kernel<<<g, R_THREADS, 0, s>>>(a, 0);
+  if (scan) {
+    r_count_kernel<<<g, R_THREADS, 0, s>>>(a, 0);
+    r_scan_kernel<<<1, 1024, 0, s>>>(a, g);
+    r_write_kernel<<<g, R_THREADS, 0, s>>>(a, 0);
+  }
   r_expand_first_kernel<<<grid_for(a.n, sm_count), R_THREADS, 0, s>>>(a);
   const StraddleQuery q = a.id_bias ? StraddleQuery{} : straddle_query(a.n);   // list regions are single leaves
   if (q.count) {
@@ -513,9 +565,11 @@ cudaError_t launch_restart_diff(const RestartArgs& args, StraddleInfo* sd, int s
     r_straddle_kernel<<<(uint32_t)sm_count * 4u, R_THREADS, 0, s>>>(a, sd);
   }
   // shifted duplicates
-  r_count_kernel<<<g, R_THREADS, 0, s>>>(a, 1);
-  r_scan_kernel<<<1, 1024, 0, s>>>(a, g);
-  r_write_kernel<<<g, R_THREADS, 0, s>>>(a, 1);
+  if (scan) {
+    r_count_kernel<<<g, R_THREADS, 0, s>>>(a, 1);
+    r_scan_kernel<<<1, 1024, 0, s>>>(a, g);
+    r_write_kernel<<<g, R_THREADS, 0, s>>>(a, 1);
+  }
   r_expand_shift_kernel<<<grid_for(a.n, sm_count), R_THREADS, 0, s>>>(a);
   return cudaGetLastError();
 }
