@@ -118,3 +118,9 @@ def test_list_not_in_batches(cuda):
     with pytest.raises(B2DError):
         CheckpointBatch().checkpoint([g], [x], [True])
     g.close()
+
+
+def test_list_long_chain_restart_windows(cuda):
+    """13 list checkpoints: device-diff restarts cross two walk windows"""
+    s = synth.ByteSeries(512 * 1024 + 64, 128, synth.plan_plain_64m, 1, 92)
+    run_both([s.next().copy() for _ in range(13)], 128)

@@ -214,3 +214,10 @@ def test_narrow_staging_units(cuda, unit):
     s = synth.plain_64m(nbytes=8 << 20)
     bufs = [s.next().copy() for _ in range(3)]
     run_both(bufs, 128, params={"leaf_unit": unit})
+
+
+def test_long_chain_restart_windows(cuda):
+    """a 13-checkpoint chain: restarts from device diffs walk the 12 older diffs in two windows
+    (8 + 4) with the NodeIDs carried between them; every checkpoint restarts like the oracle"""
+    s = synth.ByteSeries(512 * 1024 + 64, 128, synth.plan_plain_64m, 1, 91)
+    run_both([s.next().copy() for _ in range(13)], 128)
