@@ -101,6 +101,12 @@ int b2d_copy_diff(b2d_dedup* d, void* dst, uint64_t cap);
  * point.  For callers that overlap the copy-back with other checkpoints.  No reference
  * counterpart. */
 int b2d_copy_diff_async(b2d_dedup* d, void* dst, uint64_t cap, void* cuda_stream);
+/* The three CSV logs of the last checkpoint, as checkpoint(.., logname, ..) writes them
+ * (write_chkpt_log, src/tree_approach.cpp:1853-1896 with src/utils.cpp:38-124; "List" rows for
+ * a list handle), for a checkpoint taken with b2d_checkpoint_device whose diff is copied back
+ * asynchronously: its Write Time column is 0, the copy-back being the caller's.  The checkpoint
+ * id written is the diff's.  Reads only the diff's header and repeat table from the device. */
+int b2d_write_chkpt_log(b2d_dedup* d, const char* logname);
 
 /* checkpoint(uint8_t* data_ptr, size_t len, HostMirror& diff_h, bool make_baseline)
  * -- src/tree_approach.cpp:1740-1748.  *diff points at pinned host memory owned by the handle,

@@ -670,8 +670,8 @@ int checkpoint_to_pinned(b2d_dedup* d, const void* d_data, uint64_t len, bool ma
 
 // write_chkpt_log (:1853-1896) with write_metadata_breakdown (src/utils.cpp:38-124); the
 // checkpoint id written is the one just taken (logs are written before current_id += 1)
-int write_chkpt_log(b2d_dedup* d, const uint8_t* diff, uint64_t diff_len, const std::string& logname, uint32_t id) {
-  if (diff_len < 32) return B2D_ERR_FORMAT;
+// `diff` holds at least the 32-byte header; `ctab` the repeat table ((ckpt, count) rows)
+int write_chkpt_log(b2d_dedup* d, const uint8_t* diff, const uint8_t* ctab, const std::string& logname, uint32_t id) {
   const std::string base = logname + ".chunk_size." + std::to_string(d->chunk_size);
   FILE* result = fopen((base + ".csv").c_str(), "a");
   FILE* size = fopen((base + ".size.csv").c_str(), "a");
@@ -712,8 +712,7 @@ int write_chkpt_log(b2d_dedup* d, const uint8_t* diff, uint64_t diff_len, const 
     for (uint32_t i = 0; i < id; i++) {
       if (i < np) {
         uint32_t num = 0;
-        const uint64_t off = 32 + 4ull * nf + 8ull * i + 4;
-        if (off + 4 <= diff_len) memcpy(&num, diff + off, 4);
+        memcpy(&num, ctab + 8ull * i + 4, 4);
         fprintf(size, ",%llu", 8ull * num);
       } else {
         fprintf(size, ",0");
@@ -1695,6 +1694,29 @@ int b2d_copy_diff_async(b2d_dedup* d, void* dst, uint64_t cap, void* stream) {
   return B2D_OK;
 }
 
+int b2d_write_chkpt_log(b2d_dedup* d, const char* logname) {
+  B2D_GUARD({
+    if (!d || !logname || !d->diff_valid) return B2D_ERR_ARG;
+    // header and repeat table of the device diff (the first-occurrence list between them stays)
+    const uint8_t* dd = d->diff.p + d->diff_delta;
+    uint8_t hdr[32];
+    B2D_CU(cudaMemcpyAsync(hdr, dd, 32, cudaMemcpyDeviceToHost, d->stream));
+    B2D_CU(cudaStreamSynchronize(d->stream));
+    uint32_t nf = 0;
+    uint32_t np = 0;
+    memcpy(&nf, hdr + 20, 4);
+    memcpy(&np, hdr + 24, 4);
+    std::vector<uint8_t> ctab(8ull * np + 8);
+    if (np) {
+      B2D_CU(cudaMemcpyAsync(ctab.data(), dd + 32 + 4ull * nf, 8ull * np, cudaMemcpyDeviceToHost, d->stream));
+      B2D_CU(cudaStreamSynchronize(d->stream));
+    }
+    uint32_t id = 0;
+    memcpy(&id, hdr + 4, 4);   // chkpt_id of the diff
+    return write_chkpt_log(d, hdr, ctab.data(), logname, id);
+  })
+}
+
 int b2d_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, int make_baseline, const uint8_t** diff,
                    uint64_t* diff_len) {
   B2D_GUARD({
@@ -1711,7 +1733,8 @@ int b2d_checkpoint_log(b2d_dedup* d, const void* d_data, uint64_t len, const cha
     uint64_t n = 0;
     int rc = checkpoint_to_pinned(d, d_data, len, make_baseline != 0, false, &p, &n);
     if (rc) return rc;
-    rc = write_chkpt_log(d, p, n, logname, d->current_id);
+    if (n < 32) return B2D_ERR_FORMAT;
+    rc = write_chkpt_log(d, p, p + 32 + 4ull * d->F, logname, d->current_id);
     d->current_id += 1;
     if (diff) *diff = p;
     if (diff_len) *diff_len = n;
@@ -1727,7 +1750,8 @@ int b2d_checkpoint_file(b2d_dedup* d, const void* d_data, uint64_t len, const ch
     uint64_t n = 0;
     int rc = checkpoint_to_pinned(d, d_data, len, make_baseline != 0, false, &p, &n);
     if (rc) return rc;
-    rc = write_chkpt_log(d, p, n, logname, d->current_id);
+    if (n < 32) return B2D_ERR_FORMAT;
+    rc = write_chkpt_log(d, p, p + 32 + 4ull * d->F, logname, d->current_id);
     if (rc) return rc;
     FILE* f = fopen(filename, "wb");
     if (!f) return B2D_ERR_IO;
