@@ -527,6 +527,7 @@ ForestArgs forest_args(b2d_dedup* d, const RoundState* rs_dev) {
 int enqueue_checkpoint(b2d_dedup* d, cudaStream_t s, RoundState* rs_dev, bool upload, bool timing, bool skip_leaves,
                        bool managed = false, bool skip_diff = false, bool skip_forest = false) {
   DevState* ds = d->state.p;
+  bool zero_probe_skipped = false;
   if (!managed) {
     B2D_CU(cudaMemsetAsync(ds, 0, sizeof(DevState), s));
     if (upload) B2D_CU(cudaMemcpyAsync(rs_dev, d->round_h.p, sizeof(RoundState), cudaMemcpyHostToDevice, s));
@@ -546,7 +547,10 @@ int enqueue_checkpoint(b2d_dedup* d, cudaStream_t s, RoundState* rs_dev, bool up
   } else if (!skip_forest) {
     const ForestArgs fa = forest_args(d, rs_dev);
     B2D_CU(launch_forest(fa, 1, s));
-    B2D_CU(launch_zero_exists(&ds->zero_exists, rs_dev, s));
+    // the zero-digest probe matters to baselines only; launches issued one by one for a single
+    // handle skip it otherwise (a captured graph or a batch keeps it: it serves both kinds)
+    if (managed || d->use_graph || d->round_h.p->baseline) B2D_CU(launch_zero_exists(&ds->zero_exists, rs_dev, s));
+    else zero_probe_skipped = true;
     B2D_CU(launch_forest(fa, 2, s));
   }
   if (timing) B2D_CU(record_timing(d->ev[1], s));
@@ -564,7 +568,8 @@ int enqueue_checkpoint(b2d_dedup* d, cudaStream_t s, RoundState* rs_dev, bool up
     d->launches = (skip_leaves ? 0 : 1) + 1 + (skip_diff ? 0 : 12);
   else
     d->launches = (skip_leaves ? 0 : 1) +
-                  (skip_forest ? 0 : forest_launch_count(d->D, 1) + forest_launch_count(d->D, 2) + 1) +
+                  (skip_forest ? 0 : forest_launch_count(d->D, 1) + forest_launch_count(d->D, 2) +
+                                         (zero_probe_skipped ? 0 : 1)) +
                   (skip_diff ? 0 : 14);
   return B2D_OK;
 }
