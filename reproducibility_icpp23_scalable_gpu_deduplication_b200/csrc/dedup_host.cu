@@ -546,12 +546,12 @@ int enqueue_checkpoint(b2d_dedup* d, cudaStream_t s, RoundState* rs_dev, bool up
     B2D_CU(launch_list_label(forest_args(d, rs_dev), d->sm_count, s));
   } else if (!skip_forest) {
     const ForestArgs fa = forest_args(d, rs_dev);
-    B2D_CU(launch_forest(fa, 1, s));
+    B2D_CU(launch_forest(fa, 1, s, d->sm_count));
     // the zero-digest probe matters to baselines only; launches issued one by one for a single
     // handle skip it otherwise (a captured graph or a batch keeps it: it serves both kinds)
     if (managed || d->use_graph || d->round_h.p->baseline) B2D_CU(launch_zero_exists(&ds->zero_exists, rs_dev, s));
     else zero_probe_skipped = true;
-    B2D_CU(launch_forest(fa, 2, s));
+    B2D_CU(launch_forest(fa, 2, s, d->sm_count));
   }
   if (timing) B2D_CU(record_timing(d->ev[1], s));
   // collect_diff (:511-710; list approach src/list_approach.cpp:79-257, single-chunk regions in

@@ -144,7 +144,8 @@ int batch_leaf_item(const LeafArgs& a, BatchLeafItem& item);
 cudaError_t launch_leaves_batch(const BatchLeafItem* d_items, uint32_t nitems, uint32_t total_tiles, int U, int kind,
                                 unsigned int* queue, DevStatus* st, int sm_count, const LeafTuning& tune,
                                 uint32_t tiles_per_pop, cudaStream_t stream);
-cudaError_t launch_forest(const ForestArgs& a, int phase, cudaStream_t stream);
+// sm_count > 0: the first band runs on a resident grid (see forest.cu)
+cudaError_t launch_forest(const ForestArgs& a, int phase, cudaStream_t stream, int sm_count = 0);
 
 // CTA b of a segmented launch belongs to the handle h with beg[h] <= b < beg[h+1]
 __device__ __forceinline__ uint32_t seg_find(const uint32_t* beg, uint32_t n, uint32_t& bid, uint32_t& nb) {

@@ -350,8 +350,20 @@ __device__ __forceinline__ void forest_first_body(const ForestArgs& a, uint32_t 
     insert_first_parent(a, x, a.tree[x]);
   }
 }
-__global__ void __launch_bounds__(FAST_THREADS, B2D_FF_MINB) forest_first_kernel(ForestArgs a0, uint32_t in) {
-  forest_first_body(with_round(a0), blockIdx.x, in);
+// The first band of a phase has one band per 1024 (phase 1) or 4096 (phase 2) leaves, most of
+// them without work at low change rates.  With B2D_FOREST_PERSIST the launch is one resident
+// grid whose CTAs take bands in turn (a barrier between bands: shared memory is reused), so
+// tens of thousands of short-lived CTAs are not scheduled one by one.
+#ifndef B2D_FOREST_PERSIST
+#define B2D_FOREST_PERSIST 1
+#endif
+__global__ void __launch_bounds__(FAST_THREADS, B2D_FF_MINB) forest_first_kernel(ForestArgs a0, uint32_t in,
+                                                                                  uint32_t nbands) {
+  const ForestArgs a = with_round(a0);
+  for (uint32_t bid = blockIdx.x; bid < nbands; bid += gridDim.x) {
+    forest_first_body(a, bid, in);
+    __syncthreads();
+  }
 }
 __global__ void __launch_bounds__(FAST_THREADS, B2D_FF_MINB) forest_first_seg(ForestSeg s) {
   uint32_t bid, nb;
@@ -445,8 +457,13 @@ __device__ __forceinline__ void forest_fast_body(const ForestArgs& a, uint32_t b
   }
 }
 template <int PHASE>
-__global__ void __launch_bounds__(FAST_THREADS, B2D_FAST_MINB) forest_fast_kernel(ForestArgs a0, uint32_t in) {
-  forest_fast_body<PHASE>(with_round(a0), blockIdx.x, in);
+__global__ void __launch_bounds__(FAST_THREADS, B2D_FAST_MINB) forest_fast_kernel(ForestArgs a0, uint32_t in,
+                                                                                  uint32_t nbands) {
+  const ForestArgs a = with_round(a0);
+  for (uint32_t bid = blockIdx.x; bid < nbands; bid += gridDim.x) {
+    forest_fast_body<PHASE>(a, bid, in);
+    __syncthreads();
+  }
 }
 template <int PHASE>
 __global__ void __launch_bounds__(FAST_THREADS, B2D_FAST_MINB) forest_fast_seg(ForestSeg s) {
@@ -521,13 +538,29 @@ void forest_steps(uint32_t D, uint64_t N, int phase, std::vector<ForestStep>& ou
   }
 }
 
-cudaError_t launch_forest(const ForestArgs& a, int phase, cudaStream_t stream) {
+// resident CTAs per SM of a first-band kernel (queried once)
+template <class K>
+static uint32_t resident_ctas(K kernel) {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, FAST_THREADS, 0) != cudaSuccess || nb < 1) {
+    (void)cudaGetLastError();
+    nb = 1;
+  }
+  return (uint32_t)nb;
+}
+
+cudaError_t launch_forest(const ForestArgs& a, int phase, cudaStream_t stream, int sm_count) {
+  static const uint32_t res_first = resident_ctas(forest_first_kernel);
+  static const uint32_t res_fast = resident_ctas(forest_fast_kernel<2>);
   std::vector<ForestStep> steps;
   forest_steps(a.D, a.N, phase, steps);
   for (const ForestStep& st : steps) {
     if (st.kind == 0) {
-      if (phase == 1) forest_first_kernel<<<st.ctas, FAST_THREADS, 0, stream>>>(a, st.p0);
-      else forest_fast_kernel<2><<<st.ctas, FAST_THREADS, 0, stream>>>(a, st.p0);
+      uint32_t grid = st.ctas;
+      const uint32_t cap = (phase == 1 ? res_first : res_fast) * (uint32_t)(sm_count > 0 ? sm_count : 0);
+      if (B2D_FOREST_PERSIST && cap && grid > cap) grid = cap;
+      if (phase == 1) forest_first_kernel<<<grid, FAST_THREADS, 0, stream>>>(a, st.p0, st.ctas);
+      else forest_fast_kernel<2><<<grid, FAST_THREADS, 0, stream>>>(a, st.p0, st.ctas);
     } else {
       if (phase == 1) forest_band_kernel<1><<<st.ctas, FOREST_THREADS, 0, stream>>>(a, st.p0, st.p1);
       else forest_band_kernel<2><<<st.ctas, FOREST_THREADS, 0, stream>>>(a, st.p0, st.p1);
