@@ -73,7 +73,7 @@ def parse():
     p.add_argument("--rate", type=float, default=200.0, help="served form: aggregate arrivals per second")
     p.add_argument("--client-max-buffer", type=int, default=2 << 30, help="served form: largest client buffer")
     p.add_argument("--map-reserve", type=float, default=20e9,
-                   help="served form: device bytes kept mapped for digest-map growth")
+                   help="served and batched forms: device bytes kept mapped for digest-map growth")
     p.add_argument("--hbm-budget", type=float, default=150e9, help="served form: device bytes for client state")
     a = p.parse_args()
     md5 = a.workload == "md5_f32_8g"
@@ -218,6 +218,7 @@ def run_batched(args, rank, world, dev):
     import torch
 
     from reproducibility_icpp23_scalable_gpu_deduplication_b200 import CheckpointBatch, TreeDeduplicator, replicas, synth
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200.tree import reserve_map_memory
 
     sizes = synth.batched_sizes(count=args.buffers, hi=args.max_buffer)
     total = sum(sizes)
@@ -230,6 +231,7 @@ def run_batched(args, rank, world, dev):
         ss = batched_series(sizes, dev, seed)
         hs = [TreeDeduplicator(128) for _ in sizes]
         times, sums, launches = [], [], 0
+        grows0 = 0
         for c in range(ckpts):
             bufs = [s.next() for s in ss]
             torch.cuda.synchronize()
@@ -246,11 +248,18 @@ def run_batched(args, rank, world, dev):
                 times.append(e0.elapsed_time(e1))
                 launches += nl
             sums.append([h.diff_checksum() for h in hs])
+            if c == args.warmup:
+                # the maps' baselines are in place: keep device memory mapped for their growth
+                # (as a long-running service does), and count the growths of the timed steps
+                if args.map_reserve > 0:
+                    reserve_map_memory(int(args.map_reserve))
+                grows0 = sum(h.map_stats()[2] for h in hs)
+        grows = sum(h.map_stats()[2] for h in hs) - grows0
         for h in hs:
             h.close()
         del ss, bufs
         torch.cuda.empty_cache()
-        return times, sums, launches
+        return times, sums, launches, grows
 
     def plain_step(hs, bufs, base):
         n = 0
@@ -280,8 +289,9 @@ def run_batched(args, rank, world, dev):
         return batch.launch_count()
 
     with ClockSampler(int(dev.index or 0)) as clk:
-        t_plain, s_plain, l_plain = series_pass(plain_step) if not args.no_plain else ([float("nan")], None, 0)
-        t_batch, s_batch, l_batch = series_pass(batch_step)
+        t_plain, s_plain, l_plain, g_plain = (series_pass(plain_step) if not args.no_plain
+                                              else ([float("nan")], None, 0, 0))
+        t_batch, s_batch, l_batch, g_batch = series_pass(batch_step)
     same = s_plain == s_batch or args.no_plain
     ms_b, ms_p = statistics.mean(t_batch), statistics.mean(t_plain)
     rate_b, ms_b = replicas.throughput(ms_b, total, dev)
@@ -302,6 +312,8 @@ def run_batched(args, rank, world, dev):
         "plain_same_workload": None if args.no_plain else {
             "value": round(plain, 2), "unit": "GB/s", "ms_per_step": round(ms_p, 4), "gpu_launches": l_plain},
         "speedup_vs_plain": None if args.no_plain else round(value / plain, 3),
+        "map_growth": {"reserved_bytes": int(args.map_reserve), "grows_in_timed_steps": {"batched": g_batch,
+                                                                                        "one_at_a_time": g_plain}},
         "parity": ("not compared (--no-plain)" if args.no_plain else ("identical" if same else "MISMATCH") +
                    f": diff checksums of {len(sizes)} buffers x {ckpts} checkpoints, batched vs one at a time"),
         "e2e": None,
