@@ -564,13 +564,15 @@ int enqueue_checkpoint(b2d_dedup* d, cudaStream_t s, RoundState* rs_dev, bool up
   }
   if (timing) B2D_CU(record_timing(d->ev[2], s));
   if (!managed) B2D_CU(cudaMemcpyAsync(d->state_h.p, d->state.p, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+  // kernels only (memsets and copies are not counted): the diff assembly is 12 kernels, 10 in
+  // node order (no level reordering)
   if (d->list)
-    d->launches = (skip_leaves ? 0 : 1) + 1 + (skip_diff ? 0 : 12);
+    d->launches = (skip_leaves ? 0 : 1) + 1 + (skip_diff ? 0 : 10);
   else
     d->launches = (skip_leaves ? 0 : 1) +
                   (skip_forest ? 0 : forest_launch_count(d->D, 1) + forest_launch_count(d->D, 2) +
                                          (zero_probe_skipped ? 0 : 1)) +
-                  (skip_diff ? 0 : 14);
+                  (skip_diff ? 0 : 12);
   return B2D_OK;
 }
 
