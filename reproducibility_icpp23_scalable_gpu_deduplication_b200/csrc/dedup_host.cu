@@ -471,7 +471,7 @@ int prepare_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, bool make
   B2D_CU(d->hist.reserve(bcap));
   B2D_CU(d->bucket_start.reserve(bcap));
   B2D_CU(d->partial.reserve((size_t)1184 * bcap));
-  B2D_CU(d->partial2.reserve(2 * SCAN_GRID));
+  B2D_CU(d->partial2.reserve(2 * COMPACT_GRID));
   B2D_CU(d->diff.reserve(64 + 16ull * d->n + (uint64_t)d->n * d->chunk_size));
   B2D_CU(d->state.reserve(1));
   B2D_CU(d->state_h.reserve(1));
@@ -1967,7 +1967,7 @@ int b2d_estimate_memory(uint64_t len, uint32_t chunk_size, int map_max_load_pct,
   uint64_t b = N * sizeof(Digest) + N + (n + 16) + ((N + 15) / 16 * 16 + 16) + n;   // tree, labels, flags
   b += (cap + 1) * sizeof(MapSlot) + 8;                                              // map
   b += 8 * 4 * n + 68 * 4;                                                           // lists and keys
-  b += (uint64_t)64 * 4 * 2 + (uint64_t)1184 * 64 * 4 + 2 * SCAN_GRID * 4;           // buckets, partials
+  b += (uint64_t)64 * 4 * 2 + (uint64_t)1184 * 64 * 4 + 2 * COMPACT_GRID * 4;           // buckets, partials
   b += 64 + 16 * n + n * chunk_size;                                                 // diff
   b += sizeof(DevState);
   *bytes = b;

@@ -12,6 +12,13 @@ namespace b2d {
 constexpr uint32_t TMA_CONSUMER_WARPS = 8;   // 256 chunks per TMA tile
 constexpr uint32_t FOREST_BAND_LEVELS = 12;  // levels fused per forest band launch (4096-leaf subtrees)
 constexpr uint32_t SCAN_GRID = 296;          // fixed grid of the reduce-then-scan passes (2 x 148 SMs)
+// largest grid of the diff assembly's region-flag compaction and region passes (their partial
+// counts are scanned by one CTA of 1024 threads)
+#ifndef B2D_COMPACT_GRID
+#define B2D_COMPACT_GRID 592
+#endif
+constexpr uint32_t COMPACT_GRID = B2D_COMPACT_GRID;
+static_assert(COMPACT_GRID <= 1024, "one scan CTA");
 constexpr uint32_t MAX_BUCKETS = 8192;       // source-checkpoint buckets handled per shift partition
 
 // Values that change from one checkpoint to the next.  Kernels read them from device memory
@@ -89,7 +96,7 @@ struct DiffArgs {
   uint32_t* hist;         // cur+1 per-checkpoint counts
   uint32_t* bucket_start; // cur+1 exclusive offsets
   uint32_t* partial;      // SCAN_GRID * max(2, cur+1) scratch
-  uint32_t* partial2;     // SCAN_GRID * 2 scratch
+  uint32_t* partial2;     // COMPACT_GRID * 2 scratch
   uint8_t* diff;          // device diff buffer
   const RoundState* rs;
   uint32_t id_bias;       // subtracted from every node id written into the diff (list approach:

@@ -636,7 +636,7 @@ static uint32_t grid_for(uint64_t units, uint64_t per_cta, uint32_t cap) {
 // for hundreds of idle CTAs per launch; large buffers get the full grids
 DiffGrids diff_grids(const DiffArgs& a, int sm_count) {
   DiffGrids r;
-  r.g = grid_for(((uint64_t)a.N + 15u) / 16u, 512, SCAN_GRID);   // ~1 16-node load per thread
+  r.g = grid_for(((uint64_t)a.N + 15u) / 16u, 512, COMPACT_GRID);   // ~1 16-node load per thread
   // shift-entry ranges: the layout kernel scans every range's count per bucket in one CTA, so
   // fewer, longer ranges (<= 296) keep it short; the scatter walks each range with one warp
   r.gs = grid_for(a.n, 8192, SHIFT_GRID);
