@@ -73,7 +73,7 @@ def parse():
     p.add_argument("--rate", type=float, default=200.0, help="served form: aggregate arrivals per second")
     p.add_argument("--client-max-buffer", type=int, default=2 << 30, help="served form: largest client buffer")
     p.add_argument("--map-reserve", type=float, default=20e9,
-                   help="served and batched forms: device bytes kept mapped for digest-map growth")
+                   help="device bytes kept mapped for digest-map growth after the warm-up (all forms)")
     p.add_argument("--hbm-budget", type=float, default=150e9, help="served form: device bytes for client state")
     a = p.parse_args()
     md5 = a.workload == "md5_f32_8g"
@@ -509,7 +509,7 @@ def main():
 
     from reproducibility_icpp23_scalable_gpu_deduplication_b200 import (HASH_MD5, HASH_MURMUR3, ListDeduplicator,
                                                                         TreeDeduplicator, replicas, synth)
-    from reproducibility_icpp23_scalable_gpu_deduplication_b200.tree import parse_header
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200.tree import parse_header, reserve_map_memory
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -536,46 +536,65 @@ def main():
     dd.checkpoint_device(series.next(), make_baseline=True)          # checkpoint 0: baseline
     for _ in range(args.warmup):
         dd.checkpoint_device(series.next())
-    bufs = [series.next().clone() for _ in range(args.steps)]
-    torch.cuda.synchronize()
+    # the map's baseline is in place: keep device memory mapped for its growth (a long-running
+    # user's steady state; an unreserved growth is dominated by its allocation)
+    if args.map_reserve > 0:
+        reserve_map_memory(int(args.map_reserve))
+    grows0 = dd.map_stats()[2]
+    # the steps' inputs are materialised in HBM before they are timed, in groups that fit half of
+    # the free device memory (one group for the 4 GiB workload, two for the 8 GiB MD5 one); each
+    # group is timed on the device and the group times add up
+    free_b, _ = torch.cuda.mem_get_info(dev)
+    group = max(1, min(args.steps, int(0.5 * free_b) // nbytes))
+    if world > 1:   # every rank takes the same steps in the same groups
+        g_t = torch.tensor([group], device=dev)
+        dist.all_reduce(g_t, op=dist.ReduceOp.MIN)
+        group = int(g_t.item())
 
     stream = torch.cuda.current_stream()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     leaf_s, forest_s, gather_s, diff_bytes, launches = [], [], [], [], 0
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
     # inputs smaller than 2x the 126 MB L2: flush L2 before each step (outside the timed spans)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev) if nbytes < (256 << 20) else None
-    step_ms = []
+    step_ms, group_ms = [], []
     with ClockSampler(local) as clk:
-        start.record(stream)
-        for b in bufs:
-            if flush is not None:
-                flush.fill_(1)
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-            diff_bytes.append(dd.checkpoint_device(b))
-            if flush is not None:
-                e1.record(stream)
-                e1.synchronize()
-                step_ms.append(e0.elapsed_time(e1))
-            ph, path = dd.phase_times()
-            leaf_s.append(ph[0])
-            forest_s.append(ph[1])
-            gather_s.append(ph[2])
-            launches += dd.last_launch_count()
-        stop.record(stream)
-        torch.cuda.synchronize()
+        done = 0
+        while done < args.steps:
+            bufs = [series.next().clone() for _ in range(min(group, args.steps - done))]
+            torch.cuda.synchronize()
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+            start.record(stream)
+            for b in bufs:
+                if flush is not None:
+                    flush.fill_(1)
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                diff_bytes.append(dd.checkpoint_device(b))
+                if flush is not None:
+                    e1.record(stream)
+                    e1.synchronize()
+                    step_ms.append(e0.elapsed_time(e1))
+                ph, path = dd.phase_times()
+                leaf_s.append(ph[0])
+                forest_s.append(ph[1])
+                gather_s.append(ph[2])
+                launches += dd.last_launch_count()
+            stop.record(stream)
+            torch.cuda.synchronize()
+            group_ms.append(start.elapsed_time(stop))
+            done += len(bufs)
+            del bufs
     if world > 1:
         dist.barrier()
-    ms = start.elapsed_time(stop) if flush is None else sum(step_ms)
+    ms = sum(group_ms) if flush is None else sum(step_ms)
+    grows_timed = dd.map_stats()[2] - grows0
     del flush
     # replicas: the slowest rank's time, every rank's bytes
     rate, ms_max = replicas.throughput(ms, args.steps * nbytes, dev)
     value = rate / GB
     leaf_ms = 1e3 * statistics.mean(leaf_s)   # 0 when the graph runs without timing events
-    del bufs
 
     # end to end through the public API: each step copies its input from pinned host memory to
     # the device and checkpoints it with the host-diff call, which brings the diff back into the
@@ -674,6 +693,8 @@ def main():
         "data": "synthetic (seeded; reference datasets unavailable)",
         "config": {"workload": args.workload, "nbytes": nbytes, "chunk_size": cs, "hash": "md5" if md5 else "murmur3",
                    "approach": args.approach, "checkpoints": 1 + args.warmup + args.steps,
+                   "timed_groups": f"{len(group_ms)} (inputs of a group resident in HBM before it is timed)",
+                   "map_growth": {"reserved_bytes": int(args.map_reserve), "grows_in_timed_steps": grows_timed},
                    "l2": (f"inputs {nbytes / 2**30:.2f} GiB > L2, no flush" if nbytes >= (256 << 20) else
                           "L2 flushed (512 MiB write) before each step, outside the timed spans"),
                    "parallelism": f"replicas x{world}"},
