@@ -83,3 +83,60 @@ def test_list_baseline_resets_list_and_map():
     assert o.num_first_ocur() == 0 and o.num_shift_dupl() == 0
     o.checkpoint(a, True)
     assert o.num_first_ocur() == 100 and o.num_shift_dupl() == 0
+
+
+def py_list_series(bufs, cs, baselines):
+    """A second, independent reading of src/list_approach.cpp (:23-257, :843-931) in plain Python,
+    for small inputs: the per-chunk rule in ascending chunk order, then the diff layout."""
+    zero = bytes(16)
+    digests, table, diffs = [], {}, []
+    cur = base_id = 0
+    for b, mb in zip(bufs, baselines):
+        n = -(-len(b) // cs)
+        if mb:
+            digests, table = [zero] * n, {}
+        digests += [zero] * (n - len(digests))
+        if cur == 0 or mb:
+            base_id = cur
+        first, shift = [], []
+        for c in range(n):
+            d = O.hash_bytes(bytes(b[c * cs:(c + 1) * cs]))
+            if d == digests[c]:
+                continue
+            if d in table:
+                shift.append(c)
+            else:
+                table[d] = (c, cur)
+                first.append(c)
+            digests[c] = d
+        src = {c: table[digests[c]] for c in shift}
+        trees = sorted({t for _, t in src.values()})
+        rows = b"".join(np.array([t, sum(1 for _, u in src.values() if u == t)], np.uint32).tobytes() for t in trees)
+        pairs = b"".join(np.array([c, src[c][0]], np.uint32).tobytes()
+                         for t in trees for c in shift if src[c][1] == t)
+        data = b"".join(bytes(b[c * cs:(c + 1) * cs]).ljust(cs, b"\0") for c in first)
+        hdr = np.array([base_id, cur], np.uint32).tobytes() + np.array([len(b)], np.uint64).tobytes() + \
+            np.array([cs, len(first), len(trees), len(shift)], np.uint32).tobytes()
+        diffs.append(hdr + np.array(first, np.uint32).tobytes() + rows + pairs + data)
+        cur += 1
+    return diffs
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2, 3])
+def test_list_oracle_matches_independent_model(seed):
+    """random small series with many repeated chunks, reverts and baselines mid-sequence"""
+    rng = np.random.default_rng(seed)
+    cs = [16, 32, 48, 64][seed]
+    n = int(rng.integers(3, 200))
+    size = n * cs - int(rng.integers(0, cs))
+    palette = rng.integers(0, 256, (6, cs), dtype=np.uint8)
+    bufs = []
+    for k in range(6):
+        pick = rng.integers(0, len(palette) + 2, n)
+        b = np.concatenate([palette[p] if p < len(palette) else rng.integers(0, 256, cs, dtype=np.uint8)
+                            for p in pick])[:size]
+        bufs.append(b)
+    baselines = [True, False, False, bool(rng.integers(0, 2)), False, False]
+    o = O.OracleListDeduplicator(cs)
+    got = [o.checkpoint(b, mb) for b, mb in zip(bufs, baselines)]
+    assert got == py_list_series(bufs, cs, baselines)
