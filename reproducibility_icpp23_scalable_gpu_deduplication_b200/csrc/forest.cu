@@ -33,13 +33,14 @@
 namespace b2d {
 
 // resident CTAs per SM the band kernels are compiled for (register budget): phase 1 at 8
-// (32 registers) measured ~6% faster on its launches than the unconstrained 40 registers;
-// the phase-2 band gained nothing from a tighter budget
+// (32 registers) measured ~6% faster on its launches than the unconstrained 40 registers; the
+// phase-2 band at 4 (64 registers, no spills) took 0.29 instead of 0.30 ms of forest time per
+// 4 GiB step once its first band ran on a resident grid (3 CTAs per SM before)
 #ifndef B2D_FF_MINB
 #define B2D_FF_MINB 8
 #endif
 #ifndef B2D_FAST_MINB
-#define B2D_FAST_MINB 1
+#define B2D_FAST_MINB 4
 #endif
 
 constexpr uint32_t FOREST_THREADS = 512;
