@@ -46,6 +46,12 @@ def test_strerror_and_argument_errors_without_gpu():
     assert L.b2d_destroy(None) == -1
     v = ctypes.c_uint64()
     assert L.b2d_num_first_ocur(None, ctypes.byref(v)) == -1
+    # the list approach's constructor and the device-diff log writer check the same way
+    assert L.b2d_create_list(0, 0, ctypes.byref(h)) == -1
+    assert L.b2d_create_list(128, 7, ctypes.byref(h)) == -1
+    assert L.b2d_write_chkpt_log(None, b"log") == -1
+    assert L.b2d_copy_diff_async(None, None, 0, None) == -1
+    assert L.b2d_restart_noalloc(None, 0, None, None, 0, 0, None) == -1
 
 
 def test_no_oracle_in_product():
