@@ -545,11 +545,7 @@ def main():
     # the free device memory (one group for the 4 GiB workload, two for the 8 GiB MD5 one); each
     # group is timed on the device and the group times add up
     free_b, _ = torch.cuda.mem_get_info(dev)
-    group = max(1, min(args.steps, int(0.5 * free_b) // nbytes))
-    if world > 1:   # every rank takes the same steps in the same groups
-        g_t = torch.tensor([group], device=dev)
-        dist.all_reduce(g_t, op=dist.ReduceOp.MIN)
-        group = int(g_t.item())
+    group = replicas.agree_min(max(1, min(args.steps, int(0.5 * free_b) // nbytes)), dev)
 
     stream = torch.cuda.current_stream()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -19,7 +19,8 @@ def _rank(rank, world, port, q):
         first = bytes(s.next()[:64])
         ms = 10.0 * (rank + 1)
         rate, ms_max = replicas.throughput(ms, 1000 * (rank + 1))
-        q.put((rank, rate, ms_max, first, replicas.world()))
+        group = replicas.agree_min(5 + 3 * rank)   # e.g. inputs per timed group, from free memory
+        q.put((rank, rate, ms_max, first, replicas.world(), group))
         dist.barrier()
     finally:
         dist.destroy_process_group()
@@ -36,8 +37,9 @@ def test_two_gloo_replicas():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    (r0, rate0, ms0, b0, w0), (r1, rate1, ms1, b1, w1) = out
+    (r0, rate0, ms0, b0, w0, g0), (r1, rate1, ms1, b1, w1, g1) = out
     assert w0 == w1 == 2
+    assert g0 == g1 == 5                            # every rank groups its timed steps alike
     assert ms0 == ms1 == 20.0                       # the slowest rank's time
     assert rate0 == rate1 == pytest.approx(3000 / 0.020)   # everyone's units
     assert b0 != b1                                 # replicas checkpoint different data
