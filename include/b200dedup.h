@@ -61,8 +61,9 @@ int b2d_create(uint32_t chunk_size, int hash_kind, b2d_dedup** out);
  * (one digest per chunk, a changed chunk is a first occurrence or a shifted duplicate,
  * src/list_approach.cpp:23-257) behind the same handle.  Every call below takes it: checkpoint
  * overloads (:843-974, diffs naming chunk indices), host and device restarts (:259-586), file
- * and log forms ("List" rows).  Not accepted by the batched form (B2D_ERR_UNSUPPORTED) nor by
- * b2d_restart_noalloc, which restarts tree diffs. */
+ * and log forms ("List" rows), and batches (alone or mixed with tree handles; a list handle
+ * labels and assembles its diff in its own branch of the batch).  Not by b2d_restart_noalloc,
+ * which restarts tree diffs. */
 int b2d_create_list(uint32_t chunk_size, int hash_kind, b2d_dedup** out);
 /* ~TreeDeduplicator() -- src/tree_approach.cpp:11 (~ListDeduplicator(), src/list_approach.cpp:11) */
 int b2d_destroy(b2d_dedup* d);

@@ -145,7 +145,7 @@ class TreeDeduplicator {
 
 // ListDeduplicator(uint32_t bytes_per_chunk) -- src/list_approach.cpp:5-9, with the same method
 // set (include/list_approach.hpp): checkpoint overloads write list diffs naming chunk indices,
-// restarts take list diffs.  Not accepted by CheckpointBatch.
+// restarts take list diffs.  Batches take list handles beside tree handles.
 class ListDeduplicator : public TreeDeduplicator {
  public:
   explicit ListDeduplicator(uint32_t bytes_per_chunk, int hash_kind = B2D_HASH_MURMUR3)

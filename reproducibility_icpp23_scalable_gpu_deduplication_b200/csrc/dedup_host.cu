@@ -1198,7 +1198,6 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
   if (count == 0) return B2D_OK;
   for (uint32_t i = 0; i < count; i++) {
     if (!hs[i]) return B2D_ERR_ARG;
-    if (hs[i]->list) return B2D_ERR_UNSUPPORTED;   // the batched form runs tree handles
     for (uint32_t j = 0; j < i; j++)
       if (hs[j] == hs[i]) return B2D_ERR_ARG;   // one checkpoint per handle per batch
   }
@@ -1269,7 +1268,11 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
   L.queues = align_up(L.states + sizeof(DevState*) * count, 64);
   L.bstatus = align_up(L.queues + sizeof(unsigned int) * (groups.size() + 1), 64);
   L.dargs = align_up(L.bstatus + sizeof(DevStatus), 64);
-  const bool seg_diff = b->batch_diff && cand.shared;
+  // list handles label and assemble their diffs in their own branches; the shared segmented
+  // forest and diff launches take the tree handles (none: no shared launches)
+  uint32_t trees = 0;
+  for (uint32_t i = 0; i < count; i++) trees += hs[i]->list ? 0u : 1u;
+  const bool seg_diff = b->batch_diff && cand.shared && trees > 0;
   L.dtab = align_up(L.dargs + (seg_diff ? sizeof(DiffArgs) * count : 0), 64);
   const size_t tab_len = (size_t)count + 1;   // entries per table
   // shared forest phases: every handle's launch steps, one segmented launch per (phase, step,
@@ -1287,7 +1290,7 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
       fsteps[ph].resize(count);
       uint32_t K = 0;
       for (uint32_t i = 0; i < count; i++) {
-        forest_steps(hs[i]->D, hs[i]->N, ph + 1, fsteps[ph][i]);
+        if (!hs[i]->list) forest_steps(hs[i]->D, hs[i]->N, ph + 1, fsteps[ph][i]);
         K = std::max<uint32_t>(K, (uint32_t)fsteps[ph][i].size());
       }
       for (uint32_t k = 0; k < K; k++)
@@ -1320,18 +1323,20 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
   if (seg_diff) {
     auto tab = [&](int t) { return reinterpret_cast<uint32_t*>(H + L.dtab) + (size_t)t * tab_len; };
     auto dtab = [&](int t) { return reinterpret_cast<const uint32_t*>(B + L.dtab) + (size_t)t * tab_len; };
-    uint32_t tot_g = 0, tot_gl = 0, tot_gp = 0, tot_gs = 0, tot_v[GATHER_VARIANTS] = {0};
+    uint32_t tot_g = 0, tot_gl = 0, tot_gp = 0, tot_gs = 0, tot_one = 0, tot_v[GATHER_VARIANTS] = {0};
     uint32_t max_bcap = 1;
     for (uint32_t i = 0; i < count; i++) {
       b2d_dedup* d = hs[i];
       const DiffArgs da = diff_args(d, &d->state.p->round);
       std::memcpy(H + L.dargs + sizeof(DiffArgs) * i, &da, sizeof(da));
-      const DiffGrids dg = diff_grids(da, b->sm_count);
+      DiffGrids dg = diff_grids(da, b->sm_count);
+      if (d->list) dg.g = dg.gl = dg.gp = dg.gs = dg.gg = 0;   // its own branch assembles its diff
       tab(DT_G)[i] = dg.g;
       tab(DT_GS)[i] = dg.gs;
       tab(DT_BCAP)[i] = d->bcap;
       max_bcap = std::max(max_bcap, d->bcap);
-      tab(DT_ONE)[i] = i;
+      tab(DT_ONE)[i] = tot_one;
+      tot_one += d->list ? 0u : 1u;
       tab(DT_BEG_G)[i] = tot_g;
       tot_g += dg.g;
       tab(DT_BEG_GL)[i] = tot_gl;
@@ -1345,7 +1350,7 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
         if (v == dg.variant) tot_v[v] += dg.gg;
       }
     }
-    tab(DT_ONE)[count] = count;
+    tab(DT_ONE)[count] = tot_one;
     tab(DT_BEG_G)[count] = tot_g;
     tab(DT_BEG_GL)[count] = tot_gl;
     tab(DT_BEG_GP)[count] = tot_gp;
@@ -1362,6 +1367,7 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
       dplan.beg_gather[v] = dtab(DT_BEG_GATHER + v);
       dplan.tot_gather[v] = tot_v[v];
     }
+    dplan.tot_one = tot_one;
     dplan.tot_g = tot_g;
     dplan.tot_gl = tot_gl;
     dplan.tot_gp = tot_gp;
@@ -1465,9 +1471,11 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
         if (erc != B2D_OK) break;
         b2d_dedup* d = hs[i];
         const bool skip_leaves = item_of[i] >= 0;
-        if (seg_forest && skip_leaves) continue;   // nothing of this handle runs in a branch
-        const int r = enqueue_checkpoint(d, s, &d->state.p->round, false, false, skip_leaves, true, seg_diff,
-                                         seg_forest);
+        // nothing of a tree handle runs in a branch when its leaves, forest and diff are all
+        // shared; a list handle labels and assembles its diff here
+        if (seg_forest && skip_leaves && !d->list) continue;
+        const int r = enqueue_checkpoint(d, s, &d->state.p->round, false, false, skip_leaves, true,
+                                         seg_diff && !d->list, seg_forest);
         if (r != B2D_OK) erc = r;
         launches += d->launches;
       }

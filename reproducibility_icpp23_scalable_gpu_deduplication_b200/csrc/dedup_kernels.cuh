@@ -216,12 +216,13 @@ constexpr int GATHER_VARIANTS = 7;
 DiffGrids diff_grids(const DiffArgs& a, int sm_count);
 struct DiffBatch {
   SegGrid base;                     // beg unused
-  const uint32_t* beg_one;          // 0, 1, .., n: one CTA per handle
+  const uint32_t* beg_one;          // one CTA per handle that takes part (prefix table)
   const uint32_t* beg_g;
   const uint32_t* beg_gl;
   const uint32_t* beg_gp;
   const uint32_t* beg_gs;
   const uint32_t* beg_gather[GATHER_VARIANTS];
+  uint32_t tot_one;                 // handles with one CTA in the scan and layout launches
   uint32_t tot_g, tot_gl, tot_gp, tot_gs, tot_gather[GATHER_VARIANTS];
   uint32_t max_bcap;
 };

@@ -656,15 +656,15 @@ cudaError_t launch_collect_diff_batch(const DiffBatch& b, cudaStream_t stream, u
   uint32_t c = 0;
   const size_t hsm = sizeof(uint32_t) * b.max_bcap;
   s.beg = b.beg_g;   compact_count_seg<<<b.tot_g, COMPACT_THREADS, 0, stream>>>(s); c++;
-  s.beg = b.beg_one; compact_scan_seg<<<s.n, 1024, 0, stream>>>(s); c++;
+  s.beg = b.beg_one; compact_scan_seg<<<b.tot_one, 1024, 0, stream>>>(s); c++;
   s.beg = b.beg_g;   compact_write_seg<<<b.tot_g, COMPACT_THREADS, 0, stream>>>(s); c++;
   s.beg = b.beg_gl;  compact_levels_seg<<<b.tot_gl, 256, 0, stream>>>(s); c++;
   s.beg = b.beg_gp;  compact_permute_seg<<<b.tot_gp, 256, 0, stream>>>(s); c++;
   s.beg = b.beg_g;   region_count_seg<<<b.tot_g, COMPACT_THREADS, 0, stream>>>(s); c++;
-  s.beg = b.beg_one; region_scan_seg<<<s.n, 1024, 0, stream>>>(s); c++;
+  s.beg = b.beg_one; region_scan_seg<<<b.tot_one, 1024, 0, stream>>>(s); c++;
   s.beg = b.beg_g;   region_write_seg<<<b.tot_g, COMPACT_THREADS, 0, stream>>>(s); c++;
   s.beg = b.beg_gs;  shift_prev_seg<<<b.tot_gs, 128, hsm, stream>>>(s); c++;
-  s.beg = b.beg_one; layout_seg<<<s.n, 1024, 0, stream>>>(s); c++;
+  s.beg = b.beg_one; layout_seg<<<b.tot_one, 1024, 0, stream>>>(s); c++;
   s.beg = b.beg_gs;  shift_write_seg<<<b.tot_gs, 32, hsm, stream>>>(s); c++;
   for (int v = 0; v < GATHER_VARIANTS; v++) {
     if (!b.tot_gather[v]) continue;

@@ -300,7 +300,7 @@ class ListDeduplicator(TreeDeduplicator):
     Same methods and argument meaning as ``TreeDeduplicator`` (include/list_approach.hpp): one
     digest per chunk, a changed chunk is a first occurrence or a shifted duplicate of an earlier
     one, and the diff names chunk indices (src/list_approach.cpp:23-257).  Restarts take list
-    diffs (:259-586).  Not usable with ``CheckpointBatch``."""
+    diffs (:259-586).  ``CheckpointBatch`` takes list handles beside tree handles."""
 
     _create = "b2d_create_list"
 

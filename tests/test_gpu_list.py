@@ -1,7 +1,8 @@
 """GPU parity of the list approach (ListDeduplicator) through the C ABI against the oracle.
 
 Bit-exact comparisons: every diff (header, first-occurrence list, repeat table, shifted pairs,
-data) and every restarted buffer, from host diffs and from device-resident diffs.
+data) and every restarted buffer, from host diffs and from device-resident diffs; list handles
+in batches against their one-at-a-time diffs.
 """
 import numpy as np
 import pytest
@@ -108,16 +109,52 @@ def test_list_md5_float_series(cuda):
     run_both([s.next().copy() for _ in range(3)], 256, HASH_MD5)
 
 
-def test_list_not_in_batches(cuda):
-    import torch
+# (bytes, chunk size, approach): uneven sizes, short last chunks, a buffer smaller than a tile,
+# one that cannot be staged (100 B chunks: per-buffer hashing in its branch)
+MIXED = [(1 << 20, 128, "list"), ((3 << 20) + 77, 128, "tree"), (200, 128, "list"),
+         ((2 << 20) + 300, 100, "list"), (5 << 20, 128, "tree"), (64 << 10, 64, "list")]
 
-    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import B2DError, CheckpointBatch
 
-    g = ListDeduplicator(128)
-    x = torch.zeros(1 << 16, dtype=torch.uint8, device="cuda")
-    with pytest.raises(B2DError):
-        CheckpointBatch().checkpoint([g], [x], [True])
-    g.close()
+def _series(i, nbytes, cs):
+    return synth.ByteSeries(nbytes, cs, lambda rng, n: synth.plan_varied(rng, n, 64), 11, buf_id=i, device="cuda")
+
+
+def _handle(kind, cs):
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import TreeDeduplicator
+
+    return (ListDeduplicator if kind == "list" else TreeDeduplicator)(cs)
+
+
+@pytest.mark.parametrize("specs", [MIXED, [x for x in MIXED if x[2] == "list"]], ids=["mixed", "lists"])
+@pytest.mark.parametrize("shared", [1, 0])
+@pytest.mark.parametrize("graph", [0, 2])
+def test_list_handles_in_batches(cuda, specs, shared, graph):
+    """list handles in a batch (with tree handles, or alone): every handle's diff equals the diff
+    it gives checkpointing alone, over baselines, incremental rounds and a mid-series baseline"""
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import CheckpointBatch
+
+    rounds = 5
+    baselines = [[True] * len(specs)] + [[False] * len(specs) for _ in range(rounds - 1)]
+    baselines[3][0] = True
+    want = []
+    for i, (nb, cs, kind) in enumerate(specs):
+        s, h = _series(i, nb, cs), _handle(kind, cs)
+        per = []
+        for r in range(rounds):
+            h.checkpoint_device(s.next(), baselines[r][i])
+            per.append(bytes(h.copy_diff()))
+        h.close()
+        want.append(per)
+    batch = CheckpointBatch(shared=shared, graph=graph)
+    ss = [_series(i, nb, cs) for i, (nb, cs, _) in enumerate(specs)]
+    hs = [_handle(kind, cs) for (_, cs, kind) in specs]
+    for r in range(rounds):
+        batch.checkpoint(hs, [s.next() for s in ss], baselines[r])
+        for i, h in enumerate(hs):
+            assert bytes(h.copy_diff()) == want[i][r], (r, i, specs[i])
+    for h in hs:
+        h.close()
+    batch.close()
 
 
 def test_list_long_chain_restart_windows(cuda):
