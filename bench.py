@@ -48,8 +48,8 @@ def parse():
                         "the 64 MiB CPU-runnable series (5% rewritten, 2% shifted, 1% zeroed per checkpoint)")
     p.add_argument("--chunk-size", type=int, default=None, help="default 128 (plain_4g) / 256 (md5_f32_8g)")
     p.add_argument("--approach", default="tree", choices=["tree", "list"],
-                   help="plain form and reference arm: the tree approach (default) or the list approach "
-                        "(ListDeduplicator); the batched and served forms run the tree approach")
+                   help="the tree approach (default) or the list approach (ListDeduplicator), in every "
+                        "form and in the reference arm")
     p.add_argument("--nbytes", type=int, default=None, help="default 4 GiB (plain_4g) / 8 GiB (md5_f32_8g)")
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--cpu-sample-bytes", type=int, default=512 << 20)
@@ -217,8 +217,11 @@ def run_batched(args, rank, world, dev):
     """256 buffers of log-uniform sizes: the batch API against the same buffers one at a time."""
     import torch
 
-    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import CheckpointBatch, TreeDeduplicator, replicas, synth
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import (CheckpointBatch, ListDeduplicator,
+                                                                        TreeDeduplicator, replicas, synth)
     from reproducibility_icpp23_scalable_gpu_deduplication_b200.tree import reserve_map_memory
+
+    Dedup = ListDeduplicator if args.approach == "list" else TreeDeduplicator
 
     sizes = synth.batched_sizes(count=args.buffers, hi=args.max_buffer)
     total = sum(sizes)
@@ -229,7 +232,7 @@ def run_batched(args, rank, world, dev):
 
     def series_pass(step_fn, tune_fn=None):
         ss = batched_series(sizes, dev, seed)
-        hs = [TreeDeduplicator(128) for _ in sizes]
+        hs = [Dedup(128) for _ in sizes]
         times, sums, launches = [], [], 0
         grows0 = 0
         for c in range(ckpts):
@@ -273,7 +276,7 @@ def run_batched(args, rank, world, dev):
         # tuning series: a baseline, then incremental batches until the tuner settles
         batch.set_param("autotune", 1)
         ss = batched_series(sizes, dev, seed + 1000)
-        hs = [TreeDeduplicator(128) for _ in sizes]
+        hs = [Dedup(128) for _ in sizes]
         for c in range(12):
             batch.checkpoint(hs, [s.next() for s in ss])
             if batch.get_param("tuned"):
@@ -301,13 +304,13 @@ def run_batched(args, rank, world, dev):
     peak, peak_kind = measured_peak()
     alg = total + 32 * chunks
     line = {
-        "metric": "tree-dedup batched ingest GB/s", "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
+        "metric": f"{args.approach}-dedup batched ingest GB/s", "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
         "steps": len(t_batch), "warmup": args.warmup, "ms_per_step": round(ms_b, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic (seeded; reference datasets unavailable)",
         "config": {"workload": f"batched_{len(sizes)}", "buffers": len(sizes), "total_bytes": total,
                    "min_buffer": min(sizes), "max_buffer": max(sizes), "chunk_size": 128, "hash": "murmur3",
-                   "checkpoints": ckpts, "change": "uniform [0.5%, 20%] in runs of 1-256 chunks + 1% shifted",
+                   "approach": args.approach, "checkpoints": ckpts, "change": "uniform [0.5%, 20%] in runs of 1-256 chunks + 1% shifted",
                    "l2": f"inputs {total / 2**30:.1f} GiB > L2, no flush", "tuned": tuned},
         "plain_same_workload": None if args.no_plain else {
             "value": round(plain, 2), "unit": "GB/s", "ms_per_step": round(ms_p, 4), "gpu_launches": l_plain},
@@ -435,7 +438,7 @@ def run_served(args, rank, world, dev):
     clients = rng.integers(0, len(sizes), n)
     arrivals = synth.poisson_arrivals(args.rate, n, seed=synth.SEED + rank)
     budget = args.hbm_budget
-    kw = {"hbm_budget": budget, "max_batch": 64, "max_inflight": 2}
+    kw = {"hbm_budget": budget, "max_batch": 64, "max_inflight": 2, "approach": args.approach}
 
     def summarize(reqs, wall, batches, service):
         lat = [1e3 * r.latency for r in reqs]
@@ -455,12 +458,13 @@ def run_served(args, rank, world, dev):
         cap_served = summarize(*serve_capacity(kw, sizes, 4, dev))
         cap_plain = summarize(*serve_capacity(dict(kw, plain=True), sizes, 4, dev))
     line = {
-        "metric": "tree-dedup served GB/s", "value": served["value"], "unit": "GB/s", "n_gpus": world,
+        "metric": f"{args.approach}-dedup served GB/s", "value": served["value"], "unit": "GB/s", "n_gpus": world,
         "steps": n, "warmup": 2, "ms_per_step": served["p50_ms"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded; reference datasets unavailable)",
         "config": {"workload": f"served_{len(sizes)}_clients", "clients": len(sizes), "rate_hz": args.rate,
                    "requests": n, "client_bytes_total": sum(sizes), "min_buffer": min(sizes),
-                   "max_buffer": max(sizes), "chunk_size": 128, "hash": "murmur3", "hbm_budget": budget, "map_growth_reserve": args.map_reserve,
+                   "max_buffer": max(sizes), "chunk_size": 128, "hash": "murmur3", "approach": args.approach,
+                   "hbm_budget": budget, "map_growth_reserve": args.map_reserve,
                    "change": "uniform [0.5%, 20%] in runs of 1-512 chunks + 1% shifted, edited on the device",
                    "latency": "scheduled arrival -> diff in pinned host memory (includes the client's wait "
                               "for its own previous request and its device-side edit of its buffer); "
@@ -484,8 +488,6 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank)
         return
-    if args.form != "plain" and args.approach != "tree":
-        raise SystemExit("--approach list runs the plain form only")
     if args.form != "plain":
         import torch
         import torch.distributed as dist

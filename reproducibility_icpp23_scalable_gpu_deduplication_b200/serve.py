@@ -5,8 +5,9 @@ The reference has no server; its driver checkpoints one buffer per call
 clients submit "checkpoint my device buffer now" requests as they arrive.  The loop
 
 * keeps each client's Merkle tree and digest map resident on the device between its requests
-  (one ``TreeDeduplicator`` handle per client), so every request after the first is an
-  incremental checkpoint against that client's own previous one;
+  (one ``TreeDeduplicator`` handle per client, or ``ListDeduplicator`` with
+  ``approach="list"``), so every request after the first is an incremental checkpoint against
+  that client's own previous one;
 * admits a request when its client's state fits in the HBM budget (the handle's device bytes:
   ``estimate_memory`` before its first checkpoint, ``memory()`` after), evicting the least
   recently used idle clients when allowed (an evicted client's next request is a baseline);
@@ -30,7 +31,7 @@ import time
 
 from ._lib import HASH_MURMUR3
 from .batch import CheckpointBatch
-from .tree import TreeDeduplicator, estimate_memory, reserve_map_memory
+from .tree import ListDeduplicator, TreeDeduplicator, estimate_memory, reserve_map_memory
 
 __all__ = ["CheckpointServer", "Request"]
 
@@ -71,16 +72,21 @@ class _Client:
 
 class CheckpointServer:
     def __init__(self, hbm_budget=150e9, chunk_size=128, hash_kind=HASH_MURMUR3, max_batch=64, max_inflight=2,
-                 evict=True, plain=False, checksum=False, clock=time.perf_counter, map_reserve=0, **batch_params):
+                 evict=True, plain=False, checksum=False, clock=time.perf_counter, map_reserve=0, approach="tree",
+                 **batch_params):
         """`map_reserve`: bytes of device memory kept mapped for digest maps
         (``reserve_growth``), so a client whose map grows does not pay for fresh driver
-        allocations (tens of ms per GB) inside its request; released by ``close``."""
+        allocations (tens of ms per GB) inside its request; released by ``close``.
+        `approach`: "tree" (``TreeDeduplicator`` per client) or "list" (``ListDeduplicator``)."""
         import torch
 
         self.budget = int(hbm_budget)
         self.cs, self.kind = int(chunk_size), int(hash_kind)
         self.max_batch, self.plain, self.evict, self.checksum = int(max_batch), plain, evict, checksum
         self.clock = clock
+        if approach not in ("tree", "list"):
+            raise ValueError(f"approach must be 'tree' or 'list', not {approach!r}")
+        self.Dedup = ListDeduplicator if approach == "list" else TreeDeduplicator
         self.clients = collections.defaultdict(_Client)
         self.waiting = collections.deque()       # arrived, not admitted (arrival order)
         self.resident = 0                        # bytes reserved by resident clients
@@ -195,7 +201,7 @@ class CheckpointServer:
                 blocked.add(r.client)
                 continue
             if c.handle is None:
-                c.handle = TreeDeduplicator(self.cs, self.kind)
+                c.handle = self.Dedup(self.cs, self.kind)
                 c.reserved = need
                 self.resident += need
                 self.peak_resident = max(self.peak_resident, self.resident)

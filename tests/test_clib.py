@@ -98,3 +98,11 @@ def test_file_tools_build_and_check_arguments():
     r = subprocess.run([_build.tool_path("restart_chkpt_files"), "0", "1", "1", "128", "--run-full-chkpt", "x"],
                        capture_output=True, text=True)
     assert r.returncode == 2
+
+
+def test_server_rejects_unknown_approach():
+    """the served loop builds tree or list handles; any other approach is an argument error"""
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200.serve import CheckpointServer
+
+    with pytest.raises(ValueError):
+        CheckpointServer(approach="full")

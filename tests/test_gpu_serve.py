@@ -6,7 +6,7 @@ checkpoints the same buffers one at a time.  Diff checksums must be identical re
 """
 import pytest
 
-from reproducibility_icpp23_scalable_gpu_deduplication_b200 import TreeDeduplicator, synth
+from reproducibility_icpp23_scalable_gpu_deduplication_b200 import ListDeduplicator, TreeDeduplicator, synth
 from reproducibility_icpp23_scalable_gpu_deduplication_b200.serve import CheckpointServer, percentile
 from reproducibility_icpp23_scalable_gpu_deduplication_b200.tree import estimate_memory, parse_header
 
@@ -36,11 +36,11 @@ def drive(server, sizes, rounds, order_seed=1):
     return reqs
 
 
-def alone(sizes, rounds):
+def alone(sizes, rounds, dedup=TreeDeduplicator):
     out = {}
     for c, n in enumerate(sizes):
         s = synth.DeviceSeries(n, 128, c, max_run=64)
-        h = TreeDeduplicator(128)
+        h = dedup(128)
         for k in range(rounds):
             h.checkpoint_device(s.next(), k == 0)
             out[(c, k)] = h.diff_checksum()
@@ -67,6 +67,21 @@ def test_served_plain_mode_same(cuda):
     srv = CheckpointServer(hbm_budget=8e9, plain=True, checksum=True)
     reqs = drive(srv, SIZES, rounds, order_seed=2)
     want = alone(SIZES, rounds)
+    for key, r in reqs.items():
+        assert r.rc == 0 and r.checksum == want[key], key
+    srv.close()
+
+
+@pytest.mark.parametrize("plain", [False, True])
+def test_served_list_approach(cuda, plain):
+    """approach="list": one ListDeduplicator per client; every request's list diff equals the
+    one its client's buffers give checkpointed alone"""
+    rounds = 3
+    srv = CheckpointServer(hbm_budget=8e9, max_batch=4, max_inflight=2, checksum=True, plain=plain,
+                           approach="list")
+    reqs = drive(srv, SIZES, rounds, order_seed=5)
+    assert all(isinstance(c.handle, ListDeduplicator) for c in srv.clients.values())
+    want = alone(SIZES, rounds, ListDeduplicator)
     for key, r in reqs.items():
         assert r.rc == 0 and r.checksum == want[key], key
     srv.close()
