@@ -45,7 +45,9 @@ enum b2d_status {
   B2D_ERR_RESTART_RANGE = -9,  /* restart met an index/offset outside its buffers (corrupt
                                   diff, or the reference's non-power-of-two region quirk);
                                   the offending copies were skipped */
-  B2D_ERR_LEN_CHANGED = -10,   /* buffer length changed without make_baseline */
+  B2D_ERR_LEN_CHANGED = -10,   /* buffer length changed without make_baseline, or the handle
+                                  holds no complete checkpoint (after a failed one) and this
+                                  one is not a baseline */
   B2D_ERR_UNSUPPORTED = -11    /* outside the supported range (e.g. > 8192 checkpoints per baseline) */
 };
 
@@ -212,7 +214,10 @@ int b2d_estimate_memory(uint64_t len, uint32_t chunk_size, int map_max_load_pct,
  * would give: afterwards b2d_diff_device / b2d_copy_diff / b2d_num_first_ocur read it, and
  * the handle's checkpoint id has advanced.  Handles must be distinct within a call.
  * `make_baseline` may be NULL (no forced baselines); `rcs` (nullable) receives each handle's
- * status.  The graph is rebuilt only when a handle's buffers or sizes change. */
+ * status.  Every handle's arguments are checked before any handle is touched, so a call
+ * rejected by B2D_ERR_ARG / B2D_ERR_LEN_CHANGED / B2D_ERR_UNSUPPORTED leaves every handle as it
+ * was (`rcs` names the offending entry).  The graph is rebuilt only when a handle's buffers or
+ * sizes change. */
 typedef struct b2d_batch b2d_batch;
 int b2d_batch_create(b2d_batch** out);
 int b2d_batch_destroy(b2d_batch* b);

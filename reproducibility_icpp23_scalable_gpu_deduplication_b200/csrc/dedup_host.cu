@@ -416,14 +416,27 @@ LeafArgs leaf_args(const b2d_dedup* d, const RoundState* rs_dev) {
 // + enqueue (device work, identical launch parameters for every checkpoint of a buffer, so it
 // is captured once into a CUDA graph and replayed) + finish (host: status and sizes).
 // ------------------------------------------------------------------------------------------
-int prepare_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, bool make_baseline) {
+// The argument checks of one checkpoint; they change nothing, so a batch runs them for every
+// handle before it prepares any.
+int check_checkpoint(const b2d_dedup* d, const void* d_data, uint64_t len, bool make_baseline) {
   if (!d_data || len == 0) return B2D_ERR_ARG;
-  uint64_t nc = (len + d->chunk_size - 1) / d->chunk_size;
+  const uint64_t nc = (len + d->chunk_size - 1) / d->chunk_size;
   if (nc > 0x7fffffffull) return B2D_ERR_ARG;
   const bool baseline = (d->current_id == 0) || make_baseline;
   if (!baseline && (!d->have_tree || nc != d->n)) return B2D_ERR_LEN_CHANGED;
   // source-checkpoint buckets, and the map's checkpoint field (MAP_TREE_PENDING is reserved)
   if (d->current_id + 1u > MAX_BUCKETS || d->current_id >= MAP_TREE_PENDING) return B2D_ERR_UNSUPPORTED;
+  return B2D_OK;
+}
+
+int prepare_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, bool make_baseline) {
+  const int vrc = check_checkpoint(d, d_data, len, make_baseline);
+  if (vrc) return vrc;
+  const uint64_t nc = (len + d->chunk_size - 1) / d->chunk_size;
+  const bool baseline = (d->current_id == 0) || make_baseline;
+  // a baseline replaces the tree and the map: until it completes the handle holds neither the
+  // old checkpoint's state nor the new one's, and only another baseline may follow
+  if (baseline) d->have_tree = false;
   d->diff_valid = false;
   d->data = d_data;
   d->data_len = len;
@@ -447,7 +460,6 @@ int prepare_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, bool make
   if (baseline) {
     int rc = map_reset(d, map_capacity(2ull * d->N, d->map_max_load, d->map_headroom));
     if (rc) return rc;
-    d->have_tree = true;
     d->baseline_id = d->current_id;
     // the list approach starts a baseline from an all-zero digest list (src/list_approach.cpp:865-869)
     if (d->list) B2D_CU(cudaMemsetAsync(d->tree.p + (d->n - 1u), 0, sizeof(Digest) * (size_t)d->n, d->stream));
@@ -592,6 +604,8 @@ int finish_checkpoint(b2d_dedup* d, bool advance, bool timing) {
   int rc = status_code(st.status);
   d->map_size_host = st.meta.map_size;
   if (rc) {
+    // the tree and the map may be part-way updated: the next checkpoint must be a baseline
+    d->have_tree = false;
     // a failed checkpoint may leave region flags behind; they must be zero for the next one
     cudaMemsetAsync(d->push.p, 0, d->push.n, d->stream);
     cudaMemsetAsync(d->dupflag.p, 0, d->dupflag.n, d->stream);
@@ -606,6 +620,7 @@ int finish_checkpoint(b2d_dedup* d, bool advance, bool timing) {
   d->datasizes[0] = d->diff_len - meta_bytes;
   d->datasizes[1] = meta_bytes;
   d->diff_valid = true;
+  d->have_tree = true;
   if (advance) d->current_id += 1;
   return B2D_OK;
 }
@@ -1201,6 +1216,14 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
     for (uint32_t j = 0; j < i; j++)
       if (hs[j] == hs[i]) return B2D_ERR_ARG;   // one checkpoint per handle per batch
   }
+  // every handle's arguments before any handle is prepared: a rejected batch changes no handle
+  for (uint32_t i = 0; i < count; i++) {
+    const int vrc = check_checkpoint(hs[i], data[i], lens[i], make_baseline && make_baseline[i]);
+    if (vrc) {
+      if (rcs) rcs[i] = vrc;
+      return vrc;
+    }
+  }
   // tuning for this batch
   const bool scoring = b->autotune && !b->tuner.done;
   const BatchCand cand = scoring ? b->tuner.next() : b->cur;
@@ -1608,6 +1631,7 @@ int batch_finish(b2d_batch* b, int* rcs) {
     if (r == B2D_OK && first_rc != B2D_OK) {
       r = first_rc;
       d->diff_valid = false;
+      d->have_tree = false;   // its leaves may not have been hashed
     }
     d->phase[0] = d->phase[1] = d->phase[2] = 0;
     if (rcs) rcs[i] = r;

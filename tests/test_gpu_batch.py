@@ -150,6 +150,57 @@ def test_batch_rejects_duplicate_handles(cuda):
             b.checkpoint([h, h], [x, x])
 
 
+@pytest.mark.parametrize("baseline_first", [False, True])
+def test_rejected_batch_changes_no_handle(cuda, baseline_first):
+    """a batch whose second entry is invalid (length changed without a baseline, or empty) is
+    rejected before any handle is prepared: the first handle's next checkpoint still diffs
+    against its previous one, as the oracle does"""
+    import torch
+
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import B2DError
+
+    s0 = synth.ByteSeries(64 << 10, 128, synth.plan_plain_64m, 1, 5)
+    s1 = synth.ByteSeries(32 << 10, 128, synth.plan_plain_64m, 1, 6)
+    a = [s0.next().copy() for _ in range(2)]
+    b0 = s1.next().copy()
+    dev = lambda x: torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    h0, h1 = TreeDeduplicator(128), TreeDeduplicator(128)
+    o = O.OracleTreeDeduplicator(128)
+    assert h0.checkpoint(dev(a[0]), True) == o.checkpoint(a[0], True)
+    h1.checkpoint(dev(b0), True)
+    bad = [torch.zeros(len(b0) + 128, dtype=torch.uint8, device="cuda"),
+           torch.empty(0, dtype=torch.uint8, device="cuda")]
+    with CheckpointBatch() as batch:
+        for x, code in zip(bad, (-10, -1)):
+            rcs = batch.checkpoint([h0, h1], [dev(a[1]), x], [baseline_first, False], check_status=False)
+            assert rcs[1] == code, rcs
+            with pytest.raises(B2DError):
+                batch.checkpoint([h0, h1], [dev(a[1]), x], [baseline_first, False])
+    assert h0.checkpoint(dev(a[1]), False) == o.checkpoint(a[1], False)
+    h0.close()
+    h1.close()
+
+
+def test_empty_buffer_rejected(cuda):
+    """an empty buffer is an argument error and leaves the handle as it was"""
+    import torch
+
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import B2DError
+
+    s = synth.ByteSeries(16 << 10, 128, synth.plan_plain_64m, 1, 8)
+    bufs = [s.next().copy() for _ in range(2)]
+    h = TreeDeduplicator(128)
+    o = O.OracleTreeDeduplicator(128)
+    with pytest.raises(B2DError) as e:
+        h.checkpoint(torch.empty(0, dtype=torch.uint8, device="cuda"), True)
+    assert e.value.code == -1
+    for i, x in enumerate(bufs):
+        assert h.checkpoint(torch.from_numpy(x).cuda(), i == 0) == o.checkpoint(x, i == 0)
+        with pytest.raises(B2DError):
+            h.checkpoint(torch.empty(0, dtype=torch.uint8, device="cuda"), False)
+    h.close()
+
+
 @pytest.mark.parametrize("mode,batch_diff,batch_forest",
                          [(0, 1, 1), (1, 1, 1), (2, 1, 1), (0, 1, 0), (1, 1, 0), (0, 0, 0), (1, 0, 1)])
 def test_batch_graph_modes_same(cuda, mode, batch_diff, batch_forest):
