@@ -121,7 +121,9 @@ int b2d_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, int make_base
 int b2d_checkpoint_log(b2d_dedup* d, const void* d_data, uint64_t len, const char* logname, int make_baseline,
                        const uint8_t** diff, uint64_t* diff_len);
 /* checkpoint(uint8_t* data_ptr, size_t len, std::string& filename, std::string& logname,
- * bool make_baseline) -- src/tree_approach.cpp:1705-1724 (diff written to `filename`). */
+ * bool make_baseline) -- src/tree_approach.cpp:1705-1724 (diff written to `filename`).  If the
+ * log or the file cannot be written (B2D_ERR_IO) the checkpoint id does not advance and the
+ * handle accepts only a baseline next. */
 int b2d_checkpoint_file(b2d_dedup* d, const void* d_data, uint64_t len, const char* filename, const char* logname,
                         int make_baseline);
 

@@ -1789,14 +1789,24 @@ int b2d_checkpoint_file(b2d_dedup* d, const void* d_data, uint64_t len, const ch
     uint64_t n = 0;
     int rc = checkpoint_to_pinned(d, d_data, len, make_baseline != 0, false, &p, &n);
     if (rc) return rc;
-    if (n < 32) return B2D_ERR_FORMAT;
-    rc = write_chkpt_log(d, p, p + 32 + 4ull * d->F, logname, d->current_id);
-    if (rc) return rc;
-    FILE* f = fopen(filename, "wb");
-    if (!f) return B2D_ERR_IO;
-    const size_t w = fwrite(p, 1, n, f);
-    const int cl = fclose(f);
-    if (w != n || cl != 0) return B2D_ERR_IO;
+    // the tree and map now hold this checkpoint; if its file is not written, no later diff may
+    // reference it, so the handle then accepts only a baseline (with the same checkpoint id)
+    if (n < 32) rc = B2D_ERR_FORMAT;
+    if (!rc) rc = write_chkpt_log(d, p, p + 32 + 4ull * d->F, logname, d->current_id);
+    if (!rc) {
+      FILE* f = fopen(filename, "wb");
+      if (!f) {
+        rc = B2D_ERR_IO;
+      } else {
+        const size_t w = fwrite(p, 1, n, f);
+        const int cl = fclose(f);
+        if (w != n || cl != 0) rc = B2D_ERR_IO;
+      }
+    }
+    if (rc) {
+      d->have_tree = false;
+      return rc;
+    }
     d->current_id += 1;
     return B2D_OK;
   })

@@ -56,3 +56,35 @@ def test_dedup_and_restart_files(cuda, tmp_path, mode):
         assert len(lines) == 2
         assert lines[0].split(":", 1)[1].strip() == ref_digest_str(bufs[rid]).strip()
 
+
+
+def test_checkpoint_file_overload_and_write_failure(cuda, tmp_path):
+    """checkpoint(data, filename, logname, make_baseline) writes the oracle's diff bytes and one
+    log row per checkpoint; a diff that cannot be written (B2D_ERR_IO) does not advance the
+    checkpoint id, and the handle then takes only a baseline, which continues the id sequence"""
+    import torch
+
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import B2DError, TreeDeduplicator
+
+    s = synth.ByteSeries(256 << 10, 128, synth.plan_plain_64m, 1, 21)
+    bufs = [s.next().copy() for _ in range(3)]
+    o = O.OracleTreeDeduplicator(128)
+    want = [o.checkpoint(bufs[0], True), o.checkpoint(bufs[1], False), o.checkpoint(bufs[2], True)]
+    h = TreeDeduplicator(128)
+    log = str(tmp_path / "run")
+    files = [tmp_path / f"c{i}.hashtree.incr_chkpt" for i in range(3)]
+    dev = [torch.from_numpy(b).cuda() for b in bufs]
+    assert h.checkpoint(dev[0], True, filename=files[0], logname=log) is None
+    h.checkpoint(dev[1], False, filename=files[1], logname=log)
+    with pytest.raises(B2DError) as e:
+        h.checkpoint(dev[2], False, filename=tmp_path / "missing" / "c2", logname=log)
+    assert e.value.code == -5
+    with pytest.raises(B2DError) as e:
+        h.checkpoint(dev[2], False, filename=files[2], logname=log)
+    assert e.value.code == -10
+    h.checkpoint(dev[2], True, filename=files[2], logname=log)
+    assert [f.read_bytes() for f in files] == want
+    with open(log + ".chunk_size.128.csv") as f:
+        rows = f.read().splitlines()
+    assert rows[0].startswith("Approach,Chkpt ID") and [r.split(",")[1] for r in rows[1:]] == ["0", "1", "2", "2"]
+    h.close()
