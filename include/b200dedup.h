@@ -48,7 +48,9 @@ enum b2d_status {
   B2D_ERR_LEN_CHANGED = -10,   /* buffer length changed without make_baseline, or the handle
                                   holds no complete checkpoint (after a failed one) and this
                                   one is not a baseline */
-  B2D_ERR_UNSUPPORTED = -11    /* outside the supported range (e.g. > 8192 checkpoints per baseline) */
+  B2D_ERR_UNSUPPORTED = -11    /* outside the supported range: checkpoint ids (which, as in the
+                                  reference, keep counting across baselines) up to 8190 per
+                                  handle; a longer run continues on a new handle */
 };
 
 enum b2d_hash_kind {
