@@ -106,3 +106,16 @@ def test_server_rejects_unknown_approach():
 
     with pytest.raises(ValueError):
         CheckpointServer(approach="full")
+
+
+def test_status_codes_match_header():
+    """the Python status table names every code the C header declares, and the library has a
+    message for each"""
+    with open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include",
+                           "b200dedup.h")) as f:
+        text = f.read()
+    declared = {int(v): k for k, v in re.findall(r"\b(B2D_(?:OK|ERR_\w+))\s*=\s*(-?\d+)", text)}
+    assert declared == _lib.STATUS
+    L = _lib.lib()
+    msgs = {code: L.b2d_strerror(code) for code in declared}
+    assert all(msgs.values()) and len(set(msgs.values())) == len(msgs)
