@@ -232,7 +232,9 @@ def test_tree_oracle_matches_independent_model(seed, steps, rebase):
 
 
 def test_model_matches_reference_test_case_counts():
-    """the model itself against the reference's own expectations (test/test_case_*.cpp)"""
+    """the model itself against the reference's own expectations (test/test_case_*.cpp: the
+    first-occurrence and shifted-duplicate region counts of the second checkpoint), and against
+    the committed diffs of those cases"""
     import json
     import os
 
@@ -242,4 +244,6 @@ def test_model_matches_reference_test_case_counts():
         m = PyTreeModel(1, O.HASH_MURMUR3)
         d0 = m.checkpoint(c["step0"].encode(), True)
         d1 = m.checkpoint(c["step1"].encode(), False)
+        F, S = struct.unpack("<II", d1[16:20] + d1[28:32])
+        assert (F, S) == (c["first"], c["shift"]), name
         assert d0.hex() == c["diff0"] and d1.hex() == c["diff1"], name
