@@ -244,6 +244,6 @@ def test_model_matches_reference_test_case_counts():
         m = PyTreeModel(1, O.HASH_MURMUR3)
         d0 = m.checkpoint(c["step0"].encode(), True)
         d1 = m.checkpoint(c["step1"].encode(), False)
-        F, S = struct.unpack("<II", d1[16:20] + d1[28:32])
+        F, S = struct.unpack("<II", d1[20:24] + d1[28:32])
         assert (F, S) == (c["first"], c["shift"]), name
         assert d0.hex() == c["diff0"] and d1.hex() == c["diff1"], name
