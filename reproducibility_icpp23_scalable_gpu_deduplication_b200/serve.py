@@ -24,7 +24,7 @@ request's diff is exactly what its client's handle gives when it checkpoints the
 alone, one request at a time.
 
 ``plain=True`` serves the same requests the drop-in way instead: one request at a time, in
-arrival order, each through ``TreeDeduplicator.checkpoint_device``.
+arrival order, each through its client's handle (``checkpoint_device``).
 """
 import collections
 import time
