@@ -21,7 +21,11 @@ clients submit "checkpoint my device buffer now" requests as they arrive.  The l
 
 A client has at most one request in flight; its later requests wait in arrival order.  Each
 request's diff is exactly what its client's handle gives when it checkpoints the same buffers
-alone, one request at a time.
+alone, one request at a time.  A request is taken as a baseline (``Request.baseline``) when
+its client asks for one, when it is the client's first on its handle, when its buffer length
+differs from the client's previous request (the handle takes a new length only as a baseline)
+and after a failed request of the client (its tree and map may be part-way updated); so one
+client's bad request never fails a batch that other clients' requests share.
 
 ``plain=True`` serves the same requests the drop-in way instead: one request at a time, in
 arrival order, each through its client's handle (``checkpoint_device``).
@@ -38,7 +42,7 @@ __all__ = ["CheckpointServer", "Request"]
 
 class Request:
     __slots__ = ("client", "buffer", "nbytes", "make_baseline", "arrival", "admitted", "launched", "done", "rc",
-                 "diff_len", "checksum", "ready", "seq", "host", "launch_s", "batch_size")
+                 "diff_len", "checksum", "ready", "seq", "host", "launch_s", "batch_size", "baseline")
 
     def __init__(self, client, buffer, make_baseline, arrival, seq):
         self.client, self.buffer, self.make_baseline, self.arrival, self.seq = client, buffer, make_baseline, arrival, seq
@@ -51,6 +55,7 @@ class Request:
         self.host = None          # the diff in pinned host memory (with enable_host_copy)
         self.launch_s = None      # host seconds its batch's launch call took
         self.batch_size = 1
+        self.baseline = None      # whether it ran as a baseline (set at launch)
 
     @property
     def latency(self):
@@ -58,7 +63,7 @@ class Request:
 
 
 class _Client:
-    __slots__ = ("handle", "reserved", "last_use", "busy", "pending", "outstanding", "host")
+    __slots__ = ("handle", "reserved", "last_use", "busy", "pending", "outstanding", "host", "nbytes", "rebase")
 
     def __init__(self):
         self.handle = None
@@ -68,6 +73,8 @@ class _Client:
         self.pending = collections.deque()   # admitted, not launched
         self.outstanding = 0                 # submitted, not completed
         self.host = None                     # pinned buffer for diff copy-back
+        self.nbytes = None                   # buffer length of the last launched request
+        self.rebase = False                  # the next request runs as a baseline
 
 
 class CheckpointServer:
@@ -112,6 +119,8 @@ class CheckpointServer:
         import torch
 
         r = Request(client, buffer, bool(make_baseline), self.clock() if arrival is None else arrival, self.seq)
+        if r.nbytes == 0:
+            raise ValueError("an empty buffer cannot be checkpointed")
         self.seq += 1
         r.ready = torch.cuda.Event()
         r.ready.record(torch.cuda.current_stream())
@@ -181,6 +190,7 @@ class CheckpointServer:
             c = self.clients[cid]
             c.handle.close()
             c.handle = None
+            c.nbytes = None
             self.resident -= c.reserved
             c.reserved = 0
 
@@ -202,6 +212,7 @@ class CheckpointServer:
                 continue
             if c.handle is None:
                 c.handle = self.Dedup(self.cs, self.kind)
+                c.rebase = True         # a handle's first checkpoint is its baseline
                 c.reserved = need
                 self.resident += need
                 self.peak_resident = max(self.peak_resident, self.resident)
@@ -220,12 +231,12 @@ class CheckpointServer:
             batch = [self.clients[cid].pending.popleft() for _, cid in heads[:self.max_batch]]
             for r in batch:
                 stream.wait_event(r.ready)
-                self.clients[r.client].busy = True
+                self._take(self.clients[r.client], r)
             now = self.clock()
             for r in batch:
                 r.launched = now
             b.launch([self.clients[r.client].handle for r in batch], [r.buffer for r in batch],
-                     [r.make_baseline for r in batch], stream=stream)
+                     [r.baseline for r in batch], stream=stream)
             host = self.clock() - now
             for r in batch:
                 r.launch_s = host
@@ -233,9 +244,16 @@ class CheckpointServer:
             reqs.extend(batch)
             self.batches += 1
 
+    def _take(self, c, r):
+        """`r` is about to run on its client's handle: decide whether it runs as a baseline"""
+        r.baseline = r.make_baseline or c.rebase or (c.nbytes is not None and c.nbytes != r.nbytes)
+        c.nbytes, c.rebase, c.busy = r.nbytes, False, True
+
     def _finish(self, r, rc):
         c = self.clients[r.client]
         r.rc = rc
+        if rc != 0:
+            c.rebase = True
         if rc == 0:
             r.diff_len = c.handle.diff_device()[1]
             if self.checksum:
@@ -317,9 +335,10 @@ class CheckpointServer:
         c.pending.popleft()
         nxt.launched = self.clock()
         nxt.ready.synchronize()
+        self._take(c, nxt)
         rc = 0
         try:
-            c.handle.checkpoint_device(nxt.buffer, nxt.make_baseline)
+            c.handle.checkpoint_device(nxt.buffer, nxt.baseline)
         except Exception as e:   # noqa: BLE001 - the status travels with the request
             rc = getattr(e, "code", -8)
         if rc == 0 and self.to_host:

@@ -213,3 +213,61 @@ def test_percentile():
     assert serve.percentile([1, 2, 3, 4], 0) == 1
     assert serve.percentile([0, 10], 25) == 2.5
     assert serve.percentile([], 50) is None
+
+
+class FailingBatch(FakeBatch):
+    """reports a device failure for the handles in `fail` (once each)"""
+    fail = set()
+
+    def launch(self, handles, buffers, make_baseline=None, stream=None):
+        LOG["launch_flags"].append([(h, bool(mb)) for h, mb in zip(handles, make_baseline)])
+        self.handles = list(handles)
+        super().launch(handles, buffers, make_baseline, stream)
+
+    def wait(self, check_status=True):
+        rcs = super().wait(check_status)
+        for i, h in enumerate(self.handles):
+            if h in self.fail:
+                self.fail.discard(h)
+                rcs[i] = -7
+        return rcs
+
+
+def flags_of(log, handle):
+    return [mb for batch in log["launch_flags"] for h, mb in batch if h is handle]
+
+
+def test_baselines_chosen_by_the_loop(fakes, monkeypatch):
+    """first request on a handle, a length change, a client's request and a failed request each
+    make the client's next (or own) checkpoint a baseline; everything else is incremental"""
+    monkeypatch.setattr(serve, "CheckpointBatch", FailingBatch)
+    srv = serve.CheckpointServer(hbm_budget=10_000, max_batch=4)
+    buf = lambda n, v=0: torch.full((n,), v, dtype=torch.uint8)
+    srv.submit(0, buf(64))
+    srv.submit(1, buf(64))
+    srv.drain()
+    h0, h1 = srv.clients[0].handle, srv.clients[1].handle
+    FailingBatch.fail = {h1}
+    srv.submit(0, buf(64, 1))                   # incremental
+    srv.submit(1, buf(64, 1))                   # fails on the device
+    srv.drain()
+    srv.submit(0, buf(128))                     # length change
+    srv.submit(1, buf(64, 2))                   # after a failure
+    srv.drain()
+    srv.submit(0, buf(128, 3), make_baseline=True)
+    srv.submit(1, buf(64, 3))
+    srv.drain()
+    assert flags_of(fakes, h0) == [True, False, True, True]
+    assert flags_of(fakes, h1) == [True, False, True, False]
+    rcs = [r.rc for r in srv.completed]
+    assert rcs.count(-7) == 1 and rcs.count(0) == len(rcs) - 1
+    assert [r.baseline for r in srv.completed if r.client == 1] == [True, False, True, False]
+    srv.close()
+
+
+def test_empty_buffer_rejected_at_submit(fakes):
+    srv = serve.CheckpointServer(hbm_budget=10_000)
+    with pytest.raises(ValueError):
+        srv.submit(0, torch.empty(0, dtype=torch.uint8))
+    assert srv.idle() and not srv.busy(0)
+    srv.close()
