@@ -39,6 +39,10 @@ from .tree import ListDeduplicator, TreeDeduplicator, estimate_memory, reserve_m
 
 __all__ = ["CheckpointServer", "Request"]
 
+# a handle's checkpoint ids run 0..8190 (they keep counting across baselines; the digest map
+# stores them in 13 bits): a client that reaches the end continues on a new handle
+MAX_CHECKPOINTS_PER_HANDLE = 8191
+
 
 class Request:
     __slots__ = ("client", "buffer", "nbytes", "make_baseline", "arrival", "admitted", "launched", "done", "rc",
@@ -63,7 +67,8 @@ class Request:
 
 
 class _Client:
-    __slots__ = ("handle", "reserved", "last_use", "busy", "pending", "outstanding", "host", "nbytes", "rebase")
+    __slots__ = ("handle", "reserved", "last_use", "busy", "pending", "outstanding", "host", "nbytes", "rebase",
+                 "taken")
 
     def __init__(self):
         self.handle = None
@@ -75,6 +80,7 @@ class _Client:
         self.host = None                     # pinned buffer for diff copy-back
         self.nbytes = None                   # buffer length of the last launched request
         self.rebase = False                  # the next request runs as a baseline
+        self.taken = 0                       # checkpoints launched on the current handle
 
 
 class CheckpointServer:
@@ -213,6 +219,7 @@ class CheckpointServer:
             if c.handle is None:
                 c.handle = self.Dedup(self.cs, self.kind)
                 c.rebase = True         # a handle's first checkpoint is its baseline
+                c.taken = 0
                 c.reserved = need
                 self.resident += need
                 self.peak_resident = max(self.peak_resident, self.resident)
@@ -246,8 +253,13 @@ class CheckpointServer:
 
     def _take(self, c, r):
         """`r` is about to run on its client's handle: decide whether it runs as a baseline"""
+        if c.taken >= MAX_CHECKPOINTS_PER_HANDLE:
+            c.handle.close()
+            c.handle = self.Dedup(self.cs, self.kind)
+            c.taken, c.rebase = 0, True
         r.baseline = r.make_baseline or c.rebase or (c.nbytes is not None and c.nbytes != r.nbytes)
         c.nbytes, c.rebase, c.busy = r.nbytes, False, True
+        c.taken += 1
 
     def _finish(self, r, rc):
         c = self.clients[r.client]

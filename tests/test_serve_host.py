@@ -271,3 +271,21 @@ def test_empty_buffer_rejected_at_submit(fakes):
         srv.submit(0, torch.empty(0, dtype=torch.uint8))
     assert srv.idle() and not srv.busy(0)
     srv.close()
+
+
+def test_client_moves_to_a_new_handle_at_the_id_limit(fakes, monkeypatch):
+    """a client that has used up a handle's checkpoint ids continues on a new handle, starting
+    with a baseline; the old handle is closed"""
+    monkeypatch.setattr(serve, "MAX_CHECKPOINTS_PER_HANDLE", 3)
+    monkeypatch.setattr(serve, "CheckpointBatch", FailingBatch)
+    FailingBatch.fail = set()
+    srv = serve.CheckpointServer(hbm_budget=10_000)
+    for k in range(7):
+        srv.submit(0, torch.full((64,), k, dtype=torch.uint8))
+        srv.drain()
+    hs = fakes["created"]
+    assert len(hs) == 3 and hs[0].closed and hs[1].closed and not hs[2].closed
+    assert [h.count for h in hs] == [3, 3, 1]
+    assert [r.baseline for r in srv.completed] == [True, False, False, True, False, False, True]
+    assert all(r.rc == 0 for r in srv.completed)
+    srv.close()
