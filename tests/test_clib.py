@@ -119,3 +119,21 @@ def test_status_codes_match_header():
     L = _lib.lib()
     msgs = {code: L.b2d_strerror(code) for code in declared}
     assert all(msgs.values()) and len(set(msgs.values())) == len(msgs)
+
+
+@pytest.mark.skipif(__import__("torch").cuda.is_available(), reason="checks the behaviour without a GPU")
+def test_no_cpu_fallback_without_gpu():
+    """without a CUDA device every entry point fails loudly: handles and batches cannot be
+    created, and host tensors are refused before any call"""
+    import torch
+
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import (B2DError, CheckpointBatch, ListDeduplicator,
+                                                                        TreeDeduplicator)
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200.tree import hash_chunks
+
+    for make in (lambda: TreeDeduplicator(128), lambda: ListDeduplicator(128), lambda: CheckpointBatch()):
+        with pytest.raises(B2DError) as e:
+            make()
+        assert e.value.code == -2
+    with pytest.raises(TypeError):
+        hash_chunks(torch.zeros(256, dtype=torch.uint8), 128)
