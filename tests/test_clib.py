@@ -137,3 +137,25 @@ def test_no_cpu_fallback_without_gpu():
         assert e.value.code == -2
     with pytest.raises(TypeError):
         hash_chunks(torch.zeros(256, dtype=torch.uint8), 128)
+
+
+def test_header_is_plain_c(tmp_path):
+    """include/b200dedup.h compiles as C99 and C11 with warnings as errors, and a C program that
+    takes the address of every declared entry point links against the library"""
+    _build.build()
+    syms = header_symbols()
+    src = tmp_path / "abi.c"
+    src.write_text('#include "b200dedup.h"\n#include <stdio.h>\n'
+                   "typedef void (*fp)(void);\n"
+                   "int main(void) {\n  fp table[] = {\n"
+                   + "".join(f"    (fp){s},\n" for s in syms)
+                   + "  };\n  printf(\"%d %s\\n\", (int)(sizeof table / sizeof table[0]), b2d_strerror(0));\n"
+                   "  return 0;\n}\n")
+    pkg = os.path.dirname(_build.LIB_PATH)
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    for std in ("c99", "c11"):
+        exe = tmp_path / f"abi_{std}"
+        subprocess.run(["gcc", f"-std={std}", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", inc, str(src),
+                        "-o", str(exe), "-L", pkg, "-lb200dedup", f"-Wl,-rpath,{pkg}"], check=True)
+        out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
+        assert out == [str(len(syms)), "ok"]
