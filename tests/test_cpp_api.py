@@ -57,3 +57,16 @@ def test_cpp_list_chkpt(cuda, cs):
 def test_cpp_checkpoint_batch(cuda):
     r = subprocess.run([build_cpp(), "batch", "9"], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
+
+
+def test_cpp_sources_warning_free(tmp_path):
+    """the C++ mirror, the ported reference tests and the file tools compile with -Wall -Wextra
+    as errors (the mirror also with -pedantic)"""
+    inc = ["-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include"]
+    hdr = tmp_path / "hdr.cpp"
+    hdr.write_text('#include "b200dedup_tree.hpp"\nint main() { return 0; }\n')
+    base = ["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-fsyntax-only"] + inc
+    subprocess.run(base + ["-pedantic", str(hdr)], check=True)
+    cli = os.path.join(ROOT, "reproducibility_icpp23_scalable_gpu_deduplication_b200", "cli")
+    for src in [SRC] + sorted(os.path.join(cli, f) for f in os.listdir(cli) if f.endswith(".cpp")):
+        subprocess.run(base + [src], check=True)
