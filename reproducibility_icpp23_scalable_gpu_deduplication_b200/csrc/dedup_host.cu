@@ -525,7 +525,7 @@ DiffArgs diff_args(b2d_dedup* d, const RoundState* rs_dev) {
   return DiffArgs{static_cast<const uint8_t*>(d->data), d->data_len, d->chunk_size, d->n, d->N, d->D, 0, 0,
                   d->tree.p, d->push.p, m, &ds->status, &ds->meta, d->first_list.p, d->shift_list.p, d->tmp_first.p,
                   d->tmp_shift.p, d->levels.p, d->region_off.p, d->sprev.p, d->skey.p, d->hist.p, d->bucket_start.p,
-                  d->partial.p, d->partial2.p, d->diff.p, rs_dev};
+                  d->partial.p, d->partial2.p, d->diff.p, rs_dev, 0u};
 }
 
 ForestArgs forest_args(b2d_dedup* d, const RoundState* rs_dev) {
