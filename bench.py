@@ -45,7 +45,7 @@ def parse():
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--workload", default="plain_4g", choices=["plain_4g", "md5_f32_8g", "plain_64m"],
                    help="plain form: the 4 GiB Murmur3 series (default), the 8 GiB float32 MD5 series, or "
-                        "the 64 MiB CPU-runnable series (5% rewritten, 2% shifted, 1% zeroed per checkpoint)")
+                        "the 64 MiB CPU-runnable series (5%% rewritten, 2%% shifted, 1%% zeroed per checkpoint)")
     p.add_argument("--chunk-size", type=int, default=None, help="default 128 (plain_4g) / 256 (md5_f32_8g)")
     p.add_argument("--approach", default="tree", choices=["tree", "list"],
                    help="the tree approach (default) or the list approach (ListDeduplicator), in every "

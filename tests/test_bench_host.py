@@ -68,3 +68,11 @@ def test_reference_arm_other_ranks_exit_quietly():
                        timeout=300)
     assert r.returncode == 0, r.stderr
     assert r.stdout.strip() == ""
+
+
+def test_help_lists_every_option():
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--help"], capture_output=True, text=True,
+                       cwd=ROOT, timeout=120)
+    assert r.returncode == 0, r.stderr
+    for opt in ("--gpus", "--steps", "--warmup", "--impl", "--form", "--approach", "--workload"):
+        assert opt in r.stdout, opt
