@@ -242,8 +242,18 @@ class CheckpointServer:
             now = self.clock()
             for r in batch:
                 r.launched = now
-            b.launch([self.clients[r.client].handle for r in batch], [r.buffer for r in batch],
-                     [r.baseline for r in batch], stream=stream)
+            try:
+                b.launch([self.clients[r.client].handle for r in batch], [r.buffer for r in batch],
+                         [r.baseline for r in batch], stream=stream)
+            except Exception as e:   # noqa: BLE001 - the status travels with the requests
+                # nothing of the batch runs: its requests complete now with the error, and
+                # their clients' next requests are baselines
+                done = self.clock()
+                for r in batch:
+                    r.done = done
+                    self._finish(r, getattr(e, "code", -8))
+                self.batches += 1
+                continue
             host = self.clock() - now
             for r in batch:
                 r.launch_s = host

@@ -289,3 +289,39 @@ def test_client_moves_to_a_new_handle_at_the_id_limit(fakes, monkeypatch):
     assert [r.baseline for r in srv.completed] == [True, False, False, True, False, False, True]
     assert all(r.rc == 0 for r in srv.completed)
     srv.close()
+
+
+class RaisingBatch(FakeBatch):
+    """a launch that fails as a whole (as a CUDA error at launch would)"""
+    raise_for = set()
+
+    def launch(self, handles, buffers, make_baseline=None, stream=None):
+        LOG["launch_flags"].append([(h, bool(mb)) for h, mb in zip(handles, make_baseline)])
+        if any(h in self.raise_for for h in handles):
+            self.raise_for.clear()
+            err = RuntimeError("launch failed")
+            err.code = -2
+            raise err
+        super().launch(handles, buffers, make_baseline, stream)
+
+
+def test_failed_launch_completes_its_requests(fakes, monkeypatch):
+    """a batch whose launch raises completes its requests with the error code; the loop keeps
+    serving, and those clients' next requests are baselines"""
+    monkeypatch.setattr(serve, "CheckpointBatch", RaisingBatch)
+    srv = serve.CheckpointServer(hbm_budget=10_000, max_batch=4)
+    buf = lambda v: torch.full((64,), v, dtype=torch.uint8)
+    for c in range(2):
+        srv.submit(c, buf(0))
+    srv.drain()
+    h0, h1 = srv.clients[0].handle, srv.clients[1].handle
+    RaisingBatch.raise_for = {h0}
+    r = [srv.submit(c, buf(1)) for c in range(2)]
+    srv.drain()
+    assert [x.rc for x in r] == [-2, -2] and all(x.done is not None for x in r)
+    assert not srv.busy(0) and not srv.busy(1)
+    r2 = [srv.submit(c, buf(2)) for c in range(2)]
+    srv.drain()
+    assert [x.rc for x in r2] == [0, 0] and [x.baseline for x in r2] == [True, True]
+    assert flags_of(fakes, h0) == [True, False, True] and flags_of(fakes, h1) == [True, False, True]
+    srv.close()
