@@ -15,7 +15,8 @@ in HBM (each step's buffer is materialised before the timed region; 4 GiB > L2, 
              copy of the step's buffer, checkpoint, diff copied back to pinned host memory
 `roofline` : the dominant kernel (chunk hashing + labelling) against measured HBM bandwidth
 `cpu_baseline` / --impl reference: the CPU restatement of the reference algorithm (oracle/),
-             OpenMP-parallel hashing with all host threads, on a bounded sample of the workload
+             OpenMP-parallel hashing with all host threads, on the workload's full buffer: an
+             untimed baseline and warm-up checkpoints, then timed incremental checkpoints
 
 Multi-GPU (torchrun): every rank deduplicates its own buffer (independent replicas, like the
 reference's MPI driver); nothing crosses ranks but the barrier and the max-time reduction.
@@ -52,7 +53,10 @@ def parse():
                         "form and in the reference arm")
     p.add_argument("--nbytes", type=int, default=None, help="default 4 GiB (plain_4g) / 8 GiB (md5_f32_8g)")
     p.add_argument("--e2e-steps", type=int, default=2)
-    p.add_argument("--cpu-sample-bytes", type=int, default=512 << 20)
+    p.add_argument("--cpu-sample-bytes", type=int, default=0,
+                   help="CPU baseline buffer size (0 = the workload's full size)")
+    p.add_argument("--cpu-steps", type=int, default=3,
+                   help="timed incremental checkpoints of the cpu_baseline leg (after a baseline and one warm-up)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--leaf-stages", type=int, default=0, help="TMA ring depth (0 = library default)")
     p.add_argument("--leaf-ctas", type=int, default=0, help="hashing CTAs per SM (0 = library default)")
@@ -155,22 +159,41 @@ def workload_series(workload, nbytes, cs, device, seed):
     return synth.plain_4g(nbytes=nbytes, chunk_size=cs, device=device, seed=seed)
 
 
-def cpu_baseline_run(nbytes, cs, steps, threads, workload="plain_4g", approach="tree"):
-    """The oracle (sequential restatement of the reference) on the host, all threads hashing."""
+def cpu_baseline_run(nbytes, cs, steps, threads, workload="plain_4g", approach="tree", warmup=1, device=None):
+    """The oracle (sequential restatement of the reference) on the host, all threads hashing.
+
+    One definition for every CPU figure: an untimed baseline, `warmup` untimed incremental
+    checkpoints, then `steps` timed incremental checkpoints of the same series; returns (ingest
+    GB/s over the timed checkpoints, their seconds).  With `device` the series' bytes are generated
+    there and copied to host memory before each checkpoint (same bytes for the byte workloads,
+    faster than generating 4 GiB with numpy); only the oracle's checkpoint calls are timed."""
     from oracle import oracle as O
     from reproducibility_icpp23_scalable_gpu_deduplication_b200 import synth
 
-    s = workload_series(workload, nbytes, cs, None, synth.SEED)
+    s = workload_series(workload, nbytes, cs, device, synth.SEED)
+
+    def host_next():
+        b = s.next()
+        return b if device is None else b.view(-1).cpu().numpy()
+
     cls = O.OracleListDeduplicator if approach == "list" else O.OracleTreeDeduplicator
     o = cls(cs, O.HASH_MD5 if workload == "md5_f32_8g" else O.HASH_MURMUR3, threads=threads)
-    o.checkpoint(s.next(), True)
+    o.checkpoint(host_next(), True)
+    for _ in range(max(0, warmup)):
+        o.checkpoint(host_next(), False)
     t = 0.0
     for _ in range(steps):
-        b = s.next()
+        b = host_next()
         t0 = time.perf_counter()
         o.checkpoint(b, False)
         t += time.perf_counter() - t0
+    o.close()
     return steps * nbytes / t / GB, t
+
+
+def cpu_sample_text(nbytes, workload, cs, warmup, steps):
+    return (f"{nbytes / 2**30:g} GiB buffer of the {workload} series, chunk {cs} B: an untimed baseline and "
+            f"{warmup} untimed incremental checkpoint(s), then the mean of {steps} timed incremental checkpoints")
 
 
 def leaf_traffic(cs):
@@ -190,17 +213,17 @@ def run_reference(args, rank):
         return
     threads = os.cpu_count() or 1
     steps = max(1, args.steps)
-    gbps, t = cpu_baseline_run(args.cpu_sample_bytes, args.chunk_size, steps, threads, args.workload, args.approach)
-    sample = (f"{args.cpu_sample_bytes >> 20} MiB buffer with the {args.workload} workload's change pattern, "
-              f"chunk {args.chunk_size} B, {steps} incremental checkpoints after an untimed baseline")
+    warm = max(1, args.warmup)
+    nbytes = args.cpu_sample_bytes or args.nbytes
+    gbps, t = cpu_baseline_run(nbytes, args.chunk_size, steps, threads, args.workload, args.approach, warmup=warm)
     line = {
         "impl": "reference", "metric": f"{args.approach}-dedup ingest GB/s", "value": round(gbps, 4), "unit": "GB/s",
-        "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "ms_per_step": round(1e3 * t / steps, 3),
+        "n_gpus": args.gpus, "steps": steps, "warmup": warm, "ms_per_step": round(1e3 * t / steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-        "config": {"workload": args.workload, "nbytes": args.nbytes, "chunk_size": args.chunk_size,
+        "config": {"workload": args.workload, "nbytes": nbytes, "chunk_size": args.chunk_size,
                    "hash": "md5" if args.workload == "md5_f32_8g" else "murmur3", "approach": args.approach},
         "cpu_baseline": {"value": round(gbps, 4), "unit": "GB/s", "cores": threads, "kind": "port",
-                         "sample": sample},
+                         "sample": cpu_sample_text(nbytes, args.workload, args.chunk_size, warm, steps)},
         "e2e": {"value": round(gbps, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -708,10 +731,12 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        gbps, _ = cpu_baseline_run(args.cpu_sample_bytes, cs, 2, threads, args.workload, args.approach)
+        cpu_bytes = args.cpu_sample_bytes or nbytes
+        torch.cuda.empty_cache()
+        gbps, _ = cpu_baseline_run(cpu_bytes, cs, args.cpu_steps, threads, args.workload, args.approach,
+                                   warmup=1, device=dev)
         line["cpu_baseline"] = {"value": round(gbps, 4), "unit": "GB/s", "cores": threads, "kind": "port",
-                                "sample": f"{args.cpu_sample_bytes >> 20} MiB buffer with this workload's change "
-                                          f"pattern, 2 incremental checkpoints after a baseline"}
+                                "sample": cpu_sample_text(cpu_bytes, args.workload, cs, 1, args.cpu_steps)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     dd.close()

@@ -316,7 +316,11 @@ int oracle_list_checkpoint(oracle_list* d, const uint8_t* data, uint64_t len, in
     d->list = l;
     d->list_len = nc;
   }
-  if (lmap_reserve(&d->map, d->map.size + nc)) return ORACLE_ERR_NOMEM;
+  /* reserve for this checkpoint (size + chunks) and, on a baseline, also for the next one, so the
+     first incremental checkpoint does not rehash every entry; capacity changes no output */
+  uint64_t want = d->map.size + nc;
+  if ((d->current_id == 0 || make_baseline) && want < 2 * nc) want = 2 * nc;
+  if (lmap_reserve(&d->map, want)) return ORACLE_ERR_NOMEM;
   if (d->current_id == 0 || make_baseline) d->baseline_id = d->current_id;
   int rc = list_dedup(d, data, len);
   if (rc < 0) return rc;

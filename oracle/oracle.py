@@ -84,6 +84,14 @@ def _ptr(a):
     return ctypes.c_void_p(a.ctypes.data) if a.size else ctypes.c_void_p(0)
 
 
+def _take_bytes(p, n):
+    """`n` bytes at `p` as bytes (ctypes.string_at takes a C int length: 4 GiB diffs would be cut
+    to their size modulo 2^32), then the oracle's buffer is freed"""
+    out = np.ctypeslib.as_array(p, shape=(n,)).tobytes() if n else b""
+    lib().oracle_free(p)
+    return out
+
+
 def hash_bytes(data, kind=HASH_MURMUR3):
     a = np.ascontiguousarray(np.frombuffer(bytes(data), dtype=np.uint8)) if not isinstance(data, np.ndarray) else np.ascontiguousarray(data, dtype=np.uint8)
     out = np.zeros(16, np.uint8)
@@ -129,8 +137,7 @@ class OracleTreeDeduplicator:
         rc = lib().oracle_checkpoint(self._h, _ptr(a), a.size, int(bool(make_baseline)), ctypes.byref(out), ctypes.byref(n))
         if rc < 0:
             raise RuntimeError(f"oracle checkpoint failed: {rc}")
-        diff = ctypes.string_at(out, n.value)
-        lib().oracle_free(out)
+        diff = _take_bytes(out, n.value)
         self.last_rc = rc
         return diff
 
@@ -199,8 +206,7 @@ class OracleListDeduplicator:
                                           ctypes.byref(n))
         if rc < 0:
             raise RuntimeError(f"oracle list checkpoint failed: {rc}")
-        diff = ctypes.string_at(out, n.value)
-        lib().oracle_free(out)
+        diff = _take_bytes(out, n.value)
         self.last_rc = rc
         return diff
 
@@ -220,8 +226,18 @@ class OracleListDeduplicator:
         return out[0], out[1]
 
 
+def _as_u8(d):
+    """a diff as a contiguous uint8 array, without a copy when it already is one (the oracle only
+    reads it; full-size diffs are gigabytes)"""
+    if isinstance(d, np.ndarray) and d.dtype == np.uint8 and d.flags.c_contiguous:
+        return d.reshape(-1)
+    if isinstance(d, (bytes, bytearray)):
+        return np.frombuffer(d, dtype=np.uint8)
+    return np.frombuffer(bytes(d), dtype=np.uint8)
+
+
 def _restart(fn, diffs, chkpt_idx, out_len, init):
-    bufs = [np.frombuffer(bytes(d), dtype=np.uint8).copy() for d in diffs]
+    bufs = [_as_u8(d) for d in diffs]
     if out_len is None:
         out_len = int(np.frombuffer(bufs[chkpt_idx][8:16].tobytes(), np.uint64)[0])
     out = np.zeros(out_len, np.uint8) if init is None else np.array(init, dtype=np.uint8).copy()
@@ -240,16 +256,7 @@ def list_restart(diffs, chkpt_idx, out_len=None, init=None):
 
 def restart(diffs, chkpt_idx, out_len=None, init=None):
     """Host-view restart (src/tree_approach.cpp:712-1128). Returns (buffer, rc)."""
-    bufs = [np.frombuffer(bytes(d), dtype=np.uint8).copy() for d in diffs]
-    if out_len is None:
-        out_len = int(np.frombuffer(bufs[chkpt_idx][8:16].tobytes(), np.uint64)[0])
-    out = np.zeros(out_len, np.uint8) if init is None else np.array(init, dtype=np.uint8).copy()
-    ptrs = (ctypes.c_void_p * len(bufs))(*[b.ctypes.data for b in bufs])
-    sizes = (ctypes.c_uint64 * len(bufs))(*[b.size for b in bufs])
-    rc = lib().oracle_restart(ptrs, sizes, len(bufs), chkpt_idx, _ptr(out), out_len)
-    if rc < 0:
-        raise RuntimeError(f"oracle restart failed: {rc}")
-    return out, rc
+    return _restart(lib().oracle_restart, diffs, chkpt_idx, out_len, init)
 
 
 def ref_hash_lib():

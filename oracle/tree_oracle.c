@@ -571,7 +571,13 @@ int oracle_checkpoint(oracle_dedup* d, const uint8_t* data, uint64_t len, int ma
   } else if (d->tree_nodes != d->num_nodes) {
     return ORACLE_ERR_ARG;   /* a shrinking buffer makes the reference read past the input */
   }
-  if (dmap_rehash(&d->map, d->map.size + d->num_nodes)) return ORACLE_ERR_NOMEM;
+  /* the reference reserves size + num_nodes (src/tree_approach.cpp:1622-1623); a baseline also
+     reserves for the next checkpoint's rule (its own <= num_nodes entries plus num_nodes), so the
+     first incremental checkpoint after it does not rehash every entry.  The capacity of this exact
+     map changes no output. */
+  uint64_t want = d->map.size + d->num_nodes;
+  if (baseline && want < 2ull * d->num_nodes) want = 2ull * d->num_nodes;
+  if (dmap_rehash(&d->map, want)) return ORACLE_ERR_NOMEM;
   d->first_vec.n = 0; d->shift_vec.n = 0;
   if (baseline) d->baseline_id = d->current_id;
   int rc = dedup(d, data, len, baseline);

@@ -147,9 +147,10 @@ class TreeDeduplicator:
         else:
             check(lib().b2d_checkpoint(self._h, p, n, int(bool(make_baseline)), ctypes.byref(dptr),
                                        ctypes.byref(dlen)), "b2d_checkpoint")
-        if copy:
-            return ctypes.string_at(dptr, dlen.value)
         view = np.ctypeslib.as_array(dptr, shape=(dlen.value,)) if dlen.value else np.empty(0, np.uint8)
+        if copy:
+            # not ctypes.string_at: its length is a C int, which cuts diffs of 2 GiB and more
+            return view.tobytes()
         view.flags.writeable = False
         return view
 
@@ -188,6 +189,19 @@ class TreeDeduplicator:
         if check_status:
             check(rc, "b2d_restart_files")
         return rc
+
+    # -- logs (include/deduplicator_interface.hpp:172-183)
+    def write_chkpt_log(self, header, diff, logname):
+        """write_chkpt_log(header_t&, HostMirror& diff_h, std::string& logname): the three CSV
+        logs; `header` is the diff's 32-byte header (bytes, or None to take the diff's own)."""
+        d = _host_bytes(diff)
+        hb = np.frombuffer(bytes(d[:HEADER_BYTES]) if header is None else bytes(header), dtype=np.uint8)
+        check(lib().b2d_write_chkpt_log_host(self._h, ctypes.c_void_p(hb.ctypes.data), ctypes.c_void_p(d.ctypes.data),
+                                             d.size, str(logname).encode()), "b2d_write_chkpt_log_host")
+
+    def write_restart_log(self, select_chkpt, logname):
+        """write_restart_log(uint32_t select_chkpt, std::string& logname)"""
+        check(lib().b2d_write_restart_log(self._h, int(select_chkpt), str(logname).encode()), "b2d_write_restart_log")
 
     # -- state (include/tree_approach.hpp:53-59, include/deduplicator_interface.hpp:16-23)
     def _u64(self, fn):

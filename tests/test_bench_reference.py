@@ -23,3 +23,5 @@ def test_reference_arm_line(approach):
     cb = line["cpu_baseline"]
     assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == line["value"] and cb["sample"]
     assert line["config"]["approach"] == approach
+    # the line's config names the buffer size it actually timed
+    assert line["config"]["nbytes"] == 8 << 20 and "0.0078125 GiB" in cb["sample"]

@@ -119,3 +119,19 @@ def test_baseline_shift_regions_are_single_leaves():
     d = O.OracleTreeDeduplicator(64)
     d.checkpoint(c, True)
     assert d.num_first_ocur() == 1 and d.num_shift_dupl() == 14
+
+
+def test_diffs_past_4_gib_are_whole():
+    """a baseline diff of a 4 GiB buffer holds 4 GiB of data: the oracle's bindings hand it over
+    whole (a C-int length would cut it to 36 bytes) and its restart reproduces the buffer"""
+    import psutil
+
+    nbytes, cs = 4 << 30, 1 << 16
+    if psutil.virtual_memory().available < 4 * nbytes:
+        pytest.skip("needs 16 GiB of host memory")
+    data = np.arange(nbytes // 8, dtype=np.uint64).view(np.uint8)   # every chunk distinct
+    o = O.OracleTreeDeduplicator(cs, threads=os.cpu_count() or 1)
+    diff = o.checkpoint(data, True)
+    assert len(diff) == 32 + 4 + nbytes and diff[-8:] == data[-8:].tobytes()
+    out, rc = O.restart([diff], 0)
+    assert rc == 0 and np.array_equal(out, data)
