@@ -12,15 +12,15 @@
 // Limits: at most NOALLOC_MAX_CHUNKS chunks per checkpoint and checkpoint ids below
 // NOALLOC_MAX_IDS; larger restarts are rejected with B2D_ERR_UNSUPPORTED.
 //
-// The first call on a device looks up the array's device address (cudaGetSymbolAddress) with
-// that device current; that first call should come before any stream capture.  Every call
-// shares the one array and leaves its contents behind; each call clears what must start at
-// zero.  Calls that overlap on the GPU (on different streams, or from different host threads)
-// race on the array and must be serialised by the caller.
+// Every call looks up the array's device address (cudaGetSymbolAddress) with the caller's
+// device current: the address is not cached, because a cudaDeviceReset unloads the module and
+// the array can come back elsewhere.  The first call on a device should come before any stream
+// capture.  Every call shares the one array and leaves its contents behind; each call clears
+// what must start at zero.  Calls that overlap on the GPU (on different streams, or from
+// different host threads) race on the array and must be serialised by the caller.
 #include <cuda_runtime.h>
 
 #include <cstring>
-#include <mutex>
 
 #include "../../include/b200dedup.h"
 #include "restart.cuh"
@@ -48,23 +48,13 @@ static __device__ __align__(256) unsigned char g_restart_scratch[NA_BYTES];
 
 namespace {
 
-constexpr int NA_MAX_DEVICES = 64;
-std::mutex g_na_mutex;
-unsigned char* g_na_addr[NA_MAX_DEVICES] = {nullptr};
-
-// device address of the scratch array for the current device (host code cannot use the
-// symbol itself: in host code it names a host-side stand-in)
+// device address of the scratch array on the current device (host code cannot use the symbol
+// itself: in host code it names a host-side stand-in)
 int scratch_for_current_device(unsigned char** out) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NA_MAX_DEVICES) return B2D_ERR_CUDA;
-  std::lock_guard<std::mutex> lock(g_na_mutex);
-  if (!g_na_addr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_restart_scratch);
-    if (e != cudaSuccess || p == nullptr) return B2D_ERR_CUDA;
-    g_na_addr[dev] = static_cast<unsigned char*>(p);
-  }
-  *out = g_na_addr[dev];
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_restart_scratch);
+  if (e != cudaSuccess || p == nullptr) return B2D_ERR_CUDA;
+  *out = static_cast<unsigned char*>(p);
   return B2D_OK;
 }
 
@@ -110,10 +100,24 @@ extern "C" int b2d_restart_noalloc(void* d_out, uint64_t len, const void* const*
   if (rc) return rc;
   NaHdr h;
   if ((rc = read_hdr(d_diffs[chkpt_id], sizes[chkpt_id], s, h))) return rc;
+  // diffs[i] must be checkpoint i, whose baseline is not after it (as b2d_restart checks)
+  if (h.ref_id > h.chkpt_id || h.chkpt_id != chkpt_id) return B2D_ERR_FORMAT;
   if (len < h.datalen) return B2D_ERR_ARG;
   const uint64_t nc = (h.datalen + h.cs - 1) / h.cs;
   if (nc > NOALLOC_MAX_CHUNKS) return B2D_ERR_UNSUPPORTED;
   const uint32_t n = (uint32_t)nc, N = 2u * n - 1u;
+  // every header of the chain is checked before the first launch, so a rejected call leaves
+  // the output buffer untouched
+  {
+    uint32_t ref = h.ref_id;
+    for (int idx = (int)chkpt_id; idx >= 0 && idx >= (int)ref; idx--) {
+      NaHdr hh;
+      if ((rc = read_hdr(d_diffs[idx], sizes[idx], s, hh))) return rc;
+      if (idx != (int)chkpt_id) ref = hh.ref_id;
+      if (hh.F > NOALLOC_MAX_CHUNKS || hh.S > NOALLOC_MAX_CHUNKS || (uint64_t)hh.chkpt_id + 1 > NOALLOC_MAX_IDS)
+        return B2D_ERR_UNSUPPORTED;
+    }
+  }
   int dev = 0, sm_count = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev);
