@@ -81,9 +81,12 @@ int b2d_set_stream(b2d_dedup* d, void* cuda_stream);
  *   "leaf_ctas_per_sm"  resident hashing CTAs per SM, 1..8 (0 = default 3)
  *   "leaf_unit"         staged segment width 16/32/64/128 bytes, narrower than the default only
  *                       (0 = the largest that divides the chunk; MD5 needs >= 64)
- *   "map_max_load_pct"  digest-map load limit, 10..90 (default 75): a checkpoint starts only
+ *   "leaf_wait_polls"   0 = the staged kernel's barrier waits have their normal bound
+ *                       (default); n > 0 = they give up after n non-blocking polls, so the
+ *                       checkpoint fails with B2D_ERR_TIMEOUT (a test of the give-up path)
+ *   "map_max_load_pct" digest-map load limit, 10..90 (default 75): a checkpoint starts only
  *                       when the map's entries plus every node of the tree fit under it
- *   "map_headroom_pct"  size of a baseline's map over that minimum, 100..1000 (default 200);
+ *   "map_headroom_pct"  size of a baseline's map over that minimum, 100..1000 (default 150);
  *                       more headroom = fewer growths (allocate + rehash) in a long series
  *   "graph"             0 = launch a checkpoint's kernels one by one on the handle's stream
  *                       (default; measured faster), 1 = replay them as one CUDA graph, 2 = graph
@@ -112,6 +115,20 @@ int b2d_copy_diff_async(b2d_dedup* d, void* dst, uint64_t cap, void* cuda_stream
  * asynchronously: its Write Time column is 0, the copy-back being the caller's.  The checkpoint
  * id written is the diff's.  Reads only the diff's header and repeat table from the device. */
 int b2d_write_chkpt_log(b2d_dedup* d, const char* logname);
+/* write_chkpt_log(header_t& header, HostMirror& diff_h, std::string& logname)
+ * -- include/deduplicator_interface.hpp:172-174, src/tree_approach.cpp:1853-1896 with
+ * src/utils.cpp:38-124.  The three CSV logs from a host diff: the 32-byte `header` gives the
+ * metadata breakdown's counts, `diff` (diff_len bytes, header first) its repeat table; the
+ * Chkpt ID column is the handle's current_id, the Setup/Comparison/Gather/Write times and data
+ * sizes the handle's last checkpoint's, as the reference writes them.  B2D_ERR_FORMAT when the
+ * diff is shorter than the header's lists. */
+int b2d_write_chkpt_log_host(b2d_dedup* d, const void* header, const uint8_t* diff, uint64_t diff_len,
+                             const char* logname);
+/* write_restart_log(uint32_t select_chkpt, std::string& logname)
+ * -- include/deduplicator_interface.hpp:181-182, src/tree_approach.cpp:1904-1915.  Appends one
+ * row (approach, select_chkpt, chunk size, the last restart's copy time and total time); a log
+ * that cannot be opened is skipped, as in the reference. */
+int b2d_write_restart_log(b2d_dedup* d, uint32_t select_chkpt, const char* logname);
 
 /* checkpoint(uint8_t* data_ptr, size_t len, HostMirror& diff_h, bool make_baseline)
  * -- src/tree_approach.cpp:1740-1748.  *diff points at pinned host memory owned by the handle,
@@ -133,7 +150,9 @@ int b2d_checkpoint_file(b2d_dedup* d, const void* d_data, uint64_t len, const ch
  * uint32_t chkpt_id) -- src/tree_approach.cpp:1807-1813 -> restart_chkpt :712-1128.
  * Rebuilds checkpoint `chkpt_id` into the device buffer `d_out` (len >= the header's datalen;
  * datalen bytes are written, the rest untouched) from host diffs[0..num_diffs).  `logname`
- * may be NULL (no restart log). */
+ * may be NULL (no restart log).  diffs[i] must be checkpoint i: a main diff whose header has
+ * ref_id > chkpt_id, or a chkpt_id other than `chkpt_id`, is rejected with B2D_ERR_FORMAT before
+ * any device work (the reference does not check and rebuilds from the main diff alone). */
 int b2d_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* diffs, const uint64_t* sizes,
                 uint32_t num_diffs, uint32_t chkpt_id, const char* logname);
 /* restart(View data, vector<string>& chkpt_filenames, std::string& logname, uint32_t chkpt_id)
@@ -156,8 +175,10 @@ int b2d_restart_device(b2d_dedup* d, void* d_out, uint64_t len, const void* cons
  * b2d_restart, but the diffs are device-resident (d_diffs[i]: device pointer, sizes[i]: bytes)
  * and no handle is needed.  The scratch is one fixed __device__ array in the library (about
  * 10.0 MB on every GPU that loads it, held until exit): at most 2^18 chunks per checkpoint and
- * checkpoint ids below 4096, else B2D_ERR_UNSUPPORTED.  The first call on a device looks up
- * that array's address and should come before any stream capture.  All calls share the array:
+ * checkpoint ids below 4096, else B2D_ERR_UNSUPPORTED.  Every call looks up that array's
+ * device address for the current device (so it stays right after a cudaDeviceReset); the first
+ * call on a device should come before any stream capture.  The same header checks as
+ * b2d_restart (B2D_ERR_FORMAT).  All calls share the array:
  * calls that overlap on the GPU race and must be serialised by the caller.  Work runs on
  * `cuda_stream` (NULL = legacy default stream) and the call returns after it completes. */
 int b2d_restart_noalloc(void* d_out, uint64_t len, const void* const* d_diffs, const uint64_t* sizes,

@@ -111,6 +111,16 @@ class TreeDeduplicator {
           "restart");
   }
 
+  // write_chkpt_log(header_t&, HostMirror& diff_h, std::string& logname)
+  // (deduplicator_interface.hpp:172-174): the three CSV logs, Chkpt ID = current_id()
+  void write_chkpt_log(header_t& header, std::vector<uint8_t>& diff_h, std::string& logname) {
+    check(b2d_write_chkpt_log_host(h_, &header, diff_h.data(), diff_h.size(), logname.c_str()), "write_chkpt_log");
+  }
+  // write_restart_log(uint32_t select_chkpt, std::string& logname)  (deduplicator_interface.hpp:181-182)
+  void write_restart_log(uint32_t select_chkpt, std::string& logname) {
+    check(b2d_write_restart_log(h_, select_chkpt, logname.c_str()), "write_restart_log");
+  }
+
   size_t num_first_ocur() {
     uint64_t v = 0;
     check(b2d_num_first_ocur(h_, &v), "num_first_ocur");

@@ -33,6 +33,8 @@ SIGNATURES = [
     ("b2d_copy_diff", _int, [_vp, _vp, _u64]),
     ("b2d_copy_diff_async", _int, [_vp, _vp, _u64, _vp]),
     ("b2d_write_chkpt_log", _int, [_vp, ctypes.c_char_p]),
+    ("b2d_write_chkpt_log_host", _int, [_vp, _vp, _vp, _u64, _cc]),
+    ("b2d_write_restart_log", _int, [_vp, _u32, _cc]),
     ("b2d_checkpoint", _int, [_vp, _vp, _u64, _int, _u8pp, ctypes.POINTER(_u64)]),
     ("b2d_checkpoint_log", _int, [_vp, _vp, _u64, _cc, _int, _u8pp, ctypes.POINTER(_u64)]),
     ("b2d_checkpoint_file", _int, [_vp, _vp, _u64, _cc, _cc, _int]),

@@ -46,7 +46,7 @@ MAX_CHECKPOINTS_PER_HANDLE = 8191
 
 class Request:
     __slots__ = ("client", "buffer", "nbytes", "make_baseline", "arrival", "admitted", "launched", "done", "rc",
-                 "diff_len", "checksum", "ready", "seq", "host", "launch_s", "batch_size", "baseline")
+                 "diff_len", "checksum", "ready", "seq", "host", "launch_s", "batch_size", "baseline", "chkpt_id")
 
     def __init__(self, client, buffer, make_baseline, arrival, seq):
         self.client, self.buffer, self.make_baseline, self.arrival, self.seq = client, buffer, make_baseline, arrival, seq
@@ -60,6 +60,8 @@ class Request:
         self.launch_s = None      # host seconds its batch's launch call took
         self.batch_size = 1
         self.baseline = None      # whether it ran as a baseline (set at launch)
+        self.chkpt_id = None      # the checkpoint id its diff carries on its client's handle (the
+                                  # index to restart it by among that handle's diffs)
 
     @property
     def latency(self):
@@ -278,6 +280,7 @@ class CheckpointServer:
             c.rebase = True
         if rc == 0:
             r.diff_len = c.handle.diff_device()[1]
+            r.chkpt_id = c.handle.current_id - 1
             if self.checksum:
                 r.checksum = c.handle.diff_checksum()
             used = c.handle.memory()

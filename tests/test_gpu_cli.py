@@ -88,3 +88,39 @@ def test_checkpoint_file_overload_and_write_failure(cuda, tmp_path):
         rows = f.read().splitlines()
     assert rows[0].startswith("Approach,Chkpt ID") and [r.split(",")[1] for r in rows[1:]] == ["0", "1", "2", "2"]
     h.close()
+
+
+def test_log_writers(cuda, tmp_path):
+    """write_chkpt_log(header, diff_h, logname) and write_restart_log(select_chkpt, logname)
+    (include/deduplicator_interface.hpp:172-183): the rows equal the ones the log-writing
+    checkpoint and restart overloads write for the same checkpoint (Chkpt ID = current_id, as in
+    the reference, which calls them before current_id += 1)"""
+    import torch
+
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import TreeDeduplicator
+
+    s = synth.ByteSeries(256 << 10, 128, synth.plan_plain_64m, 1, 22)
+    bufs = [torch.from_numpy(s.next().copy()).cuda() for _ in range(2)]
+    a, b = TreeDeduplicator(128), TreeDeduplicator(128)
+    la, lb = str(tmp_path / "a"), str(tmp_path / "b")
+    diffs = []
+    for i, x in enumerate(bufs):
+        diffs.append(a.checkpoint(x, i == 0, logname=la))
+        # the header_t& overload's steps: checkpoint without advancing, write the logs, advance
+        b.checkpoint_device(x, i == 0, advance=False)
+        d = b.copy_diff()
+        assert d.tobytes() == diffs[-1]
+        b.write_chkpt_log(d[:32].tobytes(), d, lb)
+        b.checkpoint_device(x, i == 0)          # same diff again, now advancing the id
+    for ext, fields in ((".csv", 7), (".size.csv", None), (".timing.csv", 3)):
+        ra = open(la + ".chunk_size.128" + ext).read().splitlines()
+        rb = open(lb + ".chunk_size.128" + ext).read().splitlines()
+        assert len(ra) == len(rb) and [r.split(",")[:fields] for r in ra] == [r.split(",")[:fields] for r in rb], ext
+    out = torch.zeros(len(bufs[0]), dtype=torch.uint8, device="cuda")
+    ra_log, rb_log = str(tmp_path / "ra.csv"), str(tmp_path / "rb.csv")
+    a.restart(out, diffs, 1, logname=ra_log)
+    assert torch.equal(out, bufs[1])
+    a.write_restart_log(1, rb_log)
+    assert open(ra_log).read() == open(rb_log).read() and open(rb_log).read().startswith("Tree,1,128,")
+    a.close()
+    b.close()

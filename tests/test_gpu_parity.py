@@ -221,3 +221,25 @@ def test_long_chain_restart_windows(cuda):
     (8 + 4) with the NodeIDs carried between them; every checkpoint restarts like the oracle"""
     s = synth.ByteSeries(512 * 1024 + 64, 128, synth.plan_plain_64m, 1, 91)
     run_both([s.next().copy() for _ in range(13)], 128)
+
+
+def test_checkpoint_id_limit(cuda):
+    """checkpoint ids keep counting across baselines, as in the reference; a handle takes ids up
+    to 8190 and then refuses further checkpoints with B2D_ERR_UNSUPPORTED (the digest map keeps a
+    13-bit checkpoint field), leaving its last checkpoint intact"""
+    import torch
+
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import B2DError
+
+    x = torch.arange(4096, dtype=torch.int32, device="cuda").to(torch.uint8)
+    g = TreeDeduplicator(64)
+    for i in range(8191):
+        g.checkpoint_device(x, i % 1000 == 0)
+    assert g.current_id == 8191
+    last = g.copy_diff().tobytes()
+    for baseline in (False, True):
+        with pytest.raises(B2DError) as e:
+            g.checkpoint_device(x, baseline)
+        assert e.value.code == -11
+    assert g.current_id == 8191 and g.copy_diff().tobytes() == last
+    g.close()

@@ -50,6 +50,10 @@ class FakeHandle:
     def memory(self):
         return self.mem
 
+    @property
+    def current_id(self):       # ids count this handle's checkpoints, from 0
+        return self.count
+
     def diff_device(self):
         return 0, 32
 
@@ -287,6 +291,8 @@ def test_client_moves_to_a_new_handle_at_the_id_limit(fakes, monkeypatch):
     assert len(hs) == 3 and hs[0].closed and hs[1].closed and not hs[2].closed
     assert [h.count for h in hs] == [3, 3, 1]
     assert [r.baseline for r in srv.completed] == [True, False, False, True, False, False, True]
+    # each request carries the id its diff has on its handle (the index to restart it by)
+    assert [r.chkpt_id for r in srv.completed] == [0, 1, 2, 0, 1, 2, 0]
     assert all(r.rc == 0 for r in srv.completed)
     srv.close()
 
