@@ -67,6 +67,14 @@ def parse():
     p.add_argument("--buffers", type=int, default=256, help="batched form: number of buffers")
     p.add_argument("--max-buffer", type=int, default=512 << 20, help="batched form: largest buffer size")
     p.add_argument("--no-autotune", action="store_true")
+    p.add_argument("--tune-batches", type=int, default=12, help="batched form: most autotuning batches")
+    p.add_argument("--capacity-waves", type=int, default=4, help="served form: waves of the capacity run")
+    p.add_argument("--no-forms", action="store_true",
+                   help="plain form: skip the bounded batched and served legs the default line carries")
+    p.add_argument("--forms-steps", type=int, default=4,
+                   help="plain form: timed batches of the bounded batched leg (after 2 warm-up batches)")
+    p.add_argument("--forms-requests", type=int, default=400,
+                   help="plain form: requests of the bounded served leg (Poisson, --rate per second)")
     p.add_argument("--no-restart", action="store_true", help="plain form: skip the restart measurement")
     p.add_argument("--no-plain", action="store_true", help="batched form: skip the one-at-a-time pass")
     p.add_argument("--graph", type=int, default=None, choices=[0, 1, 2],
@@ -236,8 +244,9 @@ def batched_series(sizes, dev, seed):
             for i, n in enumerate(sizes)]
 
 
-def run_batched(args, rank, world, dev):
-    """256 buffers of log-uniform sizes: the batch API against the same buffers one at a time."""
+def run_batched(args, rank, world, dev, emit=True):
+    """256 buffers of log-uniform sizes: the batch API against the same buffers one at a time.
+    Prints the line (emit) and returns it."""
     import torch
 
     from reproducibility_icpp23_scalable_gpu_deduplication_b200 import (CheckpointBatch, ListDeduplicator,
@@ -300,7 +309,7 @@ def run_batched(args, rank, world, dev):
         batch.set_param("autotune", 1)
         ss = batched_series(sizes, dev, seed + 1000)
         hs = [Dedup(128) for _ in sizes]
-        for c in range(12):
+        for c in range(args.tune_batches):
             batch.checkpoint(hs, [s.next() for s in ss])
             if batch.get_param("tuned"):
                 break
@@ -350,11 +359,12 @@ def run_batched(args, rank, world, dev):
                      "algorithmic_bytes": alg},
         "clocks": clk.summary(),
     }
-    if rank == 0:
+    if rank == 0 and emit:
         print(json.dumps(line), flush=True)
     batch.close()
-    if not same:
+    if not same and emit:
         sys.exit(3)
+    return line
 
 
 def serve_stream(server_kw, sizes, clients, arrivals, dev, warm_rounds=2, reserve=0):
@@ -450,8 +460,9 @@ def serve_capacity(server_kw, sizes, waves, dev, warm_rounds=2):
     return reqs, busy, batches, service
 
 
-def run_served(args, rank, world, dev):
-    """64 clients, Poisson arrivals: the continuous-batching loop against the one-at-a-time loop."""
+def run_served(args, rank, world, dev, emit=True):
+    """64 clients, Poisson arrivals: the continuous-batching loop against the one-at-a-time loop.
+    Prints the line (emit) and returns it."""
     from reproducibility_icpp23_scalable_gpu_deduplication_b200 import synth
     from reproducibility_icpp23_scalable_gpu_deduplication_b200.serve import percentile
 
@@ -478,8 +489,8 @@ def run_served(args, rank, world, dev):
         plain = summarize(*serve_stream(dict(kw, plain=True), sizes, clients, arrivals, dev,
                                         reserve=args.map_reserve))
         # capacity: all clients' requests waiting at once (unbounded arrival rate), 4 waves
-        cap_served = summarize(*serve_capacity(kw, sizes, 4, dev))
-        cap_plain = summarize(*serve_capacity(dict(kw, plain=True), sizes, 4, dev))
+        cap_served = summarize(*serve_capacity(kw, sizes, args.capacity_waves, dev))
+        cap_plain = summarize(*serve_capacity(dict(kw, plain=True), sizes, args.capacity_waves, dev))
     line = {
         "metric": f"{args.approach}-dedup served GB/s", "value": served["value"], "unit": "GB/s", "n_gpus": world,
         "steps": n, "warmup": 2, "ms_per_step": served["p50_ms"], "higher_is_better": True, "scaling": "weak",
@@ -494,13 +505,47 @@ def run_served(args, rank, world, dev):
                               "service_*: submission -> diff on the host; capacity: diffs stay on the device"},
         "latency_ms": {"p50": served["p50_ms"], "p99": served["p99_ms"], "max": served["max_ms"]},
         "served": served, "plain_same_stream": plain,
-        "capacity": {"mode": "all 64 clients submit at once, buffers edited and resident; 4 waves",
+        "capacity": {"mode": f"all {len(sizes)} clients submit at once, buffers edited and resident; "
+                             f"{args.capacity_waves} waves",
                      "served": cap_served, "plain": cap_plain,
                      "speedup_vs_plain": round(cap_served["value"] / cap_plain["value"], 3)},
         "e2e": None, "clocks": clk.summary(),
     }
-    if rank == 0:
+    if rank == 0 and emit:
         print(json.dumps(line), flush=True)
+    return line
+
+
+def bounded_forms(args, rank, world, dev):
+    """The batched form (all 256 buffers, 2 warm-up and --forms-steps timed batches after at most
+    6 autotuning batches) and the served form (64 clients, --forms-requests Poisson requests, 2
+    capacity waves), summarised as two keys of the plain line."""
+    import copy
+
+    import torch
+
+    b_args = copy.copy(args)
+    b_args.warmup, b_args.steps, b_args.tune_batches = 2, max(1, args.forms_steps), 6
+    b = run_batched(b_args, rank, world, dev, emit=False)
+    torch.cuda.empty_cache()
+    s_args = copy.copy(args)
+    s_args.requests, s_args.capacity_waves = max(1, args.forms_requests), 2
+    sv = run_served(s_args, rank, world, dev, emit=False)
+    torch.cuda.empty_cache()
+    batched = {k: b[k] for k in ("value", "unit", "ms_per_step", "steps", "speedup_vs_plain", "parity",
+                                 "gpu_launches", "map_growth")}
+    batched["one_at_a_time"] = b["plain_same_workload"]
+    batched["roofline_frac"] = b["roofline"]["frac"]
+    batched["config"] = {k: b["config"][k] for k in ("workload", "buffers", "total_bytes", "checkpoints", "change",
+                                                      "tuned")}
+    served = {"value": sv["value"], "unit": sv["unit"], "latency_ms": sv["latency_ms"],
+              "one_at_a_time": {k: sv["plain_same_stream"][k] for k in ("value", "p50_ms", "p99_ms", "max_ms")},
+              "capacity": {"value": sv["capacity"]["served"]["value"],
+                           "one_at_a_time": sv["capacity"]["plain"]["value"],
+                           "speedup_vs_plain": sv["capacity"]["speedup_vs_plain"]},
+              "config": {k: sv["config"][k] for k in ("workload", "clients", "rate_hz", "requests", "hbm_budget",
+                                                       "latency")}}
+    return {"batched": batched, "served": served}
 
 
 def main():
@@ -737,6 +782,13 @@ def main():
                                    warmup=1, device=dev)
         line["cpu_baseline"] = {"value": round(gbps, 4), "unit": "GB/s", "cores": threads, "kind": "port",
                                 "sample": cpu_sample_text(cpu_bytes, args.workload, cs, 1, args.cpu_steps)}
+    if world == 1 and args.workload == "plain_4g" and not args.no_forms:
+        # the batched and served forms, bounded to a few batches and a few hundred requests, so
+        # the default line carries them next to the plain form
+        dd.close()
+        del series
+        torch.cuda.empty_cache()
+        line.update(bounded_forms(args, rank, world, dev))
     if rank == 0:
         print(json.dumps(line), flush=True)
     dd.close()

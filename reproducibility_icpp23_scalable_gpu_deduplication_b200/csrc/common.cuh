@@ -7,7 +7,8 @@
 //                            every checkpoint (include/utils.hpp:51-57 Label values)
 //   push   : uint8_t[N]      region-root flags set by each node's parent: 1 first-occurrence
 //                            root, 2 shifted-duplicate root
-//   map    : MapSlot[cap+1]  open-addressing digest -> NodeID table (32 B slots)
+//   map    : cap+1 keys (16 B) then cap+1 values (8 B): open-addressing digest -> NodeID
+//            table, 24 B per slot (map.cuh)
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>

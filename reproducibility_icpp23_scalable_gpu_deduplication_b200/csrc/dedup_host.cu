@@ -89,29 +89,22 @@ struct PinnedBuf {
   }
 };
 
-__global__ void map_special_init_kernel(MapSlot* special) {
-  special->key_lo = 0;
-  special->key_hi = 0;
-  special->val = ~0ull;
-  special->spare = 0;
-  special->pad = 0;   // unoccupied
-}
-
 // move every occupied slot of `from` into the (empty) table `to`
 __global__ void map_rehash_kernel(MapView from, MapView to, DevStatus* st) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i <= from.cap;
        i += (uint64_t)gridDim.x * blockDim.x) {
-    const MapSlot s = from.slots[i];
-    if (i == from.cap) {
-      if (s.pad) to.slots[to.cap] = s;
+    const unsigned long long v = from.vals[i];
+    if (i == from.cap) {   // the extra slot (the all-ones digest), present when its value is set
+      if (v != MAP_EMPTY) to.vals[to.cap] = v;
       continue;
     }
-    if (s.key_lo == MAP_EMPTY && s.key_hi == MAP_EMPTY) continue;
+    const Key128 k = from.keys[i];
+    if (k.lo == MAP_EMPTY && k.hi == MAP_EMPTY) continue;
     Digest d;
-    d.w[0] = (uint32_t)s.key_lo; d.w[1] = (uint32_t)(s.key_lo >> 32);
-    d.w[2] = (uint32_t)s.key_hi; d.w[3] = (uint32_t)(s.key_hi >> 32);
-    const MapRef r = map_insert_packed(to, d, s.val, st);
-    if (r.found) to.slots[r.slot].val = s.val;
+    d.w[0] = (uint32_t)k.lo; d.w[1] = (uint32_t)(k.lo >> 32);
+    d.w[2] = (uint32_t)k.hi; d.w[3] = (uint32_t)(k.hi >> 32);
+    const MapRef r = map_insert_packed(to, d, v, st);
+    if (r.found) to.vals[r.slot] = v;
   }
 }
 
@@ -137,8 +130,12 @@ struct DevState {
 using namespace b2d;
 
 // default size of a baseline's digest map over its minimum, and the factor a growing map
-// takes over its new minimum
-constexpr double MAP_HEADROOM = 2.0;
+// takes over its new minimum.  A baseline's minimum is its own N entries plus the next
+// checkpoint's N at the load limit: 2N / 0.75; times 1.5 that is 4N slots (24 B each, 96 B per
+// node: 1.5 bytes per byte of a 4 GiB buffer at 128-byte chunks), at load 0.25 after the
+// baseline, and the table grows only once its entries pass 2N (after about a hundred
+// checkpoints that each change 1% of the chunks).
+constexpr double MAP_HEADROOM = 1.5;
 constexpr double MAP_GROWTH = 2.0;
 
 struct b2d_dedup {
@@ -176,7 +173,7 @@ struct b2d_dedup {
 
   DevBuf<Digest> tree;
   DevBuf<uint8_t> lab, leaflab, push, dupflag;
-  MapSlot* map_slots = nullptr;   // map_cap + 1 slots, from the library's map pool
+  void* map_mem = nullptr;        // map_cap + 1 keys, then their values (map_at), from the library's map pool
   uint64_t map_cap = 0;
   double map_grow_s = 0;          // host seconds spent growing the map (all checkpoints)
   double map_alloc_s = 0;         // host seconds in the map allocation calls (all tables)
@@ -245,9 +242,9 @@ cudaMemPool_t map_pool(int device) {
 
 b2d_dedup::~b2d_dedup() {
   {
-    if (map_slots) {
+    if (map_mem) {
       cudaStream_t s = own_stream ? own_stream : stream;
-      cudaFreeAsync(map_slots, s);
+      cudaFreeAsync(map_mem, s);
       cudaStreamSynchronize(s);
       if (cudaMemPool_t p = map_pool(device)) {
         std::lock_guard<std::mutex> lock(g_pool_mu);
@@ -297,7 +294,7 @@ uint64_t buf_bytes(const DevBuf<T>& b) {
 // device bytes a handle holds (everything it allocated with cudaMalloc)
 uint64_t handle_bytes(const b2d_dedup* d) {
   return buf_bytes(d->tree) + buf_bytes(d->lab) + buf_bytes(d->leaflab) + buf_bytes(d->push) +
-         buf_bytes(d->dupflag) + (d->map_slots ? (d->map_cap + 1) * sizeof(MapSlot) : 0) +
+         buf_bytes(d->dupflag) + (d->map_mem ? (d->map_cap + 1) * MAP_SLOT_BYTES : 0) +
          buf_bytes(d->map_size) + buf_bytes(d->tmp_first) +
          buf_bytes(d->tmp_shift) + buf_bytes(d->levels) + buf_bytes(d->first_list) + buf_bytes(d->shift_list) +
          buf_bytes(d->region_off) + buf_bytes(d->sprev) + buf_bytes(d->skey) + buf_bytes(d->hist) +
@@ -309,36 +306,32 @@ uint64_t handle_bytes(const b2d_dedup* d) {
 }
 
 int map_view(b2d_dedup* d, MapView& m) {
-  m.slots = d->map_slots;
-  m.cap = d->map_cap;
-  m.size = d->map_size.p;
-  m.pad = 0;
+  m = map_at(d->map_mem, d->map_cap, d->map_size.p);
   return B2D_OK;
 }
 
 // a fresh map of `cap` slots (+ the special slot) on the handle's stream
-int map_alloc(b2d_dedup* d, uint64_t cap, MapSlot** out) {
+int map_alloc(b2d_dedup* d, uint64_t cap, void** out) {
   cudaMemPool_t pool = map_pool(d->device);
   if (!pool) return B2D_ERR_CUDA;
   const auto t0 = std::chrono::high_resolution_clock::now();
-  B2D_CU(cudaMallocFromPoolAsync(reinterpret_cast<void**>(out), sizeof(MapSlot) * (cap + 1), pool, d->stream));
+  B2D_CU(cudaMallocFromPoolAsync(out, MAP_SLOT_BYTES * (cap + 1), pool, d->stream));
   d->map_alloc_s += secs(t0, std::chrono::high_resolution_clock::now());
-  B2D_CU(cudaMemsetAsync(*out, 0xff, sizeof(MapSlot) * (cap + 1), d->stream));
-  map_special_init_kernel<<<1, 1, 0, d->stream>>>(*out + cap);
-  return cuda_status(cudaGetLastError());
+  // all keys EMPTY, all values all-ones (the extra slot: absent)
+  B2D_CU(cudaMemsetAsync(*out, 0xff, MAP_SLOT_BYTES * (cap + 1), d->stream));
+  return B2D_OK;
 }
 
 int map_reset(b2d_dedup* d, uint64_t cap) {
-  if (!d->map_slots || d->map_cap != cap) {
-    MapSlot* fresh = nullptr;
+  if (!d->map_mem || d->map_cap != cap) {
+    void* fresh = nullptr;
     int rc = map_alloc(d, cap, &fresh);
     if (rc) return rc;
-    if (d->map_slots) cudaFreeAsync(d->map_slots, d->stream);
-    d->map_slots = fresh;
+    if (d->map_mem) cudaFreeAsync(d->map_mem, d->stream);
+    d->map_mem = fresh;
     d->map_cap = cap;
   } else {
-    B2D_CU(cudaMemsetAsync(d->map_slots, 0xff, sizeof(MapSlot) * (cap + 1), d->stream));
-    map_special_init_kernel<<<1, 1, 0, d->stream>>>(d->map_slots + cap);
+    B2D_CU(cudaMemsetAsync(d->map_mem, 0xff, MAP_SLOT_BYTES * (cap + 1), d->stream));
   }
   B2D_CU(d->map_size.reserve(1));
   B2D_CU(cudaMemsetAsync(d->map_size.p, 0, sizeof(unsigned long long), d->stream));
@@ -350,7 +343,7 @@ int map_reset(b2d_dedup* d, uint64_t cap) {
 // (src/tree_approach.cpp:1622-1623): room for every node of the next checkpoint to be new.
 // Here that room must fit under the load limit map_max_load (default 0.75), so no checkpoint
 // can push the table past it: a new table holds its entries plus N at that load, times
-// map_headroom (default 2) at a baseline and MAP_GROWTH when it grows.  Growing allocates and
+// map_headroom (default 1.5) at a baseline and MAP_GROWTH when it grows.  Growing allocates and
 // rehashes (allocation dominates: tens of ms per GB), so a series whose digests keep changing
 // grows less often with more headroom.  Capacities are multiples of 1024, not powers of two.
 uint64_t map_capacity(uint64_t need, double max_load, double headroom) {
@@ -360,11 +353,11 @@ uint64_t map_capacity(uint64_t need, double max_load, double headroom) {
 
 int map_ensure(b2d_dedup* d) {
   const uint64_t need = d->map_size_host + d->N;
-  if (d->map_slots && (double)need <= d->map_max_load * (double)d->map_cap) return B2D_OK;
+  if (d->map_mem && (double)need <= d->map_max_load * (double)d->map_cap) return B2D_OK;
   const uint64_t cap = map_capacity(need, d->map_max_load, MAP_GROWTH);
-  if (!d->map_slots || d->map_size_host == 0) return map_reset(d, cap);
+  if (!d->map_mem || d->map_size_host == 0) return map_reset(d, cap);
   const auto t0 = std::chrono::high_resolution_clock::now();
-  MapSlot* fresh = nullptr;
+  void* fresh = nullptr;
   int rc = map_alloc(d, cap, &fresh);
   if (rc) return rc;
   DevBuf<unsigned long long> cnt;
@@ -372,16 +365,16 @@ int map_ensure(b2d_dedup* d) {
   B2D_CU(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long), d->stream));
   MapView from, to;
   map_view(d, from);
-  to.slots = fresh; to.cap = cap; to.size = cnt.p; to.pad = 0;
+  to = map_at(fresh, cap, cnt.p);
   map_rehash_kernel<<<(unsigned)d->sm_count * 8u, 256, 0, d->stream>>>(from, to, &d->state.p->status);
   const cudaError_t ke = cudaGetLastError();
   if (ke != cudaSuccess) {
     cudaFreeAsync(fresh, d->stream);
     return cuda_status(ke);
   }
-  cudaFreeAsync(d->map_slots, d->stream);
+  cudaFreeAsync(d->map_mem, d->stream);
   B2D_CU(cudaStreamSynchronize(d->stream));
-  d->map_slots = fresh;
+  d->map_mem = fresh;
   std::swap(d->map_size.p, cnt.p);
   std::swap(d->map_size.n, cnt.n);
   d->map_cap = cap;
@@ -402,13 +395,10 @@ int status_code(const DevStatus& st) {
 
 
 LeafArgs leaf_args(const b2d_dedup* d, const RoundState* rs_dev) {
-  MapView m;
-  m.slots = d->map_slots;
-  m.cap = d->map_cap;
-  m.size = d->map_size.p;
-  m.pad = 0;
+  const MapView m = map_at(d->map_mem, d->map_cap, d->map_size.p);
   return LeafArgs{static_cast<const uint8_t*>(d->data), d->data_len, d->chunk_size, d->n, d->kind, 0, 0,
-                  d->tree.p, d->leaflab.p, d->dupflag.p, m, &d->state.p->status, rs_dev};
+                  d->tree.p, d->leaflab.p, d->dupflag.p, m, &d->state.p->status, rs_dev,
+                  (uint32_t)d->tune.wait_polls, 1u};
 }
 
 // ------------------------------------------------------------------------------------------
@@ -510,7 +500,7 @@ void graph_key(const b2d_dedup* d, const RoundState* rs_dev, std::vector<uint64_
             (uint64_t)d->bucket_start.p, (uint64_t)d->partial.p, (uint64_t)d->partial2.p, (uint64_t)d->diff.p,
             (uint64_t)d->state.p, (uint64_t)d->state_h.p, (uint64_t)d->round_h.p, (uint64_t)rs_dev, d->bcap,
             (uint64_t)d->tune.allow_tma, (uint64_t)d->tune.stages, (uint64_t)d->tune.ctas_per_sm, (uint64_t)d->graph_timing,
-            (uint64_t)d->tune.unit,
+            (uint64_t)d->tune.unit, (uint64_t)d->tune.wait_polls,
             (uint64_t)d->sm_count, (uint64_t)d->list});
 }
 
@@ -582,7 +572,7 @@ int enqueue_checkpoint(b2d_dedup* d, cudaStream_t s, RoundState* rs_dev, bool up
     d->launches = (skip_leaves ? 0 : 1) + 1 + (skip_diff ? 0 : 10);
   else
     d->launches = (skip_leaves ? 0 : 1) +
-                  (skip_forest ? 0 : forest_launch_count(d->D, 1) + forest_launch_count(d->D, 2) +
+                  (skip_forest ? 0 : forest_launch_count(d->n, d->D, 1) + forest_launch_count(d->n, d->D, 2) +
                                          (zero_probe_skipped ? 0 : 1)) +
                   (skip_diff ? 0 : 12);
   return B2D_OK;
@@ -819,6 +809,9 @@ int do_restart(b2d_dedup* d, void* d_out, uint64_t len, const uint8_t* const* di
   }
   HostHdr h;
   if (!parse_hdr(diffs[id], sizes[id], h)) return B2D_ERR_FORMAT;
+  // every diff the checkpoint path writes has ref_id <= chkpt_id == its position in the list;
+  // a list that breaks this names no chain to walk, so it is rejected before any device work
+  if (h.ref_id > h.chkpt_id || h.chkpt_id != id) return B2D_ERR_FORMAT;
   if (len < h.datalen) return B2D_ERR_ARG;
   uint64_t nc = (h.datalen + h.cs - 1) / h.cs;
   if (nc > 0x7fffffffull) return B2D_ERR_FORMAT;
@@ -1313,11 +1306,11 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
       fsteps[ph].resize(count);
       uint32_t K = 0;
       for (uint32_t i = 0; i < count; i++) {
-        if (!hs[i]->list) forest_steps(hs[i]->D, hs[i]->N, ph + 1, fsteps[ph][i]);
+        if (!hs[i]->list) forest_steps_batch(hs[i]->n, hs[i]->D, hs[i]->N, ph + 1, fsteps[ph][i]);
         K = std::max<uint32_t>(K, (uint32_t)fsteps[ph][i].size());
       }
       for (uint32_t k = 0; k < K; k++)
-        for (int kind = 0; kind < 2; kind++) {
+        for (int kind = 0; kind < 3; kind++) {
           uint32_t ctas = 0;
           for (uint32_t i = 0; i < count; i++)
             if (k < fsteps[ph][i].size() && fsteps[ph][i][k].kind == kind) ctas += fsteps[ph][i][k].ctas;
@@ -1756,6 +1749,27 @@ int b2d_write_chkpt_log(b2d_dedup* d, const char* logname) {
   })
 }
 
+int b2d_write_chkpt_log_host(b2d_dedup* d, const void* header, const uint8_t* diff, uint64_t diff_len,
+                             const char* logname) {
+  B2D_GUARD({
+    if (!d || !header || !diff || !logname) return B2D_ERR_ARG;
+    const uint8_t* h = static_cast<const uint8_t*>(header);
+    uint32_t nf = 0;
+    uint32_t np = 0;
+    memcpy(&nf, h + 20, 4);
+    memcpy(&np, h + 24, 4);
+    if (diff_len < 32ull + 4ull * nf + 8ull * np) return B2D_ERR_FORMAT;
+    return write_chkpt_log(d, h, diff + 32 + 4ull * nf, logname, d->current_id);
+  })
+}
+
+int b2d_write_restart_log(b2d_dedup* d, uint32_t select_chkpt, const char* logname) {
+  B2D_GUARD({
+    if (!d || !logname) return B2D_ERR_ARG;
+    return write_restart_log(d, select_chkpt, logname);
+  })
+}
+
 int b2d_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, int make_baseline, const uint8_t** diff,
                    uint64_t* diff_len) {
   B2D_GUARD({
@@ -1863,6 +1877,7 @@ int b2d_set_param(b2d_dedup* d, const char* name, int64_t value) {
   else if (k == "leaf_ctas_per_sm" && value >= 0 && value <= 8) d->tune.ctas_per_sm = (int)value;
   else if (k == "leaf_unit" && (value == 0 || value == 16 || value == 32 || value == 64 || value == 128))
     d->tune.unit = (int)value;
+  else if (k == "leaf_wait_polls" && value >= 0 && value <= (1 << 20)) d->tune.wait_polls = (int)value;
   else if (k == "map_max_load_pct" && value >= 10 && value <= 90) d->map_max_load = value / 100.0;
   else if (k == "map_headroom_pct" && value >= 100 && value <= 1000) d->map_headroom = value / 100.0;
   else if (k == "graph" && value >= 0 && value <= 2) {
@@ -2007,7 +2022,7 @@ int b2d_estimate_memory(uint64_t len, uint32_t chunk_size, int map_max_load_pct,
   const uint64_t n = (len + chunk_size - 1) / chunk_size, N = 2 * n - 1;
   const uint64_t cap = map_capacity(2 * N, map_max_load_pct / 100.0, MAP_HEADROOM);
   uint64_t b = N * sizeof(Digest) + N + (n + 16) + ((N + 15) / 16 * 16 + 16) + n;   // tree, labels, flags
-  b += (cap + 1) * sizeof(MapSlot) + 8;                                              // map
+  b += (cap + 1) * MAP_SLOT_BYTES + 8;                                               // map
   b += 8 * 4 * n + 68 * 4;                                                           // lists and keys
   b += (uint64_t)64 * 4 * 2 + (uint64_t)1184 * 64 * 4 + 2 * COMPACT_GRID * 4;           // buckets, partials
   b += 64 + 16 * n + n * chunk_size;                                                 // diff

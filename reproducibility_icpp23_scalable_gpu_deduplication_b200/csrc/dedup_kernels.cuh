@@ -46,6 +46,9 @@ struct LeafArgs {
   MapView map;
   DevStatus* st;
   const RoundState* rs;
+  uint32_t wait_polls;   // 0: the barrier waits' normal bound; else give up after this many
+                         // non-blocking polls (a test of the give-up path)
+  uint32_t one;          // 1, as a value the compiler cannot see (md5_compress_fma)
 };
 
 struct ForestArgs {
@@ -132,6 +135,7 @@ struct LeafTuning {
   int stages = 0;        // TMA ring depth per CTA (default: a 64 KB ring)
   int ctas_per_sm = 0;   // resident CTAs per SM (default 3)
   int unit = 0;          // staged segment width in bytes (0: the largest of 128/64/32/16 dividing the chunk)
+  int wait_polls = 0;    // see LeafArgs::wait_polls
 };
 int launch_leaves(const LeafArgs& a, int sm_count, const LeafTuning& tune, cudaStream_t stream);
 
@@ -166,12 +170,17 @@ __device__ __forceinline__ uint32_t seg_find(const uint32_t* beg, uint32_t n, ui
   return lo;
 }
 // one launch of a forest phase of a tree: kind 0 = a full band with input level p0, kind 1 = a
-// general band of levels p0 (top) .. p1 (bottom); `ctas` CTAs
+// general band of levels p0 (top) .. p1 (bottom), kind 2 = a warp band over the leaves; `ctas`
+// CTAs
 struct ForestStep {
   uint8_t kind;
   uint32_t p0, p1, ctas;
 };
 void forest_steps(uint32_t D, uint64_t N, int phase, std::vector<ForestStep>& out);
+// the steps of the batched form: a warp band first where the tree allows one (kind 2: p0 = D,
+// one warp per task of 128 (phase 1) or 512 (phase 2) leaves, 8 tasks per CTA), then the bands
+// above it
+void forest_steps_batch(uint32_t n, uint32_t D, uint64_t N, int phase, std::vector<ForestStep>& out);
 // the same step of many handles' trees in one launch (batched form); handles without this
 // step have no CTAs
 struct ForestSeg {
@@ -183,7 +192,7 @@ struct ForestSeg {
 };
 cudaError_t launch_forest_seg(const ForestSeg& s, int phase, int kind, uint32_t ctas, cudaStream_t stream);
 cudaError_t launch_zero_exists_seg(const ForestArgs* args, uint32_t n, cudaStream_t stream);
-int forest_launch_count(uint32_t D, int phase);
+int forest_launch_count(uint32_t n, uint32_t D, int phase);
 cudaError_t launch_zero_exists(int* flag, const RoundState* rs, cudaStream_t stream);
 // bcap: bucket capacity the scratch was sized for (>= rs->buckets of every checkpoint run).
 // node_order: the region lists stay in node order (the list approach's order, whose regions

@@ -473,6 +473,182 @@ __global__ void __launch_bounds__(FAST_THREADS, B2D_FAST_MINB) forest_fast_seg(F
   forest_fast_body<PHASE>(with_round(s.args[h]), bid, s.p0[h]);
 }
 
+// Warp bands: the first band of each phase of a tree whose chunk count is a power of two, as
+// independent warp tasks (no CTA barrier).  A CTA band stalls all its warps on three barriers
+// per band and a CTA takes its bands one after another, so most of a band's time was load and
+// barrier latency; a warp task folds its leaves in registers and by shuffles only, and each
+// warp loads the next task's labels before it works on the current one.
+//   phase 1: 128 leaves per task (4 per lane, one 32-bit label load), 7 levels: 2 in registers
+//            (with the parents' digests), 5 by shuffles; a parent is hashed and inserted where
+//            its label is decided
+//   phase 2: 512 leaves per task (16 per lane, one 16-byte label load), 9 levels: 4 in
+//            registers, 5 by shuffles
+// A task writes its root's label to `lab` for the band above (which is a CTA band again: few
+// nodes are left there).  Same per-node rules as the CTA bands, so the labels, digests, map
+// entries and push flags are the same.
+#ifndef B2D_WARP_BANDS
+#define B2D_WARP_BANDS 1
+#endif
+constexpr uint32_t WB1_LEVELS = 7;
+constexpr uint32_t WB2_LEVELS = 9;
+constexpr uint32_t WB_THREADS = 256;
+
+static bool warp_bands(uint32_t n, uint32_t D, int phase) {
+  return B2D_WARP_BANDS && n >= 2u && (n & (n - 1u)) == 0 && D >= (phase == 1 ? WB1_LEVELS : WB2_LEVELS);
+}
+
+__device__ __forceinline__ void warp1_task(const ForestArgs& a, uint32_t task, uint32_t lane, uint32_t w) {
+  const uint64_t root = ((1ull << (a.D - WB1_LEVELS)) - 1ull) + task;
+  const uint32_t c0 = task * 128u + 4u * lane;          // first chunk of this lane
+  const uint64_t x0 = (uint64_t)(a.n - 1u) + c0;        // its leaf (a left child)
+  const uint32_t z = ~(((w & 0x7f7f7f7fu) + 0x7f7f7f7fu) | w | 0x7f7f7f7fu);   // exact: byte == FIRST (0)
+  uint32_t m0 = ((z >> 7) & 1u) | ((z >> 14) & 2u) | ((z >> 21) & 4u) | ((z >> 28) & 8u);
+  if (!__any_sync(0xffffffffu, m0 != 0u)) {
+    if (lane == 0) band_output<1>(a, root, DONE);
+    return;
+  }
+  if (m0 && *reinterpret_cast<const uint32_t*>(a.dupflag + c0)) {
+    // lowest-index relabel of the first occurrences the leaf stage flagged as sharing a digest
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      if ((m0 >> j) & 1u)
+        if (leaf_view<1>(a, (uint32_t)(x0 + j), FIRST_OCUR) != FIRST_OCUR) m0 &= ~(1u << j);
+  }
+  // height 1: nodes p0, p0 + 1; height 2: node y
+  const uint64_t p0 = (x0 - 1ull) >> 1;
+  Digest d1[2];
+  uint32_t m1 = 0;
+#pragma unroll
+  for (int j = 0; j < 2; j++) {
+    d1[j].w[0] = d1[j].w[1] = d1[j].w[2] = d1[j].w[3] = 0u;
+    if (((m0 >> (2 * j)) & 3u) == 3u) {
+      d1[j] = hash_pair(a.kind, a.tree[x0 + 2 * j], a.tree[x0 + 2 * j + 1]);
+      a.tree[p0 + j] = d1[j];
+      insert_first_parent(a, (uint32_t)(p0 + j), d1[j]);
+      m1 |= 1u << j;
+    }
+  }
+  uint64_t y = (p0 - 1ull) >> 1;
+  uint32_t b = 0;
+  Digest dg;
+  dg.w[0] = dg.w[1] = dg.w[2] = dg.w[3] = 0u;
+  if (m1 == 3u) {
+    dg = hash_pair(a.kind, d1[0], d1[1]);
+    a.tree[y] = dg;
+    insert_first_parent(a, (uint32_t)y, dg);
+    b = 1;
+  }
+  // heights 3..7: shuffles; lane 0 ends at the task root
+  if (__any_sync(0xffffffffu, b)) {
+#pragma unroll
+    for (int s = 0; s < 5; s++) {
+      const uint32_t rb = __shfl_down_sync(0xffffffffu, b, 1u << s);
+      const Digest rd = shfl_down_digest(dg, 1u << s);
+      if ((lane & ((2u << s) - 1u)) == 0) {
+        y = (y - 1ull) >> 1;
+        b &= rb;
+        if (b) {
+          dg = hash_pair(a.kind, dg, rd);
+          a.tree[y] = dg;
+          insert_first_parent(a, (uint32_t)y, dg);
+        }
+      }
+    }
+  } else {
+    b = 0;
+  }
+  if (lane == 0) band_output<1>(a, root, b ? FIRST_OCUR : DONE);
+}
+
+__device__ __forceinline__ void warp2_task(const ForestArgs& a, uint32_t task, uint32_t lane, const uint4& w) {
+  const uint64_t root = ((1ull << (a.D - WB2_LEVELS)) - 1ull) + task;
+  const uint32_t c0 = task * 512u + 16u * lane;
+  const uint64_t x0 = (uint64_t)(a.n - 1u) + c0;
+  bool fast = !a.baseline && w.x == 0x01010101u && w.y == 0x01010101u && w.z == 0x01010101u &&
+              w.w == 0x01010101u;   // all 16 leaves FIXED
+  if (__all_sync(0xffffffffu, fast)) {
+    if (lane == 0) band_output<2>(a, root, FIXED_DUPL);
+    return;
+  }
+  uint8_t lab = FIXED_DUPL;
+  if (!fast) {
+    uint8_t v[16];
+    const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int j = 0; j < 16; j++) v[j] = (uint8_t)(ws[j >> 2] >> (8 * (j & 3)));
+    uint64_t first = x0;
+#pragma unroll
+    for (int width = 8; width >= 1; width >>= 1) {
+      first = (first - 1ull) >> 1;
+#pragma unroll
+      for (int j = 0; j < width; j++) v[j] = forest_node<2>(a, (uint32_t)(first + j), v[2 * j], v[2 * j + 1]);
+    }
+    lab = v[0];
+  }
+  uint64_t y = ((x0 + 1ull) >> 4) - 1ull;   // the lane's 16-leaf subtree root
+#pragma unroll
+  for (int s = 0; s < 5; s++) {
+    __syncwarp();   // digests written by the partner lane at the previous level are visible
+    const uint8_t rl = (uint8_t)__shfl_down_sync(0xffffffffu, (uint32_t)lab, 1u << s);
+    if ((lane & ((2u << s) - 1u)) == 0) {
+      y = (y - 1ull) >> 1;
+      if (a.baseline || lab != FIXED_DUPL || rl != FIXED_DUPL) lab = forest_node<2>(a, (uint32_t)y, lab, rl);
+    }
+  }
+  if (lane == 0) band_output<2>(a, root, lab);
+}
+
+// Resident grid of warps; warp g takes tasks g, g + G, ... and loads the next one's labels first.
+__global__ void __launch_bounds__(WB_THREADS) forest_warp1_kernel(ForestArgs a0, uint32_t ntasks) {
+  const ForestArgs a = with_round(a0);
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t G = (gridDim.x * WB_THREADS) >> 5;
+  uint32_t task = (blockIdx.x * WB_THREADS + threadIdx.x) >> 5;
+  const uint32_t* lab32 = reinterpret_cast<const uint32_t*>(a.leaflab);
+  uint32_t w = task < ntasks ? lab32[task * 32u + lane] : 0u;
+  for (; task < ntasks; task += G) {
+    const uint32_t next = task + G;
+    const uint32_t wn = next < ntasks ? lab32[next * 32u + lane] : 0u;
+    warp1_task(a, task, lane, w);
+    w = wn;
+  }
+}
+__global__ void __launch_bounds__(WB_THREADS) forest_warp2_kernel(ForestArgs a0, uint32_t ntasks) {
+  const ForestArgs a = with_round(a0);
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t G = (gridDim.x * WB_THREADS) >> 5;
+  uint32_t task = (blockIdx.x * WB_THREADS + threadIdx.x) >> 5;
+  const uint4* lab128 = reinterpret_cast<const uint4*>(a.leaflab);
+  uint4 w = task < ntasks ? lab128[task * 32u + lane] : make_uint4(0, 0, 0, 0);
+  for (; task < ntasks; task += G) {
+    const uint32_t next = task + G;
+    const uint4 wn = next < ntasks ? lab128[next * 32u + lane] : make_uint4(0, 0, 0, 0);
+    warp2_task(a, task, lane, w);
+    w = wn;
+  }
+}
+
+// Segmented warp bands (batched form): CTA b of a handle's range holds its tasks 8b .. 8b+7,
+// one per warp.
+__global__ void __launch_bounds__(WB_THREADS) forest_warp1_seg(ForestSeg s) {
+  uint32_t bid, nb;
+  const uint32_t h = seg_find(s.beg, s.n, bid, nb);
+  const ForestArgs a = with_round(s.args[h]);
+  const uint32_t task = bid * (WB_THREADS / 32u) + (threadIdx.x >> 5);
+  if (task >= (a.n >> WB1_LEVELS)) return;
+  const uint32_t lane = threadIdx.x & 31u;
+  warp1_task(a, task, lane, reinterpret_cast<const uint32_t*>(a.leaflab)[task * 32u + lane]);
+}
+__global__ void __launch_bounds__(WB_THREADS) forest_warp2_seg(ForestSeg s) {
+  uint32_t bid, nb;
+  const uint32_t h = seg_find(s.beg, s.n, bid, nb);
+  const ForestArgs a = with_round(s.args[h]);
+  const uint32_t task = bid * (WB_THREADS / 32u) + (threadIdx.x >> 5);
+  if (task >= (a.n >> WB2_LEVELS)) return;
+  const uint32_t lane = threadIdx.x & 31u;
+  warp2_task(a, task, lane, reinterpret_cast<const uint4*>(a.leaflab)[task * 32u + lane]);
+}
+
 // General band: levels [top, bot] (top <= bot <= D), level by level through shared memory.
 // Nodes at level `bot` are leaves or combine children at level bot+1 read from `lab`.
 template <int PHASE>
@@ -516,14 +692,14 @@ __global__ void __launch_bounds__(FOREST_THREADS) forest_band_seg(ForestSeg s) {
 
 static uint32_t band_levels(int phase) { return phase == 1 ? FF_LEVELS : FAST_LEVELS; }
 
-// The launches of one phase for a tree of depth D: full bands of band_levels(phase) levels from
-// the leaves up (kind 0, p0 = input level), then general bands of up to FOREST_BAND_LEVELS
-// levels (kind 1, p0 = top, p1 = bottom level) for what is left above.
-void forest_steps(uint32_t D, uint64_t N, int phase, std::vector<ForestStep>& out) {
+// The launches of one phase for a tree of depth D whose labels at level `in` are known (the
+// leaves, in = D, or a warp band's outputs): full bands of band_levels(phase) levels up from
+// `in` (kind 0, p0 = input level), then general bands of up to FOREST_BAND_LEVELS levels
+// (kind 1, p0 = top, p1 = bottom level) for what is left above.
+static void forest_steps_from(uint32_t D, uint32_t in, uint64_t N, int phase, std::vector<ForestStep>& out) {
   out.clear();
   if (N <= 1) return;   // one chunk: no inner nodes; the reference never pushes a region
   const uint32_t L = band_levels(phase);
-  uint32_t in = D;      // labels at level `in` are known (leaves, or a band's output)
   while (in >= L) {
     out.push_back(ForestStep{0, in, 0, 1u << (in - L)});
     in -= L;
@@ -537,6 +713,21 @@ void forest_steps(uint32_t D, uint64_t N, int phase, std::vector<ForestStep>& ou
     out.push_back(ForestStep{1, (uint32_t)top, (uint32_t)bot, 1u << top});
     bot = top - 1;
   }
+}
+void forest_steps(uint32_t D, uint64_t N, int phase, std::vector<ForestStep>& out) {
+  forest_steps_from(D, D, N, phase, out);
+}
+void forest_steps_batch(uint32_t n, uint32_t D, uint64_t N, int phase, std::vector<ForestStep>& out) {
+  if (!warp_bands(n, D, phase)) {
+    forest_steps(D, N, phase, out);
+    return;
+  }
+  const uint32_t levels = phase == 1 ? WB1_LEVELS : WB2_LEVELS;
+  std::vector<ForestStep> rest;
+  forest_steps_from(D, D - levels, N, phase, rest);
+  out.clear();
+  out.push_back(ForestStep{2, D, 0, ((n >> levels) + WB_THREADS / 32u - 1u) / (WB_THREADS / 32u)});
+  out.insert(out.end(), rest.begin(), rest.end());
 }
 
 // resident CTAs per SM of a first-band kernel (queried once)
@@ -554,7 +745,22 @@ cudaError_t launch_forest(const ForestArgs& a, int phase, cudaStream_t stream, i
   static const uint32_t res_first = resident_ctas(forest_first_kernel);
   static const uint32_t res_fast = resident_ctas(forest_fast_kernel<2>);
   std::vector<ForestStep> steps;
-  forest_steps(a.D, a.N, phase, steps);
+  if (warp_bands(a.n, a.D, phase)) {
+    static const uint32_t res_w1 = resident_ctas(forest_warp1_kernel);
+    static const uint32_t res_w2 = resident_ctas(forest_warp2_kernel);
+    const uint32_t levels = phase == 1 ? WB1_LEVELS : WB2_LEVELS;
+    const uint32_t ntasks = a.n >> levels;
+    const uint32_t want = (ntasks + WB_THREADS / 32u - 1u) / (WB_THREADS / 32u);
+    const uint32_t cap = (phase == 1 ? res_w1 : res_w2) * (uint32_t)(sm_count > 0 ? sm_count : 1);
+    const uint32_t grid = want < cap ? want : cap;
+    if (phase == 1) forest_warp1_kernel<<<grid, WB_THREADS, 0, stream>>>(a, ntasks);
+    else forest_warp2_kernel<<<grid, WB_THREADS, 0, stream>>>(a, ntasks);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    forest_steps_from(a.D, a.D - levels, a.N, phase, steps);
+  } else {
+    forest_steps(a.D, a.N, phase, steps);
+  }
   for (const ForestStep& st : steps) {
     if (st.kind == 0) {
       uint32_t grid = st.ctas;
@@ -572,15 +778,22 @@ cudaError_t launch_forest(const ForestArgs& a, int phase, cudaStream_t stream, i
   return cudaSuccess;
 }
 
-int forest_launch_count(uint32_t D, int phase) {
+int forest_launch_count(uint32_t n, uint32_t D, int phase) {
   std::vector<ForestStep> steps;
+  if (warp_bands(n, D, phase)) {
+    forest_steps_from(D, D - (phase == 1 ? WB1_LEVELS : WB2_LEVELS), 2, phase, steps);
+    return 1 + (int)steps.size();
+  }
   forest_steps(D, D == 0 ? 1 : 2, phase, steps);
   return (int)steps.size();
 }
 
 cudaError_t launch_forest_seg(const ForestSeg& s, int phase, int kind, uint32_t ctas, cudaStream_t stream) {
   if (ctas == 0) return cudaSuccess;
-  if (kind == 0) {
+  if (kind == 2) {
+    if (phase == 1) forest_warp1_seg<<<ctas, WB_THREADS, 0, stream>>>(s);
+    else forest_warp2_seg<<<ctas, WB_THREADS, 0, stream>>>(s);
+  } else if (kind == 0) {
     if (phase == 1) forest_first_seg<<<ctas, FAST_THREADS, 0, stream>>>(s);
     else forest_fast_seg<2><<<ctas, FAST_THREADS, 0, stream>>>(s);
   } else {

@@ -100,18 +100,52 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait: gives up after `limit` polls (each try_wait may suspend for a while in
-// hardware), records the timeout and returns false.  Never spins forever.
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+constexpr uint32_t MBAR_WAIT_POLLS = 1u << 24;
+// Bounded wait: gives up after MBAR_WAIT_POLLS polls (each try_wait may suspend for a while in
+// hardware), or early once another warp of the CTA has given up, records the timeout and
+// returns false.  Never spins forever.  `test_polls` != 0 replaces the bound by that many
+// non-blocking polls (a test of this give-up path: the first stage has not landed that soon).
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, DevStatus* st,
-                                                  volatile int* abort_flag) {
-  const uint32_t limit = 1u << 24;
-  for (uint32_t i = 0; i < limit; i++) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if ((i & 1023u) == 1023u && *abort_flag) return false;
+                                                  volatile int* abort_flag, uint32_t test_polls = 0) {
+  if (test_polls) {
+    for (uint32_t i = 0; i < test_polls; i++)
+      if (mbar_test_wait(bar, parity)) return true;
+  } else {
+    for (uint32_t i = 0; i < MBAR_WAIT_POLLS; i++) {
+      if (mbar_try_wait(bar, parity)) return true;
+      if ((i & 1023u) == 1023u && *abort_flag) return false;
+    }
   }
   set_error(st, DERR_WAIT_TIMEOUT, 1);
   *abort_flag = 1;
   return false;
+}
+// A consumer warp's wait for a staged tile: every lane polls, and the warp goes on together if
+// any lane saw the phase complete (completion is monotonic: the phase cannot move on before
+// this warp releases the stage), so no lane leaves while the others reach a __syncwarp.
+__device__ __forceinline__ bool warp_wait_full(uint64_t* bar, uint32_t parity, DevStatus* st,
+                                               volatile int* abort_flag, uint32_t test_polls) {
+  const bool ok = mbar_wait_bounded(bar, parity, st, abort_flag, test_polls);
+  return __any_sync(0xffffffffu, ok);
+}
+// Wait for a copy this CTA issued, before the CTA may exit: copies in flight write into its
+// shared memory.  Unlike mbar_wait_bounded it does not give up because another warp did (that
+// is when it runs), only after the full bound, which a copy from valid memory never reaches.
+__device__ __forceinline__ void mbar_wait_drain(uint64_t* bar, uint32_t parity, DevStatus* st) {
+  for (uint32_t i = 0; i < MBAR_WAIT_POLLS; i++)
+    if (mbar_try_wait(bar, parity)) return;
+  set_error(st, DERR_WAIT_TIMEOUT, 2);
 }
 // a tensor map read from global memory (written there by a copy before this launch)
 __device__ __forceinline__ void tensormap_acquire(const CUtensorMap* map) {
@@ -139,7 +173,8 @@ __device__ __forceinline__ uint32_t swz(uint32_t o) {
 
 // fold the U-byte segment of row `row` of a staged tile into a lane's running digest state
 template <int U, int KIND>
-__device__ __forceinline__ void hash_segment(const uint8_t* stage, uint32_t row, Murmur3& mm, uint32_t md[4]) {
+__device__ __forceinline__ void hash_segment(const uint8_t* stage, uint32_t row, Murmur3& mm, uint32_t md[4],
+                                             uint32_t one) {
   const uint32_t base = row * U;
   if constexpr (KIND == HASH_MD5) {
 #pragma unroll
@@ -150,7 +185,7 @@ __device__ __forceinline__ void hash_segment(const uint8_t* stage, uint32_t row,
         const uint4 v = *reinterpret_cast<const uint4*>(stage + swz<U>(base + blk * 64u + 16u * j));
         m[4 * j + 0] = v.x; m[4 * j + 1] = v.y; m[4 * j + 2] = v.z; m[4 * j + 3] = v.w;
       }
-      md5_compress(md, m);
+      md5_compress_fma(md, m, one);
     }
   } else {
 #pragma unroll
@@ -161,9 +196,16 @@ __device__ __forceinline__ void hash_segment(const uint8_t* stage, uint32_t row,
   }
 }
 template <int KIND>
-__device__ __forceinline__ Digest finish_segments(Murmur3& mm, uint32_t md[4], uint32_t cs) {
+__device__ __forceinline__ Digest finish_segments(Murmur3& mm, uint32_t md[4], uint32_t cs, uint32_t one) {
   if constexpr (KIND == HASH_MD5) {
-    md5_pad_block64(md, cs);
+    // the padding block of a message of whole 64-byte blocks (md5_pad_block64)
+    uint32_t m[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) m[i] = 0;
+    m[0] = 0x80u;
+    m[14] = cs << 3;
+    m[15] = cs >> 29;
+    md5_compress_fma(md, m, one);
     return md5_digest(md);
   } else {
     return mm.finish(cs);
@@ -206,7 +248,10 @@ __global__ void __launch_bounds__((TMA_CONSUMER_WARPS + 1) * 32)
       for (uint32_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
         for (uint32_t g = 0; g < S; g++, k++) {
           const uint32_t s = k % stages, ph = (k / stages) & 1u;
-          if (k >= stages && !mbar_wait_bounded(&empty[s], ph ^ 1u, a.st, &abort_flag)) { ok = false; break; }
+          if (k >= stages && !mbar_wait_bounded(&empty[s], ph ^ 1u, a.st, &abort_flag, a.wait_polls)) {
+            ok = false;
+            break;
+          }
           mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
           tma_load_3d(smem + (size_t)s * STAGE_BYTES, &tmap, &full[s], 0, (int)g, (int)(t * R));
         }
@@ -214,10 +259,9 @@ __global__ void __launch_bounds__((TMA_CONSUMER_WARPS + 1) * 32)
       // wait for this CTA's copies still in flight before the CTA may exit
       const uint32_t issued = k;
       const uint32_t first = issued > stages ? issued - stages : 0;
-      for (uint32_t q = first; q < issued; q++)
-        mbar_wait_bounded(&full[q % stages], (q / stages) & 1u, a.st, &abort_flag);
+      for (uint32_t q = first; q < issued; q++) mbar_wait_drain(&full[q % stages], (q / stages) & 1u, a.st);
       // the short last chunk (len not a multiple of cs) is hashed here with byte loads
-      if (blockIdx.x == 0 && nfull < a.n) {
+      if (ok && blockIdx.x == 0 && nfull < a.n) {
         for (uint64_t c = nfull; c < a.n; c++) {
           const uint64_t off = c * a.cs;
           const uint64_t nb = (c == a.n - 1u) ? a.len - off : a.cs;
@@ -244,13 +288,13 @@ __global__ void __launch_bounds__((TMA_CONSUMER_WARPS + 1) * 32)
     md5_init(md);
     for (uint32_t g = 0; g < S; g++, k++) {
       const uint32_t s = k % stages, ph = (k / stages) & 1u;
-      if (!mbar_wait_bounded(&full[s], ph, a.st, &abort_flag)) return;
+      if (!warp_wait_full(&full[s], ph, a.st, &abort_flag, a.wait_polls)) return;
       const uint8_t* stage = smem + (size_t)s * STAGE_BYTES;
-      if (valid) hash_segment<U, KIND>(stage, row, mm, md);
+      if (valid) hash_segment<U, KIND>(stage, row, mm, md, a.one);
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
     }
-    if (valid) leaf_finish(a, chunk, finish_segments<KIND>(mm, md, a.cs), old);
+    if (valid) leaf_finish(a, chunk, finish_segments<KIND>(mm, md, a.cs, a.one), old);
   }
 }
 
@@ -319,8 +363,7 @@ __global__ void __launch_bounds__((TMA_CONSUMER_WARPS + 1) * 32)
       const uint32_t issued = k;
       // wait for this CTA's copies still in flight (before the sentinel reuses a stage's barrier)
       const uint32_t first = issued > stages ? issued - stages : 0;
-      for (uint32_t q = first; q < issued; q++)
-        mbar_wait_bounded(&full[q % stages], (q / stages) & 1u, st, &abort_flag);
+      for (uint32_t q = first; q < issued; q++) mbar_wait_drain(&full[q % stages], (q / stages) & 1u, st);
       if (ok) {   // sentinel: a stage with no data whose owner says "done"
         const uint32_t s = k % stages, ph = (k / stages) & 1u;
         if (k < stages || mbar_wait_bounded(&empty[s], ph ^ 1u, st, &abort_flag)) {
@@ -349,7 +392,7 @@ __global__ void __launch_bounds__((TMA_CONSUMER_WARPS + 1) * 32)
   bool valid = false;
   for (uint32_t k = 0;; k++) {
     const uint32_t s = k % stages, ph = (k / stages) & 1u;
-    if (!mbar_wait_bounded(&full[s], ph, st, &abort_flag)) return;
+    if (!warp_wait_full(&full[s], ph, st, &abort_flag, 0)) return;
     const uint32_t it = slot_item[s];
     if (it == NO_ITEM) break;
     const uint32_t tile = slot_tile[s], g = slot_seg[s];
@@ -362,12 +405,12 @@ __global__ void __launch_bounds__((TMA_CONSUMER_WARPS + 1) * 32)
       old.w[0] = old.w[1] = old.w[2] = old.w[3] = 0u;
       if (valid) old = prior_digest(with_round(items[it].args), chunk);
     }
-    if (valid) hash_segment<U, KIND>(smem + (size_t)s * STAGE_BYTES, row, mm, md);
+    if (valid) hash_segment<U, KIND>(smem + (size_t)s * STAGE_BYTES, row, mm, md, items[it].args.one);
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
     if (g + 1 == S && valid) {
       const LeafArgs a = with_round(items[it].args);
-      leaf_finish(a, chunk, finish_segments<KIND>(mm, md, a.cs), old);
+      leaf_finish(a, chunk, finish_segments<KIND>(mm, md, a.cs, a.one), old);
     }
   }
 }

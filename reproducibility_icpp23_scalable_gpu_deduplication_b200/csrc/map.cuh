@@ -5,34 +5,29 @@
 //   insert(key, value): insert-if-absent; reports inserted vs existing plus the slot;
 //   the slot's value stays mutable for the lowest-index update (tree_approach.cpp:85,339).
 //
-// Slot layout (32 bytes, one quarter of a 128-byte line):
-//   key  : two u64 words, claimed with one 128-bit atomicCAS (EMPTY = all ones)
-//   val  : u64 = priority << 45 | checkpoint << 32 | node.  Every insert of the current
-//          checkpoint applies atomicMin to it; within one checkpoint the checkpoint field is
-//          the same, so the value left behind is the one the reference's sequential execution
-//          order inserts first (leaves by index, then first-occurrence parents by level and
-//          index, then the baseline's per-level inserts).  One atomic sets the owner and its
-//          checkpoint together.  All ones (checkpoint field MAP_TREE_PENDING) while the
-//          inserting thread has claimed the key but not yet merged its value: readers treat
-//          that as "this checkpoint".  Checkpoint ids are below MAP_TREE_PENDING.
-// The digest equal to the EMPTY pattern is kept in one extra slot at index `cap`.
+// Table layout (24 bytes per slot, in one allocation of cap + 1 slots):
+//   keys[i] : the 128-bit digest, claimed with one 128-bit atomicCAS (EMPTY = all ones); the
+//             keys sit together (eight to a 128-byte line), so a probe sequence reads only keys
+//   vals[i] : u64 = priority << 45 | checkpoint << 32 | node.  Every insert of the current
+//             checkpoint applies atomicMin to it; within one checkpoint the checkpoint field is
+//             the same, so the value left behind is the one the reference's sequential
+//             execution order inserts first (leaves by index, then first-occurrence parents by
+//             level and index, then the baseline's per-level inserts).  One atomic sets the
+//             owner and its checkpoint together.  All ones (checkpoint field MAP_TREE_PENDING)
+//             while the inserting thread has claimed the key but not yet merged its value:
+//             readers treat that as "this checkpoint".  Checkpoint ids are below
+//             MAP_TREE_PENDING.
+// The digest equal to the EMPTY pattern is kept in the extra slot `cap`: present once its
+// value is no longer all ones.
 #pragma once
 #include "common.cuh"
 
 namespace b2d {
 
-struct __align__(32) MapSlot {
-  unsigned long long key_lo;
-  unsigned long long key_hi;
-  unsigned long long val;
-  uint32_t spare;
-  uint32_t pad;        // special slot only: 1 once occupied
-};
-static_assert(sizeof(MapSlot) == 32, "slot must be 32 bytes");
-
 struct __align__(16) Key128 {
   unsigned long long lo, hi;
 };
+constexpr uint64_t MAP_SLOT_BYTES = sizeof(Key128) + sizeof(unsigned long long);
 
 constexpr unsigned long long MAP_EMPTY = ~0ull;
 constexpr uint32_t MAP_TREE_BITS = 13;
@@ -48,11 +43,21 @@ __device__ __forceinline__ uint32_t map_val_tree(unsigned long long v) {
 }
 
 struct MapView {
-  MapSlot* slots;      // cap + 1 slots
-  uint64_t cap;        // any positive count (homes are mapped onto [0, cap) by a multiply)
+  Key128* keys;               // cap + 1 keys
+  unsigned long long* vals;   // cap + 1 values, right behind the keys
+  uint64_t cap;               // any positive count (homes are mapped onto [0, cap) by a multiply)
   unsigned long long* size;   // device counter of occupied slots
-  uint64_t pad;
 };
+
+// keys and values of a table of `cap` slots (+ the extra slot) at `mem`
+__host__ __device__ __forceinline__ MapView map_at(void* mem, uint64_t cap, unsigned long long* size) {
+  MapView m;
+  m.keys = static_cast<Key128*>(mem);
+  m.vals = reinterpret_cast<unsigned long long*>(m.keys + cap + 1);
+  m.cap = cap;
+  m.size = size;
+  return m;
+}
 
 struct MapRef {
   uint64_t slot;       // valid when found
@@ -84,16 +89,12 @@ __device__ __forceinline__ uint64_t map_next(uint64_t i, uint64_t cap) { return 
 // before the launch).  Returns cap+1 when absent.
 __device__ __forceinline__ uint64_t map_find(const MapView& m, const Digest& d) {
   const Key128 k = digest_key(d);
-  if (key_is_empty_pattern(k)) {
-    const MapSlot& s = m.slots[m.cap];
-    return s.pad ? m.cap : m.cap + 1;
-  }
+  if (key_is_empty_pattern(k)) return m.vals[m.cap] != MAP_EMPTY ? m.cap : m.cap + 1;
   uint64_t i = map_home(k, m.cap);
   for (uint64_t probe = 0; probe < m.cap; probe++) {
-    const MapSlot* s = &m.slots[i];
-    const unsigned long long lo = s->key_lo, hi = s->key_hi;
-    if (lo == k.lo && hi == k.hi) return i;
-    if (lo == MAP_EMPTY && hi == MAP_EMPTY) return m.cap + 1;
+    const Key128 s = m.keys[i];
+    if (s.lo == k.lo && s.hi == k.hi) return i;
+    if (s.lo == MAP_EMPTY && s.hi == MAP_EMPTY) return m.cap + 1;
     i = map_next(i, m.cap);
   }
   return m.cap + 1;
@@ -107,10 +108,6 @@ __device__ __forceinline__ void count_insert(unsigned long long* size) {
   if (lane == (unsigned)(__ffs(am) - 1)) atomicAdd(size, (unsigned long long)__popc(am));
 }
 
-__device__ __forceinline__ Key128 atomic_cas_key(MapSlot* s, Key128 cmp, Key128 val) {
-  return atomicCAS(reinterpret_cast<Key128*>(&s->key_lo), cmp, val);
-}
-
 // Insert-if-absent of an already packed value (map_pack).  On success the value is merged
 // with atomicMin.  On an existing key nothing is written here; the caller decides (through
 // map_merge_current) whether the entry belongs to the current checkpoint.
@@ -119,12 +116,11 @@ __device__ __forceinline__ MapRef map_insert_packed(const MapView& m, const Dige
   const Key128 k = digest_key(d);
   MapRef r{0, false, false, ~0ull};
   if (key_is_empty_pattern(k)) {
-    MapSlot* s = &m.slots[m.cap];
-    const uint32_t old = atomicCAS(&s->pad, 0u, 1u);
-    r.prev = atomicMin(&s->val, val);
+    // the extra slot: the first value merged into it inserts the key
+    r.prev = atomicMin(&m.vals[m.cap], val);
     r.slot = m.cap;
     r.found = true;
-    r.inserted = (old == 0u);
+    r.inserted = r.prev == MAP_EMPTY;
     if (r.inserted) atomicAdd(m.size, 1ull);   // one slot, rare: no aggregation needed
     return r;
   }
@@ -133,11 +129,11 @@ __device__ __forceinline__ MapRef map_insert_packed(const MapView& m, const Dige
   const Key128 empty{MAP_EMPTY, MAP_EMPTY};
   uint64_t i = map_home(k, m.cap);
   for (uint64_t probe = 0; probe < m.cap; probe++) {
-    MapSlot* s = &m.slots[i];
+    Key128* s = &m.keys[i];
     bool try_cas = true;
     if (!cas_only) {
-      const unsigned long long lo = *reinterpret_cast<volatile unsigned long long*>(&s->key_lo);
-      const unsigned long long hi = *reinterpret_cast<volatile unsigned long long*>(&s->key_hi);
+      const unsigned long long lo = *reinterpret_cast<volatile unsigned long long*>(&s->lo);
+      const unsigned long long hi = *reinterpret_cast<volatile unsigned long long*>(&s->hi);
       if (lo == k.lo && hi == k.hi) {
         r.slot = i; r.found = true; r.inserted = false;
         return r;
@@ -147,9 +143,9 @@ __device__ __forceinline__ MapRef map_insert_packed(const MapView& m, const Dige
       try_cas = (lo == MAP_EMPTY) || (hi == MAP_EMPTY);
     }
     if (try_cas) {
-      const Key128 old = atomic_cas_key(s, empty, k);
+      const Key128 old = atomicCAS(s, empty, k);
       if (old.lo == MAP_EMPTY && old.hi == MAP_EMPTY) {
-        r.prev = atomicMin(&s->val, val);
+        r.prev = atomicMin(&m.vals[i], val);
         count_insert(m.size);
         r.slot = i; r.found = true; r.inserted = true;
         return r;
@@ -177,10 +173,10 @@ __device__ __forceinline__ MapRef map_insert(const MapView& m, const Digest& d, 
 // older checkpoint is never changed by this one, so its id cannot change under the test.
 __device__ __forceinline__ bool map_merge_current(const MapView& m, uint64_t slot, unsigned long long val,
                                                   uint32_t cur, unsigned long long* prev = nullptr) {
-  MapSlot* s = &m.slots[slot];
-  const uint32_t t = map_val_tree(*reinterpret_cast<volatile unsigned long long*>(&s->val));
+  unsigned long long* v = &m.vals[slot];
+  const uint32_t t = map_val_tree(*reinterpret_cast<volatile unsigned long long*>(v));
   if (t == (cur & MAP_TREE_PENDING) || t == MAP_TREE_PENDING) {
-    const unsigned long long p = atomicMin(&s->val, map_pack(val, cur));
+    const unsigned long long p = atomicMin(v, map_pack(val, cur));
     if (prev) *prev = p;
     return true;
   }
@@ -188,10 +184,10 @@ __device__ __forceinline__ bool map_merge_current(const MapView& m, uint64_t slo
 }
 
 __device__ __forceinline__ uint32_t map_node(const MapView& m, uint64_t slot) {
-  return (uint32_t)(m.slots[slot].val & 0xffffffffull);
+  return (uint32_t)(m.vals[slot] & 0xffffffffull);
 }
 __device__ __forceinline__ uint32_t map_tree(const MapView& m, uint64_t slot) {
-  return map_val_tree(m.slots[slot].val);
+  return map_val_tree(m.vals[slot]);
 }
 
 }  // namespace b2d
