@@ -249,7 +249,10 @@ class CheckpointServer:
                          [r.baseline for r in batch], stream=stream)
             except Exception as e:   # noqa: BLE001 - the status travels with the requests
                 # nothing of the batch runs: its requests complete now with the error, and
-                # their clients' next requests are baselines
+                # their clients' next requests are baselines.  Handles prepared before the
+                # failure may have queued work on this slot's stream; it completes before their
+                # clients become idle (their next batch may run on another slot's stream).
+                stream.synchronize()
                 done = self.clock()
                 for r in batch:
                     r.done = done

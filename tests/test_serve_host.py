@@ -30,6 +30,9 @@ class FakeStream:
     def wait_event(self, ev):
         pass
 
+    def synchronize(self):
+        LOG["stream_syncs"].append(self)
+
 
 class FakeHandle:
     grow = 0              # bytes a handle's memory grows by per checkpoint
@@ -325,6 +328,8 @@ def test_failed_launch_completes_its_requests(fakes, monkeypatch):
     r = [srv.submit(c, buf(1)) for c in range(2)]
     srv.drain()
     assert [x.rc for x in r] == [-2, -2] and all(x.done is not None for x in r)
+    # the slot's stream was synchronised before those clients became idle again
+    assert len(fakes["stream_syncs"]) == 1
     assert not srv.busy(0) and not srv.busy(1)
     r2 = [srv.submit(c, buf(2)) for c in range(2)]
     srv.drain()
