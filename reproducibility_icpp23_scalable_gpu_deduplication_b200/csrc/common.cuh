@@ -5,8 +5,8 @@
 //                            (include/kokkos_merkle_tree.hpp:30-33 of the reference)
 //   lab    : uint8_t[N]      per-node labels (leaf labels + band-top labels), rewritten
 //                            every checkpoint (include/utils.hpp:51-57 Label values)
-//   push   : uint8_t[N]      region-root flags set by each node's parent: 1 first-occurrence
-//                            root, 2 shifted-duplicate root
+//   push   : 2 bits per node region-root flags set by each node's parent: 1 first-occurrence
+//                            root, 2 shifted-duplicate root (16 nodes per 32-bit word)
 //   map    : cap+1 keys (16 B) then cap+1 values (8 B): open-addressing digest -> NodeID
 //            table, 24 B per slot (map.cuh)
 #pragma once

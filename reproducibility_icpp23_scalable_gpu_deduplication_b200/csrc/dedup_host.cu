@@ -442,9 +442,10 @@ int prepare_checkpoint(b2d_dedup* d, const void* d_data, uint64_t len, bool make
     B2D_CU(d->dupflag.reserve(d->n));
     B2D_CU(cudaMemsetAsync(d->dupflag.p, 0, d->dupflag.n, d->stream));
   }
-  if (d->push.n < d->N + 16ull || !d->push.p) {
+  const uint64_t push_bytes = ((uint64_t)d->N + 63ull) / 64ull * 16ull + 16ull;   // 2 bits per node
+  if (d->push.n < push_bytes || !d->push.p) {
     // flags stay all-zero between checkpoints (the compaction clears what it reads)
-    B2D_CU(d->push.reserve(((uint64_t)d->N + 15ull) / 16ull * 16ull + 16ull));
+    B2D_CU(d->push.reserve(push_bytes));
     B2D_CU(cudaMemsetAsync(d->push.p, 0, d->push.n, d->stream));
   }
   if (baseline) {
@@ -2021,7 +2022,7 @@ int b2d_estimate_memory(uint64_t len, uint32_t chunk_size, int map_max_load_pct,
   // the allocations prepare_checkpoint makes for a buffer of `len` bytes (checkpoint side)
   const uint64_t n = (len + chunk_size - 1) / chunk_size, N = 2 * n - 1;
   const uint64_t cap = map_capacity(2 * N, map_max_load_pct / 100.0, MAP_HEADROOM);
-  uint64_t b = N * sizeof(Digest) + N + (n + 16) + ((N + 15) / 16 * 16 + 16) + n;   // tree, labels, flags
+  uint64_t b = N * sizeof(Digest) + N + (n + 16) + ((N + 63) / 64 * 16 + 16) + n;   // tree, labels, flags
   b += (cap + 1) * MAP_SLOT_BYTES + 8;                                               // map
   b += 8 * 4 * n + 68 * 4;                                                           // lists and keys
   b += (uint64_t)64 * 4 * 2 + (uint64_t)1184 * 64 * 4 + 2 * COMPACT_GRID * 4;           // buckets, partials

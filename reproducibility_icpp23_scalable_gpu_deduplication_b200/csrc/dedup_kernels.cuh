@@ -106,6 +106,31 @@ struct DiffArgs {
                           // n - 1, so leaf heap indices become chunk indices; tree: 0)
 };
 
+// Programmatic dependent launch (sm_90 and later).  The forest and diff-assembly kernels of one
+// checkpoint are launched with launch_dependent(): each may be scheduled while the kernel before
+// it on the stream is still finishing, because every such kernel first lets its own successor
+// launch and then waits (griddepcontrol.wait) until its predecessor has completed and its memory
+// is visible, before it reads anything.  Launched the ordinary way, both are no-ops.
+__device__ __forceinline__ void griddep_enter() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+template <typename... KArgs, typename... Args>
+cudaError_t launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                             Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // launch parameters carry the buffer geometry; the per-checkpoint values come from *rs
 __device__ __forceinline__ LeafArgs with_round(const LeafArgs& p) {
   LeafArgs a = p;

@@ -22,8 +22,8 @@
 //   every inner node (:218-224); this is reproduced with `zero_exists`.
 // Map priorities reproduce the sequential insert order: leaves 0, phase-1 parents
 // 1 + height, baseline per-level inserts 64 + height (height = D - level).
-// `push` holds only nonzero flags: it is all-zero between checkpoints (the compaction clears
-// what it reads), so a region-free subtree writes nothing.
+// `push` holds 2-bit flags, set with atomicOr (16 nodes share a word): it is all-zero between
+// checkpoints (the compaction clears what it reads), so a region-free subtree writes nothing.
 #include <vector>
 
 #include "dedup_kernels.cuh"
@@ -50,6 +50,10 @@ constexpr uint8_t NONE_LABEL = 5;         // node index beyond the tree
 
 __device__ __forceinline__ uint8_t push_flag(uint8_t label) {
   return label == SHIFT_DUPL ? PUSH_SHIFT : (label == FIRST_OCUR ? PUSH_FIRST : PUSH_NONE);
+}
+// region-root flag of node x: 2 bits per node, 16 nodes per word (gather.cu reads them)
+__device__ __forceinline__ void push_set(uint8_t* push, uint64_t x, uint32_t flag) {
+  atomicOr(reinterpret_cast<uint32_t*>(push) + (x >> 4), flag << (2u * (uint32_t)(x & 15u)));
 }
 
 // phase-1 parent insert, priority 1 + height (:133, :390).  The rare heavy paths (hashing,
@@ -80,8 +84,8 @@ __device__ __noinline__ uint8_t shift_pair(const ForestArgs& a, uint32_t x) {
     exists = map_find(a.map, d) <= a.map.cap;
   }
   if (exists) return SHIFT_DUPL;
-  a.push[l] = PUSH_SHIFT;
-  a.push[r] = PUSH_SHIFT;
+  push_set(a.push, l, PUSH_SHIFT);
+  push_set(a.push, r, PUSH_SHIFT);
   return DONE;
 }
 
@@ -110,8 +114,8 @@ __device__ __forceinline__ uint8_t forest_node(const ForestArgs& a, uint32_t x, 
     if (ll != rl) {
       out = DONE;
       const uint8_t pl = push_flag(ll), pr = push_flag(rl);
-      if (pl) a.push[2u * x + 1u] = pl;
-      if (pr) a.push[2u * x + 2u] = pr;
+      if (pl) push_set(a.push, 2u * x + 1u, pl);
+      if (pr) push_set(a.push, 2u * x + 2u, pr);
     } else if (ll == SHIFT_DUPL) {
       out = shift_pair(a, x);
     } else {
@@ -171,7 +175,7 @@ __device__ __forceinline__ uint8_t input_label(const ForestArgs& a, uint64_t x) 
 template <int PHASE>
 __device__ __forceinline__ void band_output(const ForestArgs& a, uint64_t x, uint8_t lab) {
   if (x == 0) {
-    if (PHASE == 2 && a.n >= 2u && lab == FIRST_OCUR) a.push[0] = PUSH_FIRST;
+    if (PHASE == 2 && a.n >= 2u && lab == FIRST_OCUR) push_set(a.push, 0, PUSH_FIRST);
   } else if (x < (uint64_t)a.n - 1u) {
     a.lab[x] = lab;
   }
@@ -360,6 +364,7 @@ __device__ __forceinline__ void forest_first_body(const ForestArgs& a, uint32_t 
 #endif
 __global__ void __launch_bounds__(FAST_THREADS, B2D_FF_MINB) forest_first_kernel(ForestArgs a0, uint32_t in,
                                                                                   uint32_t nbands) {
+  griddep_enter();
   const ForestArgs a = with_round(a0);
   for (uint32_t bid = blockIdx.x; bid < nbands; bid += gridDim.x) {
     forest_first_body(a, bid, in);
@@ -460,6 +465,7 @@ __device__ __forceinline__ void forest_fast_body(const ForestArgs& a, uint32_t b
 template <int PHASE>
 __global__ void __launch_bounds__(FAST_THREADS, B2D_FAST_MINB) forest_fast_kernel(ForestArgs a0, uint32_t in,
                                                                                   uint32_t nbands) {
+  griddep_enter();
   const ForestArgs a = with_round(a0);
   for (uint32_t bid = blockIdx.x; bid < nbands; bid += gridDim.x) {
     forest_fast_body<PHASE>(a, bid, in);
@@ -600,6 +606,7 @@ __device__ __forceinline__ void warp2_task(const ForestArgs& a, uint32_t task, u
 
 // Resident grid of warps; warp g takes tasks g, g + G, ... and loads the next one's labels first.
 __global__ void __launch_bounds__(WB_THREADS) forest_warp1_kernel(ForestArgs a0, uint32_t ntasks) {
+  griddep_enter();
   const ForestArgs a = with_round(a0);
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t G = (gridDim.x * WB_THREADS) >> 5;
@@ -614,6 +621,7 @@ __global__ void __launch_bounds__(WB_THREADS) forest_warp1_kernel(ForestArgs a0,
   }
 }
 __global__ void __launch_bounds__(WB_THREADS) forest_warp2_kernel(ForestArgs a0, uint32_t ntasks) {
+  griddep_enter();
   const ForestArgs a = with_round(a0);
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t G = (gridDim.x * WB_THREADS) >> 5;
@@ -681,6 +689,7 @@ __device__ __forceinline__ void forest_band_body(const ForestArgs& a, uint32_t b
 }
 template <int PHASE>
 __global__ void __launch_bounds__(FOREST_THREADS) forest_band_kernel(ForestArgs a0, uint32_t top, uint32_t bot) {
+  griddep_enter();
   forest_band_body<PHASE>(with_round(a0), blockIdx.x, top, bot);
 }
 template <int PHASE>
@@ -753,26 +762,25 @@ cudaError_t launch_forest(const ForestArgs& a, int phase, cudaStream_t stream, i
     const uint32_t want = (ntasks + WB_THREADS / 32u - 1u) / (WB_THREADS / 32u);
     const uint32_t cap = (phase == 1 ? res_w1 : res_w2) * (uint32_t)(sm_count > 0 ? sm_count : 1);
     const uint32_t grid = want < cap ? want : cap;
-    if (phase == 1) forest_warp1_kernel<<<grid, WB_THREADS, 0, stream>>>(a, ntasks);
-    else forest_warp2_kernel<<<grid, WB_THREADS, 0, stream>>>(a, ntasks);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = phase == 1 ? launch_dependent(forest_warp1_kernel, grid, WB_THREADS, 0, stream, a, ntasks)
+                               : launch_dependent(forest_warp2_kernel, grid, WB_THREADS, 0, stream, a, ntasks);
     if (e != cudaSuccess) return e;
     forest_steps_from(a.D, a.D - levels, a.N, phase, steps);
   } else {
     forest_steps(a.D, a.N, phase, steps);
   }
   for (const ForestStep& st : steps) {
+    cudaError_t e;
     if (st.kind == 0) {
       uint32_t grid = st.ctas;
       const uint32_t cap = (phase == 1 ? res_first : res_fast) * (uint32_t)(sm_count > 0 ? sm_count : 0);
       if (B2D_FOREST_PERSIST && cap && grid > cap) grid = cap;
-      if (phase == 1) forest_first_kernel<<<grid, FAST_THREADS, 0, stream>>>(a, st.p0, st.ctas);
-      else forest_fast_kernel<2><<<grid, FAST_THREADS, 0, stream>>>(a, st.p0, st.ctas);
+      e = phase == 1 ? launch_dependent(forest_first_kernel, grid, FAST_THREADS, 0, stream, a, st.p0, st.ctas)
+                     : launch_dependent(forest_fast_kernel<2>, grid, FAST_THREADS, 0, stream, a, st.p0, st.ctas);
     } else {
-      if (phase == 1) forest_band_kernel<1><<<st.ctas, FOREST_THREADS, 0, stream>>>(a, st.p0, st.p1);
-      else forest_band_kernel<2><<<st.ctas, FOREST_THREADS, 0, stream>>>(a, st.p0, st.p1);
+      e = phase == 1 ? launch_dependent(forest_band_kernel<1>, st.ctas, FOREST_THREADS, 0, stream, a, st.p0, st.p1)
+                     : launch_dependent(forest_band_kernel<2>, st.ctas, FOREST_THREADS, 0, stream, a, st.p0, st.p1);
     }
-    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -810,7 +818,10 @@ __device__ __forceinline__ void zero_exists_kernel_body(int* flag, const RoundSt
   const MapView m = rs->map;
   *flag = map_find(m, z) <= m.cap ? 1 : 0;
 }
-__global__ void zero_exists_kernel(int* flag, const RoundState* rs) { zero_exists_kernel_body(flag, rs); }
+__global__ void zero_exists_kernel(int* flag, const RoundState* rs) {
+  griddep_enter();
+  zero_exists_kernel_body(flag, rs);
+}
 
 __global__ void zero_exists_seg(const ForestArgs* args, uint32_t n) {
   const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
@@ -823,8 +834,7 @@ cudaError_t launch_zero_exists_seg(const ForestArgs* args, uint32_t n, cudaStrea
 }
 
 cudaError_t launch_zero_exists(int* flag, const RoundState* rs, cudaStream_t stream) {
-  zero_exists_kernel<<<1, 1, 0, stream>>>(flag, rs);
-  return cudaGetLastError();
+  return launch_dependent(zero_exists_kernel, 1, 1, 0, stream, flag, rs);
 }
 
 // List approach (src/list_approach.cpp:41-71): a changed chunk whose digest was new is a first
@@ -834,6 +844,7 @@ cudaError_t launch_zero_exists(int* flag, const RoundState* rs, cudaStream_t str
 // entry's owner after the leaf stage's minimum, so the others become shifted duplicates.  The
 // region flags for the diff are set per chunk (its leaf), and the duplicate flags are cleared.
 __global__ void list_label_kernel(ForestArgs a0) {
+  griddep_enter();
   const ForestArgs a = with_round(a0);
   for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < a.n; c += (uint64_t)gridDim.x * blockDim.x) {
     uint8_t lab = a.leaflab[c];
@@ -852,8 +863,8 @@ __global__ void list_label_kernel(ForestArgs a0) {
         }
       }
     }
-    if (lab == FIRST_OCUR) a.push[leaf] = PUSH_FIRST;
-    else if (lab == SHIFT_DUPL) a.push[leaf] = PUSH_SHIFT;
+    if (lab == FIRST_OCUR) push_set(a.push, leaf, PUSH_FIRST);
+    else if (lab == SHIFT_DUPL) push_set(a.push, leaf, PUSH_SHIFT);
   }
 }
 
@@ -861,8 +872,7 @@ cudaError_t launch_list_label(const ForestArgs& a, int sm_count, cudaStream_t st
   const uint64_t want = ((uint64_t)a.n + 255u) / 256u;
   const uint64_t cap = (uint64_t)sm_count * 8u;
   const uint32_t grid = (uint32_t)(want < cap ? (want ? want : 1) : cap);
-  list_label_kernel<<<grid, 256, 0, stream>>>(a);
-  return cudaGetLastError();
+  return launch_dependent(list_label_kernel, grid, 256, 0, stream, a);
 }
 
 

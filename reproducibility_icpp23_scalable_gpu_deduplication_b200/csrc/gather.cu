@@ -40,36 +40,39 @@ __device__ __forceinline__ uint32_t seg_locate(const SegGrid& s, uint32_t& bid, 
 }
 constexpr uint32_t SHIFT_GRID = 296;    // at most 2 x 148 ranges for the shift-entry passes
 
-// Region roots are flagged in `push` (node-indexed, zero-padded to a multiple of 16 nodes,
-// all-zero between checkpoints).  Compaction runs in node order with 16-byte loads; since the
+// Region roots are flagged in `push`: 2 bits per node (PUSH_FIRST = 1, PUSH_SHIFT = 2), 16 nodes
+// per 32-bit word, zero-padded to a multiple of 64 nodes, all-zero between checkpoints (a quarter
+// of the bytes of one flag byte per node, so the two passes below read 16 MB instead of 64 MB
+// for a 2^26-node tree).  Compaction runs in node order with 16-byte loads of 64 nodes; since the
 // canonical order is "level descending, node ascending" and node order is "level ascending,
 // node ascending", the canonical list is the node-order list with its per-level runs reversed,
 // which compact_permute_kernel applies after a per-level split of the node-order lists.
+constexpr uint32_t PUSH_GROUP = 64;   // nodes per 16-byte load
 __device__ __forceinline__ uint4 ld_push16(const uint8_t* push, uint64_t g) {
   return reinterpret_cast<const uint4*>(push)[g];
 }
-__device__ __forceinline__ void count16(uint4 v, uint32_t& cf, uint32_t& cs) {
-  const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-  for (int k = 0; k < 4; k++) {
-#pragma unroll
-    for (int b = 0; b < 4; b++) {
-      const uint32_t f = (w[k] >> (8 * b)) & 0xffu;
-      cf += f == PUSH_FIRST;
-      cs += f == PUSH_SHIFT;
-    }
-  }
+// one bit (the low bit of each 2-bit field) per node flagged first / shifted
+__device__ __forceinline__ uint32_t push_first_bits(uint32_t w) { return w & ~(w >> 1) & 0x55555555u; }
+__device__ __forceinline__ uint32_t push_shift_bits(uint32_t w) { return (w >> 1) & ~w & 0x55555555u; }
+__device__ __forceinline__ void count64(uint4 v, uint32_t& cf, uint32_t& cs) {
+  cf += __popc(push_first_bits(v.x)) + __popc(push_first_bits(v.y)) + __popc(push_first_bits(v.z)) +
+        __popc(push_first_bits(v.w));
+  cs += __popc(push_shift_bits(v.x)) + __popc(push_shift_bits(v.y)) + __popc(push_shift_bits(v.z)) +
+        __popc(push_shift_bits(v.w));
 }
 
 __device__ __forceinline__ void compact_count_body(const DiffArgs& a, uint32_t bid, uint32_t nb) {
   __shared__ uint32_t sh[COMPACT_THREADS / 32 + 1];
-  const uint64_t groups = ((uint64_t)a.N + 15u) / 16u;
+  const uint64_t groups = ((uint64_t)a.N + PUSH_GROUP - 1u) / PUSH_GROUP;
   uint64_t beg, end;
   cta_range(groups, bid, nb, beg, end);
   uint32_t cf = 0, cs = 0;
-  for (uint64_t g = beg + threadIdx.x; g < end; g += blockDim.x) {
-    const uint4 v = ld_push16(a.push, g);
-    if (v.x | v.y | v.z | v.w) count16(v, cf, cs);
+  // two independent loads per thread per iteration
+  for (uint64_t g = beg + threadIdx.x; g < end; g += 2ull * blockDim.x) {
+    const uint4 v0 = ld_push16(a.push, g);
+    const uint4 v1 = g + blockDim.x < end ? ld_push16(a.push, g + blockDim.x) : make_uint4(0, 0, 0, 0);
+    if (v0.x | v0.y | v0.z | v0.w) count64(v0, cf, cs);
+    if (v1.x | v1.y | v1.z | v1.w) count64(v1, cf, cs);
   }
   const uint32_t tf = block_reduce_sum(cf, sh);
   const uint32_t ts = block_reduce_sum(cs, sh);
@@ -79,6 +82,7 @@ __device__ __forceinline__ void compact_count_body(const DiffArgs& a, uint32_t b
   }
 }
 __global__ void __launch_bounds__(COMPACT_THREADS) compact_count_kernel(DiffArgs a0) {
+  griddep_enter();
   compact_count_body(with_round(a0), blockIdx.x, gridDim.x);
 }
 __global__ void __launch_bounds__(COMPACT_THREADS) compact_count_seg(SegGrid s) {
@@ -103,8 +107,11 @@ __device__ __forceinline__ void compact_scan_body(const DiffArgs& a, uint32_t bi
     a.meta->S = ts;
   }
 }
-__global__ void __launch_bounds__(1024) compact_scan_kernel(DiffArgs a0, uint32_t g) {
+__global__ void __launch_bounds__(1024) compact_scan_kernel(DiffArgs a0, uint32_t g, uint32_t bcap) {
+  griddep_enter();
   compact_scan_body(with_round(a0), blockIdx.x, gridDim.x, g);
+  // the per-checkpoint bucket counts start at zero
+  for (uint32_t t = threadIdx.x; t < bcap; t += blockDim.x) a0.hist[t] = 0u;
 }
 __global__ void __launch_bounds__(1024) compact_scan_seg(SegGrid s) {
   uint32_t bid, nb;
@@ -114,59 +121,40 @@ __global__ void __launch_bounds__(1024) compact_scan_seg(SegGrid s) {
   for (uint32_t t = threadIdx.x; t < s.bcap[h]; t += blockDim.x) s.args[h].hist[t] = 0u;
 }
 
-// node-order lists of first / shift roots; clears the flags it consumed.  Each thread owns
-// COMPACT_GROUPS consecutive 16-node groups of a tile, so one block scan covers
-// COMPACT_THREADS * COMPACT_GROUPS * 16 nodes and the loads of a thread are independent.
-constexpr uint32_t COMPACT_GROUPS = 4;   // tile of 32768 nodes keeps both packed 16-bit counts exact
+// node-order lists of first / shift roots; clears the flags it consumed.  Each thread owns one
+// 64-node group of a tile, so one block scan covers COMPACT_THREADS * 64 = 32768 nodes, which
+// keeps both 16-bit halves of the packed counts exact.
 __device__ __forceinline__ void compact_write_body(const DiffArgs& a, uint32_t bid, uint32_t nb) {
   __shared__ uint32_t sh[COMPACT_THREADS / 32 + 1];
-  const uint64_t groups = ((uint64_t)a.N + 15u) / 16u;
+  const uint64_t groups = ((uint64_t)a.N + PUSH_GROUP - 1u) / PUSH_GROUP;
   uint64_t beg, end;
   cta_range(groups, bid, nb, beg, end);
   uint32_t bf = a.partial2[2 * bid], bs = a.partial2[2 * bid + 1];
-  constexpr uint32_t TILE = COMPACT_THREADS * COMPACT_GROUPS;
-  for (uint64_t t0 = beg; t0 < end; t0 += TILE) {
-    const uint64_t g0 = t0 + (uint64_t)threadIdx.x * COMPACT_GROUPS;
-    uint4 v[COMPACT_GROUPS];
-    uint32_t cf = 0, cs = 0, nzmask = 0;
-#pragma unroll
-    for (uint32_t j = 0; j < COMPACT_GROUPS; j++) {
-      v[j] = make_uint4(0, 0, 0, 0);
-      if (g0 + j < end) v[j] = ld_push16(a.push, g0 + j);
-    }
-#pragma unroll
-    for (uint32_t j = 0; j < COMPACT_GROUPS; j++) {
-      if (v[j].x | v[j].y | v[j].z | v[j].w) {
-        nzmask |= 1u << j;
-        count16(v[j], cf, cs);
-      }
-    }
+  for (uint64_t t0 = beg; t0 < end; t0 += COMPACT_THREADS) {
+    const uint64_t g = t0 + threadIdx.x;
+    const uint4 v = g < end ? ld_push16(a.push, g) : make_uint4(0, 0, 0, 0);
+    const bool nz = (v.x | v.y | v.z | v.w) != 0u;
+    uint32_t cf = 0, cs = 0;
+    if (nz) count64(v, cf, cs);
     uint32_t tot;
     const uint32_t ex = block_excl_scan((cf << 16) | cs, sh, &tot);
-    if (nzmask) {
+    if (nz) {
       uint32_t of = bf + (ex >> 16), os = bs + (ex & 0xffffu);
+      const uint32_t w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-      for (uint32_t j = 0; j < COMPACT_GROUPS; j++) {
-        if (!((nzmask >> j) & 1u)) continue;
-        const uint32_t w[4] = {v[j].x, v[j].y, v[j].z, v[j].w};
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-#pragma unroll
-          for (int b = 0; b < 4; b++) {
-            const uint32_t f = (w[k] >> (8 * b)) & 0xffu;
-            const uint32_t node = (uint32_t)(16ull * (g0 + j)) + 4u * k + b;
-            if (f == PUSH_FIRST) a.tmp_first[of++] = node;
-            else if (f == PUSH_SHIFT) a.tmp_shift[os++] = node;
-          }
-        }
-        reinterpret_cast<uint4*>(a.push)[g0 + j] = make_uint4(0, 0, 0, 0);
+      for (int k = 0; k < 4; k++) {
+        const uint32_t base = (uint32_t)(PUSH_GROUP * g) + 16u * k;
+        for (uint32_t m = push_first_bits(w[k]); m; m &= m - 1u) a.tmp_first[of++] = base + ((__ffs(m) - 1u) >> 1);
+        for (uint32_t m = push_shift_bits(w[k]); m; m &= m - 1u) a.tmp_shift[os++] = base + ((__ffs(m) - 1u) >> 1);
       }
+      reinterpret_cast<uint4*>(a.push)[g] = make_uint4(0, 0, 0, 0);
     }
     bf += tot >> 16;
     bs += tot & 0xffffu;
   }
 }
 __global__ void __launch_bounds__(COMPACT_THREADS) compact_write_kernel(DiffArgs a0) {
+  griddep_enter();
   compact_write_body(with_round(a0), blockIdx.x, gridDim.x);
 }
 __global__ void __launch_bounds__(COMPACT_THREADS) compact_write_seg(SegGrid s) {
@@ -209,6 +197,7 @@ __device__ __forceinline__ void compact_levels_body(const DiffArgs& a, uint32_t 
   }
 }
 __global__ void compact_levels_kernel(DiffArgs a0) {
+  griddep_enter();
   compact_levels_body(with_round(a0), blockIdx.x, gridDim.x);
 }
 __global__ void compact_levels_seg(SegGrid s) {
@@ -235,6 +224,7 @@ __device__ __forceinline__ void compact_permute_body(const DiffArgs& a, uint32_t
   }
 }
 __global__ void compact_permute_kernel(DiffArgs a0) {
+  griddep_enter();
   compact_permute_body(with_round(a0), blockIdx.x, gridDim.x);
 }
 __global__ void compact_permute_seg(SegGrid s) {
@@ -262,6 +252,7 @@ __device__ __forceinline__ void region_count_body(const DiffArgs& a, uint32_t bi
   if (threadIdx.x == 0) a.partial2[bid] = t;
 }
 __global__ void __launch_bounds__(COMPACT_THREADS) region_count_kernel(DiffArgs a0) {
+  griddep_enter();
   region_count_body(with_round(a0), blockIdx.x, gridDim.x);
 }
 __global__ void __launch_bounds__(COMPACT_THREADS) region_count_seg(SegGrid s) {
@@ -280,6 +271,7 @@ __device__ __forceinline__ void region_scan_body(const DiffArgs& a, uint32_t bid
   if (i == 0) a.meta->T = tot;
 }
 __global__ void __launch_bounds__(1024) region_scan_kernel(DiffArgs a0, uint32_t g) {
+  griddep_enter();
   region_scan_body(with_round(a0), blockIdx.x, gridDim.x, g);
 }
 __global__ void __launch_bounds__(1024) region_scan_seg(SegGrid s) {
@@ -303,6 +295,7 @@ __device__ __forceinline__ void region_write_body(const DiffArgs& a, uint32_t bi
   }
 }
 __global__ void __launch_bounds__(COMPACT_THREADS) region_write_kernel(DiffArgs a0) {
+  griddep_enter();
   region_write_body(with_round(a0), blockIdx.x, gridDim.x);
 }
 __global__ void __launch_bounds__(COMPACT_THREADS) region_write_seg(SegGrid s) {
@@ -346,6 +339,7 @@ __device__ __forceinline__ void shift_prev_body(const DiffArgs& a, uint32_t bid,
   }
 }
 __global__ void __launch_bounds__(128) shift_prev_kernel(DiffArgs a0, uint32_t bcap) {
+  griddep_enter();
   shift_prev_body(with_round(a0), blockIdx.x, gridDim.x, bcap);
 }
 __global__ void __launch_bounds__(128) shift_prev_seg(SegGrid s) {
@@ -440,6 +434,7 @@ __device__ __forceinline__ void layout_body(const DiffArgs& a, uint32_t bid, uin
   }
 }
 __global__ void __launch_bounds__(1024) layout_kernel(DiffArgs a0, uint32_t bcap, uint32_t g) {
+  griddep_enter();
   layout_body(with_round(a0), blockIdx.x, gridDim.x, bcap, g);
 }
 __global__ void __launch_bounds__(1024) layout_seg(SegGrid s) {
@@ -459,25 +454,39 @@ __device__ __forceinline__ void shift_write_body(const DiffArgs& a, uint32_t bid
   __syncwarp();
   const uint64_t shift_off = a.meta->shift_off;
   const uint32_t lane = threadIdx.x;
-  for (uint64_t t0 = beg; t0 < end; t0 += 32) {
-    const uint64_t i = t0 + lane;
-    const bool act = i < end;
-    const uint32_t key = act ? a.skey[i] : 0xffffffffu;
-    const uint32_t peers = __match_any_sync(0xffffffffu, key);
-    const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
-    uint32_t pos = 0;
-    if (act) pos = run[key] + rank;
-    __syncwarp();
-    if (act && rank == 0) run[key] += __popc(peers);
-    __syncwarp();
-    if (act) {
-      uint32_t* e = reinterpret_cast<uint32_t*>(a.diff + shift_off + 8ull * pos);
-      e[0] = a.shift_list[i] - a.id_bias;
-      e[1] = a.sprev[i] - a.id_bias;
+  // UNR groups of 32 entries per pass: their loads are issued together (they do
+  // not depend on the running bucket positions), then the groups are placed in order
+  constexpr uint32_t UNR = 4;
+  for (uint64_t t0 = beg; t0 < end; t0 += 32ull * UNR) {
+    uint32_t key[UNR], node[UNR], prev[UNR];
+#pragma unroll
+    for (uint32_t u = 0; u < UNR; u++) {
+      const uint64_t i = t0 + 32ull * u + lane;
+      const bool act = i < end;
+      key[u] = act ? a.skey[i] : 0xffffffffu;
+      node[u] = act ? a.shift_list[i] : 0u;
+      prev[u] = act ? a.sprev[i] : 0u;
+    }
+#pragma unroll
+    for (uint32_t u = 0; u < UNR; u++) {
+      const bool act = t0 + 32ull * u + lane < end;
+      const uint32_t peers = __match_any_sync(0xffffffffu, key[u]);
+      const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+      uint32_t pos = 0;
+      if (act) pos = run[key[u]] + rank;
+      __syncwarp();
+      if (act && rank == 0) run[key[u]] += __popc(peers);
+      __syncwarp();
+      if (act) {
+        uint32_t* e = reinterpret_cast<uint32_t*>(a.diff + shift_off + 8ull * pos);
+        e[0] = node[u] - a.id_bias;
+        e[1] = prev[u] - a.id_bias;
+      }
     }
   }
 }
 __global__ void __launch_bounds__(32) shift_write_kernel(DiffArgs a0, uint32_t bcap) {
+  griddep_enter();
   shift_write_body(with_round(a0), blockIdx.x, gridDim.x, bcap);
 }
 __global__ void __launch_bounds__(32) shift_write_seg(SegGrid s) {
@@ -586,6 +595,7 @@ __device__ __forceinline__ void gather_vec_body(const DiffArgs& a, uint32_t bid,
 }
 template <uint32_t LPC>
 __global__ void __launch_bounds__(256) gather_vec_kernel(DiffArgs a0) {
+  griddep_enter();
   gather_vec_body<LPC>(with_round(a0), blockIdx.x, gridDim.x);
 }
 template <uint32_t LPC>
@@ -619,6 +629,7 @@ __device__ __forceinline__ void gather_bytes_body(const DiffArgs& a, uint32_t bi
   }
 }
 __global__ void __launch_bounds__(256) gather_bytes_kernel(DiffArgs a0) {
+  griddep_enter();
   gather_bytes_body(with_round(a0), blockIdx.x, gridDim.x);
 }
 __global__ void __launch_bounds__(256) gather_bytes_seg(SegGrid s) {
@@ -636,7 +647,7 @@ static uint32_t grid_for(uint64_t units, uint64_t per_cta, uint32_t cap) {
 // for hundreds of idle CTAs per launch; large buffers get the full grids
 DiffGrids diff_grids(const DiffArgs& a, int sm_count) {
   DiffGrids r;
-  r.g = grid_for(((uint64_t)a.N + 15u) / 16u, 512, COMPACT_GRID);   // ~1 16-node load per thread
+  r.g = grid_for(((uint64_t)a.N + 63u) / 64u, 512, COMPACT_GRID);   // ~1 64-node load per thread
   // shift-entry ranges: the layout kernel scans every range's count per bucket in one CTA, so
   // fewer, longer ranges (<= 296) keep it short; the scatter walks each range with one warp
   r.gs = grid_for(a.n, 8192, SHIFT_GRID);
@@ -691,40 +702,44 @@ cudaError_t launch_collect_diff(const DiffArgs& args, uint32_t bcap, int sm_coun
   const uint32_t g = dg.g, gs = dg.gs;
   const uint32_t B = bcap;   // capacity; each kernel reads the checkpoint's bucket count from rs
   if (B > MAX_BUCKETS) return cudaErrorInvalidValue;
-  compact_count_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);
-  compact_scan_kernel<<<1, 1024, 0, stream>>>(a, g);
-  compact_write_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);
+  // one kernel after another, each launched to overlap its start with its predecessor's end
+  // (launch_dependent); the scan kernel also clears the per-checkpoint bucket counts
+  cudaError_t e;
+#define B2D_LD(...)                                              \
+  if ((e = launch_dependent(__VA_ARGS__)) != cudaSuccess) return e;
+  B2D_LD(compact_count_kernel, g, COMPACT_THREADS, 0, stream, a)
+  B2D_LD(compact_scan_kernel, 1, 1024, 0, stream, a, g, B)
+  B2D_LD(compact_write_kernel, g, COMPACT_THREADS, 0, stream, a)
   if (node_order) {
     a.first_list = a.tmp_first;
     a.shift_list = a.tmp_shift;
   } else {
-    compact_levels_kernel<<<dg.gl, 256, 0, stream>>>(a);
-    compact_permute_kernel<<<dg.gp, 256, 0, stream>>>(a);
+    B2D_LD(compact_levels_kernel, dg.gl, 256, 0, stream, a)
+    B2D_LD(compact_permute_kernel, dg.gp, 256, 0, stream, a)
   }
-  region_count_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);
-  region_scan_kernel<<<1, 1024, 0, stream>>>(a, g);
-  region_write_kernel<<<g, COMPACT_THREADS, 0, stream>>>(a);
-  cudaError_t e = cudaMemsetAsync(a.hist, 0, sizeof(uint32_t) * B, stream);
-  if (e != cudaSuccess) return e;
+  B2D_LD(region_count_kernel, g, COMPACT_THREADS, 0, stream, a)
+  B2D_LD(region_scan_kernel, 1, 1024, 0, stream, a, g)
+  B2D_LD(region_write_kernel, g, COMPACT_THREADS, 0, stream, a)
   const size_t hsm = sizeof(uint32_t) * B;   // <= 32 KB for MAX_BUCKETS
-  shift_prev_kernel<<<gs, 128, hsm, stream>>>(a, B);
-  layout_kernel<<<1, 1024, 0, stream>>>(a, B, gs);
-  shift_write_kernel<<<gs, 32, hsm, stream>>>(a, B);
+  B2D_LD(shift_prev_kernel, gs, 128, hsm, stream, a, B)
+  B2D_LD(layout_kernel, 1, 1024, 0, stream, a, B, gs)
+  B2D_LD(shift_write_kernel, gs, 32, hsm, stream, a, B)
   const uint32_t gblocks = dg.gg;
   const bool vec = (a.cs % 16u == 0) && ((reinterpret_cast<uintptr_t>(a.data) & 15u) == 0) &&
                    ((reinterpret_cast<uintptr_t>(a.diff) & 15u) == 0);
   if (vec) {
     const uint32_t units = a.cs / 16u;
-    if (units >= 32) gather_vec_kernel<32><<<gblocks, 256, 0, stream>>>(a);
-    else if (units >= 16) gather_vec_kernel<16><<<gblocks, 256, 0, stream>>>(a);
-    else if (units >= 8) gather_vec_kernel<8><<<gblocks, 256, 0, stream>>>(a);
-    else if (units >= 4) gather_vec_kernel<4><<<gblocks, 256, 0, stream>>>(a);
-    else if (units >= 2) gather_vec_kernel<2><<<gblocks, 256, 0, stream>>>(a);
-    else gather_vec_kernel<1><<<gblocks, 256, 0, stream>>>(a);
+    if (units >= 32) { B2D_LD(gather_vec_kernel<32>, gblocks, 256, 0, stream, a) }
+    else if (units >= 16) { B2D_LD(gather_vec_kernel<16>, gblocks, 256, 0, stream, a) }
+    else if (units >= 8) { B2D_LD(gather_vec_kernel<8>, gblocks, 256, 0, stream, a) }
+    else if (units >= 4) { B2D_LD(gather_vec_kernel<4>, gblocks, 256, 0, stream, a) }
+    else if (units >= 2) { B2D_LD(gather_vec_kernel<2>, gblocks, 256, 0, stream, a) }
+    else { B2D_LD(gather_vec_kernel<1>, gblocks, 256, 0, stream, a) }
   } else {
-    gather_bytes_kernel<<<gblocks, 256, 0, stream>>>(a);
+    B2D_LD(gather_bytes_kernel, gblocks, 256, 0, stream, a)
   }
-  return cudaGetLastError();
+#undef B2D_LD
+  return cudaSuccess;
 }
 
 }  // namespace b2d

@@ -64,6 +64,7 @@ __device__ __forceinline__ Digest prior_digest(const LeafArgs& a, uint64_t chunk
 }
 
 __global__ void leaf_generic_kernel(LeafArgs a0, uint32_t c_begin, uint32_t c_end) {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const LeafArgs a = with_round(a0);
   for (uint64_t c = (uint64_t)c_begin + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < c_end;
        c += (uint64_t)gridDim.x * blockDim.x) {
@@ -218,6 +219,7 @@ template <int U, int KIND>
 __global__ void __launch_bounds__((TMA_CONSUMER_WARPS + 1) * 32)
     leaf_tma_kernel(const __grid_constant__ CUtensorMap tmap, LeafArgs a0, uint32_t nfull, uint32_t S,
                     uint32_t stages) {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const LeafArgs a = with_round(a0);
   constexpr uint32_t R = 32u * TMA_CONSUMER_WARPS;
   constexpr uint32_t STAGE_BYTES = R * U;

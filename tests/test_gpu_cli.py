@@ -118,9 +118,10 @@ def test_log_writers(cuda, tmp_path):
         assert len(ra) == len(rb) and [r.split(",")[:fields] for r in ra] == [r.split(",")[:fields] for r in rb], ext
     out = torch.zeros(len(bufs[0]), dtype=torch.uint8, device="cuda")
     ra_log, rb_log = str(tmp_path / "ra.csv"), str(tmp_path / "rb.csv")
-    a.restart(out, diffs, 1, logname=ra_log)
+    a.restart(out, diffs, 1, logname=ra_log)   # the host-view overload names its log after logname
     assert torch.equal(out, bufs[1])
-    a.write_restart_log(1, rb_log)
-    assert open(ra_log).read() == open(rb_log).read() and open(rb_log).read().startswith("Tree,1,128,")
+    a.write_restart_log(1, rb_log)              # the interface method writes to logname itself
+    ra = open(ra_log + ".chunk_size.128.restart_timing.csv").read()
+    assert ra == open(rb_log).read() and ra.startswith("Tree,1,128,")
     a.close()
     b.close()
