@@ -14,6 +14,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_HASH_PATH = os.path.join(HERE, "_ref", "libref_hash.so")
+REF_DEDUP_PATH = os.path.join(HERE, "_ref", "libref_dedup.so")
 
 HASH_MURMUR3 = 0
 HASH_MD5 = 1
@@ -267,3 +268,84 @@ def ref_hash_lib():
     for f in (L.ref_murmur3, L.ref_md5):
         f.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]
     return L
+
+
+_ref_dedup = None
+
+
+def ref_dedup_lib():
+    """The reference's own tree and list deduplicators compiled in place against the sequential
+    Kokkos stand-in (oracle/kokkos_shim), or None where the reference source was not present."""
+    global _ref_dedup
+    if _ref_dedup is None and os.path.exists(REF_DEDUP_PATH):
+        L = ctypes.CDLL(REF_DEDUP_PATH)
+        vp, u8pp, u64 = ctypes.c_void_p, ctypes.POINTER(ctypes.POINTER(ctypes.c_uint8)), ctypes.c_uint64
+        for a in ("tree", "list"):
+            getattr(L, f"ref_{a}_create").restype = vp
+            getattr(L, f"ref_{a}_create").argtypes = [ctypes.c_uint32]
+            getattr(L, f"ref_{a}_destroy").argtypes = [vp]
+            getattr(L, f"ref_{a}_checkpoint").restype = ctypes.c_int
+            getattr(L, f"ref_{a}_checkpoint").argtypes = [vp, vp, u64, ctypes.c_int, u8pp, ctypes.POINTER(u64)]
+            getattr(L, f"ref_{a}_restart").restype = ctypes.c_int
+            getattr(L, f"ref_{a}_restart").argtypes = [ctypes.c_uint32, ctypes.POINTER(vp), ctypes.POINTER(u64),
+                                                       ctypes.c_uint32, ctypes.c_uint32, vp, u64]
+        L.ref_tree_num_first_ocur.restype = u64
+        L.ref_tree_num_first_ocur.argtypes = [vp]
+        L.ref_tree_num_shift_dupl.restype = u64
+        L.ref_tree_num_shift_dupl.argtypes = [vp]
+        L.ref_free.argtypes = [vp]
+        _ref_dedup = L
+    return _ref_dedup
+
+
+class RefDeduplicator:
+    """The reference's own TreeDeduplicator / ListDeduplicator (approach "tree" / "list"),
+    compiled from its source (Murmur3, the hash it is built with); checkpoint() is the host-view
+    overload (src/tree_approach.cpp:1740-1748, src/list_approach.cpp)."""
+
+    def __init__(self, chunk_size, approach="tree"):
+        self.L = ref_dedup_lib()
+        if self.L is None:
+            raise RuntimeError("the compiled reference (oracle/_ref/libref_dedup.so) is not built")
+        self.approach = approach
+        self._h = getattr(self.L, f"ref_{approach}_create")(chunk_size)
+
+    def checkpoint(self, data, make_baseline=False):
+        a = np.ascontiguousarray(data, dtype=np.uint8).reshape(-1)
+        out = ctypes.POINTER(ctypes.c_uint8)()
+        n = ctypes.c_uint64(0)
+        rc = getattr(self.L, f"ref_{self.approach}_checkpoint")(self._h, _ptr(a), a.size, int(bool(make_baseline)),
+                                                                ctypes.byref(out), ctypes.byref(n))
+        if rc != 0:
+            raise RuntimeError("reference checkpoint failed")
+        diff = np.ctypeslib.as_array(out, shape=(n.value,)).tobytes() if n.value else b""
+        self.L.ref_free(out)
+        return diff
+
+    def close(self):
+        if self._h:
+            getattr(self.L, f"ref_{self.approach}_destroy")(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def ref_restart(diffs, chkpt_idx, approach="tree", out_len=None, init=None):
+    """The reference's own host-view restart of checkpoint `chkpt_idx` (src/tree_approach.cpp:
+    1786-1817; src/list_approach.cpp), into a buffer that starts as `init` (zeros by default)."""
+    L = ref_dedup_lib()
+    if L is None:
+        raise RuntimeError("the compiled reference (oracle/_ref/libref_dedup.so) is not built")
+    bufs = [_as_u8(d) for d in diffs]
+    hdr = np.frombuffer(bufs[chkpt_idx][:32].tobytes(), np.uint32)
+    if out_len is None:
+        out_len = int(hdr[2]) | (int(hdr[3]) << 32)
+    out = np.zeros(out_len, np.uint8) if init is None else np.array(init, dtype=np.uint8).copy()
+    ptrs = (ctypes.c_void_p * len(bufs))(*[b.ctypes.data for b in bufs])
+    sizes = (ctypes.c_uint64 * len(bufs))(*[b.size for b in bufs])
+    getattr(L, f"ref_{approach}_restart")(int(hdr[4]), ptrs, sizes, len(bufs), chkpt_idx, _ptr(out), out_len)
+    return out

@@ -347,6 +347,21 @@ class DeviceSeries:
         return self.data
 
 
+def duplicate_heavy(n_chunks, chunk_size, checkpoints, seed=SEED):
+    """Buffers with few distinct chunk values (equal chunks and equal subtrees at many depths,
+    all-zero pages): every chunk of checkpoint k holds one of four byte patterns, drawn per
+    chunk from numpy's PCG64 seeded by (seed, checkpoint)."""
+    bufs = []
+    for k in range(checkpoints):
+        rng = plan_rng(seed, 7, n_chunks, k)
+        pat = rng.integers(0, 4, n_chunks)
+        b = np.zeros((n_chunks, chunk_size), np.uint8)
+        for v in range(1, 4):
+            b[pat == v] = v + (k % 3)
+        bufs.append(b.reshape(-1))
+    return bufs
+
+
 # ----------------------------------------------------------------------------- float32 / MD5
 class FloatSeries:
     """Training-state-like float32 buffer (md5_f32_8g)."""

@@ -7,6 +7,12 @@
                   two 8-byte checkpoints with chunk size 1 and the expected (first, shift) region
                   counts, transcribed from those files; plus the oracle's diff bytes for each
   series.json     sha256 of every oracle diff of small seeded checkpoint series (regression pins)
+  ref_series.json sha256 of every diff the REFERENCE's own TreeDeduplicator and ListDeduplicator
+                  write (src/tree_approach.cpp, src/list_approach.cpp compiled unmodified against
+                  the sequential Kokkos stand-in into oracle/_ref/libref_dedup.so) for seeded
+                  series -- full-size config 1 included -- and of every buffer its restarts
+                  rebuild where the reference's restart is defined (power-of-two chunk counts
+                  for the tree; always for the list)
 
 Run from the repository root, where the reference source tree is available:
     make -C oracle && python tests/golden/make_golden.py
@@ -52,6 +58,50 @@ SERIES = [
 ]
 
 
+# (name, approach, generator, nbytes or chunk count, chunk, checkpoints, baselines): Murmur3, the
+# hash the reference is built with
+REF_SERIES = [
+    ("tree_plain_64m_cs128", "tree", "plain_64m", 64 << 20, 128, 5, [1, 0, 0, 0, 0]),
+    ("tree_plain_1m_cs64_rebase", "tree", "plain_64m", 1 << 20, 64, 6, [1, 0, 0, 1, 0, 0]),
+    ("tree_ragged_1m_cs128", "tree", "plain_64m", (1 << 20) + 77, 128, 5, [1, 0, 0, 0, 0]),
+    ("tree_plain_4m_cs4096", "tree", "plain_4g", 4 << 20, 4096, 4, [1, 0, 0, 0]),
+    ("tree_nonpow2_96k_cs100", "tree", "plain_64m", (96 << 10) + 13, 100, 5, [1, 0, 0, 0, 0]),
+    ("tree_chain13_512k_cs128", "tree", "plain_64m", (512 << 10) + 64, 128, 13, [1] + [0] * 12),
+    ("tree_dupheavy_3077x64", "tree", "dup_heavy", 3077, 64, 5, [1, 0, 0, 0, 0]),
+    ("tree_tiny_cs1", "tree", "plain_64m", 3000, 1, 4, [1, 0, 0, 0]),
+    ("list_plain_1m_cs128_rebase", "list", "plain_64m", 1 << 20, 128, 6, [1, 0, 0, 1, 0, 0]),
+    ("list_ragged_1m_cs64", "list", "plain_64m", (1 << 20) + 77, 64, 5, [1, 0, 0, 0, 0]),
+    ("list_dupheavy_3077x64", "list", "dup_heavy", 3077, 64, 5, [1, 0, 0, 0, 0]),
+]
+
+
+def ref_series_inputs(gen, size, cs, nck):
+    """the checkpoint buffers of one REF_SERIES entry"""
+    if gen == "dup_heavy":
+        return synth.duplicate_heavy(size, cs, nck)
+    plan = synth.plan_plain_64m if gen == "plain_64m" else synth.plan_plain_4g
+    s = synth.ByteSeries(size, cs, plan, 1, size % 1000)
+    return [s.next().copy() for _ in range(nck)]
+
+
+def ref_series_entry(approach, gen, size, cs, nck, baselines):
+    bufs = ref_series_inputs(gen, size, cs, nck)
+    r = O.RefDeduplicator(cs, approach)
+    diffs = [r.checkpoint(b, m) for b, m in zip(bufs, baselines)]
+    r.close()
+    n = (len(bufs[0]) + cs - 1) // cs
+    restarts = None
+    if approach == "list" or n & (n - 1) == 0:
+        restarts = []
+        for k in range(nck):
+            out = O.ref_restart(diffs, k, approach)
+            assert np.array_equal(out, bufs[k]), (approach, gen, size, k)
+            restarts.append(hashlib.sha256(out.tobytes()).hexdigest())
+    return {"approach": approach, "generator": gen, "size": size, "chunk_size": cs, "checkpoints": nck,
+            "baselines": baselines, "sha256": [hashlib.sha256(x).hexdigest() for x in diffs],
+            "sizes": [len(x) for x in diffs], "restart_sha256": restarts}
+
+
 def series_diffs(name, nbytes, cs, kind, nck, gen):
     s = synth.ByteSeries(nbytes, cs, synth.plan_plain_64m if gen == "plain_64m" else synth.plan_plain_4g, 1, 0)
     d = O.OracleTreeDeduplicator(cs, kind)
@@ -95,6 +145,13 @@ def main():
                         "sha256": [hashlib.sha256(x).hexdigest() for x in diffs], "sizes": [len(x) for x in diffs]}
     with open(os.path.join(HERE, "series.json"), "w") as f:
         json.dump(series, f, indent=1)
+    if O.ref_dedup_lib() is None:
+        raise SystemExit("oracle/_ref/libref_dedup.so missing: run `make -C oracle` where the reference exists")
+    ref = {"source": "reference src/tree_approach.cpp, src/list_approach.cpp (unmodified) on oracle/kokkos_shim"}
+    for name, approach, gen, size, cs, nck, bl in REF_SERIES:
+        ref[name] = ref_series_entry(approach, gen, size, cs, nck, bl)
+    with open(os.path.join(HERE, "ref_series.json"), "w") as f:
+        json.dump(ref, f, indent=1)
     print("wrote", os.listdir(HERE))
 
 

@@ -243,3 +243,35 @@ def test_checkpoint_id_limit(cuda):
         assert e.value.code == -11
     assert g.current_id == 8191 and g.copy_diff().tobytes() == last
     g.close()
+
+
+REF = load("ref_series.json")
+
+
+@pytest.mark.parametrize("name", sorted(k for k in REF if k != "source"))
+def test_reference_series_gpu(cuda, name):
+    """every diff equals, by sha256, the one the reference's own code writes for the same series
+    (src/tree_approach.cpp / src/list_approach.cpp compiled unmodified on a sequential Kokkos
+    stand-in, tests/golden/ref_series.json), and every restart rebuilds the same buffer"""
+    import torch
+
+    from reproducibility_icpp23_scalable_gpu_deduplication_b200 import ListDeduplicator
+
+    e = REF[name]
+    if e["generator"] == "dup_heavy":
+        bufs = synth.duplicate_heavy(e["size"], e["chunk_size"], e["checkpoints"])
+    else:
+        plan = synth.plan_plain_64m if e["generator"] == "plain_64m" else synth.plan_plain_4g
+        s = synth.ByteSeries(e["size"], e["chunk_size"], plan, 1, e["size"] % 1000)
+        bufs = [s.next().copy() for _ in range(e["checkpoints"])]
+    g = (ListDeduplicator if e["approach"] == "list" else TreeDeduplicator)(e["chunk_size"])
+    diffs = [g.checkpoint(to_dev(b), bool(m)) for b, m in zip(bufs, e["baselines"])]
+    assert [len(d) for d in diffs] == e["sizes"]
+    assert [hashlib.sha256(d).hexdigest() for d in diffs] == e["sha256"]
+    if e["restart_sha256"] is not None:
+        dev = [to_dev(np.frombuffer(d, np.uint8)) for d in diffs]
+        for k, want in enumerate(e["restart_sha256"]):
+            out = torch.zeros(len(bufs[k]), dtype=torch.uint8, device="cuda")
+            g.restart_device(out, dev, k)
+            assert hashlib.sha256(out.cpu().numpy().tobytes()).hexdigest() == want, k
+    g.close()
