@@ -93,18 +93,18 @@ struct PinnedBuf {
 __global__ void map_rehash_kernel(MapView from, MapView to, DevStatus* st) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i <= from.cap;
        i += (uint64_t)gridDim.x * blockDim.x) {
-    const unsigned long long v = from.vals[i];
+    const unsigned long long v = *map_val(from, i);
     if (i == from.cap) {   // the extra slot (the all-ones digest), present when its value is set
-      if (v != MAP_EMPTY) to.vals[to.cap] = v;
+      if (v != MAP_EMPTY) *map_val(to, to.cap) = v;
       continue;
     }
-    const Key128 k = from.keys[i];
+    const Key128 k = *map_key(from, i);
     if (k.lo == MAP_EMPTY && k.hi == MAP_EMPTY) continue;
     Digest d;
     d.w[0] = (uint32_t)k.lo; d.w[1] = (uint32_t)(k.lo >> 32);
     d.w[2] = (uint32_t)k.hi; d.w[3] = (uint32_t)(k.hi >> 32);
     const MapRef r = map_insert_packed(to, d, v, st);
-    if (r.found) to.vals[r.slot] = v;
+    if (r.found) *map_val(to, r.slot) = v;
   }
 }
 
@@ -131,8 +131,8 @@ using namespace b2d;
 
 // default size of a baseline's digest map over its minimum, and the factor a growing map
 // takes over its new minimum.  A baseline's minimum is its own N entries plus the next
-// checkpoint's N at the load limit: 2N / 0.75; times 1.5 that is 4N slots (24 B each, 96 B per
-// node: 1.5 bytes per byte of a 4 GiB buffer at 128-byte chunks), at load 0.25 after the
+// checkpoint's N at the load limit: 2N / 0.75; times 1.5 that is 4N slots (32 B each, 128 B per
+// node: 2 bytes per byte of a 4 GiB buffer at 128-byte chunks), at load 0.25 after the
 // baseline, and the table grows only once its entries pass 2N (after about a hundred
 // checkpoints that each change 1% of the chunks).
 constexpr double MAP_HEADROOM = 1.5;
@@ -398,7 +398,7 @@ LeafArgs leaf_args(const b2d_dedup* d, const RoundState* rs_dev) {
   const MapView m = map_at(d->map_mem, d->map_cap, d->map_size.p);
   return LeafArgs{static_cast<const uint8_t*>(d->data), d->data_len, d->chunk_size, d->n, d->kind, 0, 0,
                   d->tree.p, d->leaflab.p, d->dupflag.p, m, &d->state.p->status, rs_dev,
-                  (uint32_t)d->tune.wait_polls, 1u};
+                  (uint32_t)d->tune.wait_polls};
 }
 
 // ------------------------------------------------------------------------------------------

@@ -48,7 +48,6 @@ struct LeafArgs {
   const RoundState* rs;
   uint32_t wait_polls;   // 0: the barrier waits' normal bound; else give up after this many
                          // non-blocking polls (a test of the give-up path)
-  uint32_t one;          // 1, as a value the compiler cannot see (md5_compress_fma)
 };
 
 struct ForestArgs {

@@ -492,18 +492,43 @@ __global__ void __launch_bounds__(FAST_THREADS, B2D_FAST_MINB) forest_fast_seg(F
 // A task writes its root's label to `lab` for the band above (which is a CTA band again: few
 // nodes are left there).  Same per-node rules as the CTA bands, so the labels, digests, map
 // entries and push flags are the same.
+// bit 0: phase 1 starts with a warp band, bit 1: phase 2 does
 #ifndef B2D_WARP_BANDS
-#define B2D_WARP_BANDS 1
+#define B2D_WARP_BANDS 3
 #endif
 constexpr uint32_t WB1_LEVELS = 7;
 constexpr uint32_t WB2_LEVELS = 9;
 constexpr uint32_t WB_THREADS = 256;
 
 static bool warp_bands(uint32_t n, uint32_t D, int phase) {
-  return B2D_WARP_BANDS && n >= 2u && (n & (n - 1u)) == 0 && D >= (phase == 1 ? WB1_LEVELS : WB2_LEVELS);
+  return (B2D_WARP_BANDS & (phase == 1 ? 1 : 2)) && n >= 2u && (n & (n - 1u)) == 0 &&
+         D >= (phase == 1 ? WB1_LEVELS : WB2_LEVELS);
 }
 
-__device__ __forceinline__ void warp1_task(const ForestArgs& a, uint32_t task, uint32_t lane, uint32_t w) {
+// Parents a phase-1 warp task created, inserted into the map together once the task's hashing is
+// done (spread over the lanes): inserting each where it is hashed put a chain of dependent map
+// round trips on the lanes that carry the upper levels.  At most 127 per task of 128 leaves.
+struct WarpInserts {
+  uint32_t* node;   // 128 entries of this warp's buffer in shared memory
+  Digest* dig;
+  uint32_t* count;
+};
+__device__ __forceinline__ void wi_add(const WarpInserts& wi, uint32_t x, const Digest& d) {
+  const uint32_t pos = atomicAdd(wi.count, 1u);
+  wi.node[pos] = x;
+  wi.dig[pos] = d;
+}
+__device__ __forceinline__ void wi_flush(const ForestArgs& a, const WarpInserts& wi, uint32_t lane) {
+  __syncwarp();
+  const uint32_t cnt = *wi.count;
+  for (uint32_t r = lane; r < cnt; r += 32u) insert_first_parent(a, wi.node[r], wi.dig[r]);
+  __syncwarp();
+  if (lane == 0) *wi.count = 0;
+  __syncwarp();
+}
+
+__device__ __forceinline__ void warp1_task(const ForestArgs& a, uint32_t task, uint32_t lane, uint32_t w,
+                                           const WarpInserts& wi) {
   const uint64_t root = ((1ull << (a.D - WB1_LEVELS)) - 1ull) + task;
   const uint32_t c0 = task * 128u + 4u * lane;          // first chunk of this lane
   const uint64_t x0 = (uint64_t)(a.n - 1u) + c0;        // its leaf (a left child)
@@ -530,7 +555,7 @@ __device__ __forceinline__ void warp1_task(const ForestArgs& a, uint32_t task, u
     if (((m0 >> (2 * j)) & 3u) == 3u) {
       d1[j] = hash_pair(a.kind, a.tree[x0 + 2 * j], a.tree[x0 + 2 * j + 1]);
       a.tree[p0 + j] = d1[j];
-      insert_first_parent(a, (uint32_t)(p0 + j), d1[j]);
+      wi_add(wi, (uint32_t)(p0 + j), d1[j]);
       m1 |= 1u << j;
     }
   }
@@ -541,7 +566,7 @@ __device__ __forceinline__ void warp1_task(const ForestArgs& a, uint32_t task, u
   if (m1 == 3u) {
     dg = hash_pair(a.kind, d1[0], d1[1]);
     a.tree[y] = dg;
-    insert_first_parent(a, (uint32_t)y, dg);
+    wi_add(wi, (uint32_t)y, dg);
     b = 1;
   }
   // heights 3..7: shuffles; lane 0 ends at the task root
@@ -556,7 +581,7 @@ __device__ __forceinline__ void warp1_task(const ForestArgs& a, uint32_t task, u
         if (b) {
           dg = hash_pair(a.kind, dg, rd);
           a.tree[y] = dg;
-          insert_first_parent(a, (uint32_t)y, dg);
+          wi_add(wi, (uint32_t)y, dg);
         }
       }
     }
@@ -564,6 +589,7 @@ __device__ __forceinline__ void warp1_task(const ForestArgs& a, uint32_t task, u
     b = 0;
   }
   if (lane == 0) band_output<1>(a, root, b ? FIRST_OCUR : DONE);
+  wi_flush(a, wi, lane);
 }
 
 __device__ __forceinline__ void warp2_task(const ForestArgs& a, uint32_t task, uint32_t lane, const uint4& w) {
@@ -605,8 +631,16 @@ __device__ __forceinline__ void warp2_task(const ForestArgs& a, uint32_t task, u
 }
 
 // Resident grid of warps; warp g takes tasks g, g + G, ... and loads the next one's labels first.
+#define B2D_WARP_INSERT_BUFFERS                                                                 \
+  __shared__ uint32_t wi_node_[WB_THREADS / 32u][128];                                          \
+  __shared__ Digest wi_dig_[WB_THREADS / 32u][128];                                             \
+  __shared__ uint32_t wi_count_[WB_THREADS / 32u];                                              \
+  const WarpInserts wi{wi_node_[threadIdx.x >> 5], wi_dig_[threadIdx.x >> 5], &wi_count_[threadIdx.x >> 5]}; \
+  if ((threadIdx.x & 31u) == 0) *wi.count = 0;                                                  \
+  __syncwarp();
 __global__ void __launch_bounds__(WB_THREADS) forest_warp1_kernel(ForestArgs a0, uint32_t ntasks) {
   griddep_enter();
+  B2D_WARP_INSERT_BUFFERS
   const ForestArgs a = with_round(a0);
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t G = (gridDim.x * WB_THREADS) >> 5;
@@ -616,7 +650,7 @@ __global__ void __launch_bounds__(WB_THREADS) forest_warp1_kernel(ForestArgs a0,
   for (; task < ntasks; task += G) {
     const uint32_t next = task + G;
     const uint32_t wn = next < ntasks ? lab32[next * 32u + lane] : 0u;
-    warp1_task(a, task, lane, w);
+    warp1_task(a, task, lane, w, wi);
     w = wn;
   }
 }
@@ -639,13 +673,14 @@ __global__ void __launch_bounds__(WB_THREADS) forest_warp2_kernel(ForestArgs a0,
 // Segmented warp bands (batched form): CTA b of a handle's range holds its tasks 8b .. 8b+7,
 // one per warp.
 __global__ void __launch_bounds__(WB_THREADS) forest_warp1_seg(ForestSeg s) {
+  B2D_WARP_INSERT_BUFFERS
   uint32_t bid, nb;
   const uint32_t h = seg_find(s.beg, s.n, bid, nb);
   const ForestArgs a = with_round(s.args[h]);
   const uint32_t task = bid * (WB_THREADS / 32u) + (threadIdx.x >> 5);
   if (task >= (a.n >> WB1_LEVELS)) return;
   const uint32_t lane = threadIdx.x & 31u;
-  warp1_task(a, task, lane, reinterpret_cast<const uint32_t*>(a.leaflab)[task * 32u + lane]);
+  warp1_task(a, task, lane, reinterpret_cast<const uint32_t*>(a.leaflab)[task * 32u + lane], wi);
 }
 __global__ void __launch_bounds__(WB_THREADS) forest_warp2_seg(ForestSeg s) {
   uint32_t bid, nb;

@@ -139,90 +139,6 @@ __host__ __device__ __forceinline__ void md5_compress(uint32_t st[4], const uint
   st[0] += a; st[1] += b; st[2] += c; st[3] += d;
 }
 
-#ifdef __CUDACC__
-// MD5 rounds for the staged hashing kernels, which are integer-pipe bound on MD5: the same
-// steps with two of each step's additions (a + x, and + b after the rotate) written as
-// multiply-adds by `one`, a runtime 1 the compiler cannot fold.  They then issue as IMAD on the
-// FMA pipe, which the integer ALU's adds, funnel shifts and logic ops otherwise leave idle.
-__device__ __forceinline__ uint32_t md5_madd(uint32_t x, uint32_t one, uint32_t y) {
-  uint32_t r;
-  asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(x), "r"(one), "r"(y));
-  return r;
-}
-#define B2D_MD5_STEP_FMA(f, a, b, c, d, x, t, s) \
-  a = md5_madd((x), one, a) + f(b, c, d) + (t);  \
-  a = ((a << (s)) | (a >> (32 - (s))));          \
-  a = md5_madd(a, one, b);
-
-__device__ __forceinline__ void md5_compress_fma(uint32_t st[4], const uint32_t m[16], uint32_t one) {
-  uint32_t a = st[0], b = st[1], c = st[2], d = st[3];
-  B2D_MD5_STEP_FMA(B2D_MD5_F, a, b, c, d, m[0], 0xd76aa478u, 7)
-  B2D_MD5_STEP_FMA(B2D_MD5_F, d, a, b, c, m[1], 0xe8c7b756u, 12)
-  B2D_MD5_STEP_FMA(B2D_MD5_F, c, d, a, b, m[2], 0x242070dbu, 17)
-  B2D_MD5_STEP_FMA(B2D_MD5_F, b, c, d, a, m[3], 0xc1bdceeeu, 22)
-  B2D_MD5_STEP_FMA(B2D_MD5_F, a, b, c, d, m[4], 0xf57c0fafu, 7)
-  B2D_MD5_STEP_FMA(B2D_MD5_F, d, a, b, c, m[5], 0x4787c62au, 12)
-  B2D_MD5_STEP_FMA(B2D_MD5_F, c, d, a, b, m[6], 0xa8304613u, 17)
-  B2D_MD5_STEP_FMA(B2D_MD5_F, b, c, d, a, m[7], 0xfd469501u, 22)
-  B2D_MD5_STEP_FMA(B2D_MD5_F, a, b, c, d, m[8], 0x698098d8u, 7)
-  B2D_MD5_STEP_FMA(B2D_MD5_F, d, a, b, c, m[9], 0x8b44f7afu, 12)
-  B2D_MD5_STEP_FMA(B2D_MD5_F, c, d, a, b, m[10], 0xffff5bb1u, 17)
-  B2D_MD5_STEP_FMA(B2D_MD5_F, b, c, d, a, m[11], 0x895cd7beu, 22)
-  B2D_MD5_STEP_FMA(B2D_MD5_F, a, b, c, d, m[12], 0x6b901122u, 7)
-  B2D_MD5_STEP_FMA(B2D_MD5_F, d, a, b, c, m[13], 0xfd987193u, 12)
-  B2D_MD5_STEP_FMA(B2D_MD5_F, c, d, a, b, m[14], 0xa679438eu, 17)
-  B2D_MD5_STEP_FMA(B2D_MD5_F, b, c, d, a, m[15], 0x49b40821u, 22)
-  B2D_MD5_STEP_FMA(B2D_MD5_G, a, b, c, d, m[1], 0xf61e2562u, 5)
-  B2D_MD5_STEP_FMA(B2D_MD5_G, d, a, b, c, m[6], 0xc040b340u, 9)
-  B2D_MD5_STEP_FMA(B2D_MD5_G, c, d, a, b, m[11], 0x265e5a51u, 14)
-  B2D_MD5_STEP_FMA(B2D_MD5_G, b, c, d, a, m[0], 0xe9b6c7aau, 20)
-  B2D_MD5_STEP_FMA(B2D_MD5_G, a, b, c, d, m[5], 0xd62f105du, 5)
-  B2D_MD5_STEP_FMA(B2D_MD5_G, d, a, b, c, m[10], 0x02441453u, 9)
-  B2D_MD5_STEP_FMA(B2D_MD5_G, c, d, a, b, m[15], 0xd8a1e681u, 14)
-  B2D_MD5_STEP_FMA(B2D_MD5_G, b, c, d, a, m[4], 0xe7d3fbc8u, 20)
-  B2D_MD5_STEP_FMA(B2D_MD5_G, a, b, c, d, m[9], 0x21e1cde6u, 5)
-  B2D_MD5_STEP_FMA(B2D_MD5_G, d, a, b, c, m[14], 0xc33707d6u, 9)
-  B2D_MD5_STEP_FMA(B2D_MD5_G, c, d, a, b, m[3], 0xf4d50d87u, 14)
-  B2D_MD5_STEP_FMA(B2D_MD5_G, b, c, d, a, m[8], 0x455a14edu, 20)
-  B2D_MD5_STEP_FMA(B2D_MD5_G, a, b, c, d, m[13], 0xa9e3e905u, 5)
-  B2D_MD5_STEP_FMA(B2D_MD5_G, d, a, b, c, m[2], 0xfcefa3f8u, 9)
-  B2D_MD5_STEP_FMA(B2D_MD5_G, c, d, a, b, m[7], 0x676f02d9u, 14)
-  B2D_MD5_STEP_FMA(B2D_MD5_G, b, c, d, a, m[12], 0x8d2a4c8au, 20)
-  B2D_MD5_STEP_FMA(B2D_MD5_H, a, b, c, d, m[5], 0xfffa3942u, 4)
-  B2D_MD5_STEP_FMA(B2D_MD5_H, d, a, b, c, m[8], 0x8771f681u, 11)
-  B2D_MD5_STEP_FMA(B2D_MD5_H, c, d, a, b, m[11], 0x6d9d6122u, 16)
-  B2D_MD5_STEP_FMA(B2D_MD5_H, b, c, d, a, m[14], 0xfde5380cu, 23)
-  B2D_MD5_STEP_FMA(B2D_MD5_H, a, b, c, d, m[1], 0xa4beea44u, 4)
-  B2D_MD5_STEP_FMA(B2D_MD5_H, d, a, b, c, m[4], 0x4bdecfa9u, 11)
-  B2D_MD5_STEP_FMA(B2D_MD5_H, c, d, a, b, m[7], 0xf6bb4b60u, 16)
-  B2D_MD5_STEP_FMA(B2D_MD5_H, b, c, d, a, m[10], 0xbebfbc70u, 23)
-  B2D_MD5_STEP_FMA(B2D_MD5_H, a, b, c, d, m[13], 0x289b7ec6u, 4)
-  B2D_MD5_STEP_FMA(B2D_MD5_H, d, a, b, c, m[0], 0xeaa127fau, 11)
-  B2D_MD5_STEP_FMA(B2D_MD5_H, c, d, a, b, m[3], 0xd4ef3085u, 16)
-  B2D_MD5_STEP_FMA(B2D_MD5_H, b, c, d, a, m[6], 0x04881d05u, 23)
-  B2D_MD5_STEP_FMA(B2D_MD5_H, a, b, c, d, m[9], 0xd9d4d039u, 4)
-  B2D_MD5_STEP_FMA(B2D_MD5_H, d, a, b, c, m[12], 0xe6db99e5u, 11)
-  B2D_MD5_STEP_FMA(B2D_MD5_H, c, d, a, b, m[15], 0x1fa27cf8u, 16)
-  B2D_MD5_STEP_FMA(B2D_MD5_H, b, c, d, a, m[2], 0xc4ac5665u, 23)
-  B2D_MD5_STEP_FMA(B2D_MD5_I, a, b, c, d, m[0], 0xf4292244u, 6)
-  B2D_MD5_STEP_FMA(B2D_MD5_I, d, a, b, c, m[7], 0x432aff97u, 10)
-  B2D_MD5_STEP_FMA(B2D_MD5_I, c, d, a, b, m[14], 0xab9423a7u, 15)
-  B2D_MD5_STEP_FMA(B2D_MD5_I, b, c, d, a, m[5], 0xfc93a039u, 21)
-  B2D_MD5_STEP_FMA(B2D_MD5_I, a, b, c, d, m[12], 0x655b59c3u, 6)
-  B2D_MD5_STEP_FMA(B2D_MD5_I, d, a, b, c, m[3], 0x8f0ccc92u, 10)
-  B2D_MD5_STEP_FMA(B2D_MD5_I, c, d, a, b, m[10], 0xffeff47du, 15)
-  B2D_MD5_STEP_FMA(B2D_MD5_I, b, c, d, a, m[1], 0x85845dd1u, 21)
-  B2D_MD5_STEP_FMA(B2D_MD5_I, a, b, c, d, m[8], 0x6fa87e4fu, 6)
-  B2D_MD5_STEP_FMA(B2D_MD5_I, d, a, b, c, m[15], 0xfe2ce6e0u, 10)
-  B2D_MD5_STEP_FMA(B2D_MD5_I, c, d, a, b, m[6], 0xa3014314u, 15)
-  B2D_MD5_STEP_FMA(B2D_MD5_I, b, c, d, a, m[13], 0x4e0811a1u, 21)
-  B2D_MD5_STEP_FMA(B2D_MD5_I, a, b, c, d, m[4], 0xf7537e82u, 6)
-  B2D_MD5_STEP_FMA(B2D_MD5_I, d, a, b, c, m[11], 0xbd3af235u, 10)
-  B2D_MD5_STEP_FMA(B2D_MD5_I, c, d, a, b, m[2], 0x2ad7d2bbu, 15)
-  B2D_MD5_STEP_FMA(B2D_MD5_I, b, c, d, a, m[9], 0xeb86d391u, 21)
-  st[0] += a; st[1] += b; st[2] += c; st[3] += d;
-}
-#endif
 
 __host__ __device__ __forceinline__ void md5_init(uint32_t st[4]) {
   st[0] = 0x67452301u; st[1] = 0xefcdab89u; st[2] = 0x98badcfeu; st[3] = 0x10325476u;

@@ -174,8 +174,7 @@ __device__ __forceinline__ uint32_t swz(uint32_t o) {
 
 // fold the U-byte segment of row `row` of a staged tile into a lane's running digest state
 template <int U, int KIND>
-__device__ __forceinline__ void hash_segment(const uint8_t* stage, uint32_t row, Murmur3& mm, uint32_t md[4],
-                                             uint32_t one) {
+__device__ __forceinline__ void hash_segment(const uint8_t* stage, uint32_t row, Murmur3& mm, uint32_t md[4]) {
   const uint32_t base = row * U;
   if constexpr (KIND == HASH_MD5) {
 #pragma unroll
@@ -186,7 +185,7 @@ __device__ __forceinline__ void hash_segment(const uint8_t* stage, uint32_t row,
         const uint4 v = *reinterpret_cast<const uint4*>(stage + swz<U>(base + blk * 64u + 16u * j));
         m[4 * j + 0] = v.x; m[4 * j + 1] = v.y; m[4 * j + 2] = v.z; m[4 * j + 3] = v.w;
       }
-      md5_compress_fma(md, m, one);
+      md5_compress(md, m);
     }
   } else {
 #pragma unroll
@@ -197,16 +196,9 @@ __device__ __forceinline__ void hash_segment(const uint8_t* stage, uint32_t row,
   }
 }
 template <int KIND>
-__device__ __forceinline__ Digest finish_segments(Murmur3& mm, uint32_t md[4], uint32_t cs, uint32_t one) {
+__device__ __forceinline__ Digest finish_segments(Murmur3& mm, uint32_t md[4], uint32_t cs) {
   if constexpr (KIND == HASH_MD5) {
-    // the padding block of a message of whole 64-byte blocks (md5_pad_block64)
-    uint32_t m[16];
-#pragma unroll
-    for (int i = 0; i < 16; i++) m[i] = 0;
-    m[0] = 0x80u;
-    m[14] = cs << 3;
-    m[15] = cs >> 29;
-    md5_compress_fma(md, m, one);
+    md5_pad_block64(md, cs);
     return md5_digest(md);
   } else {
     return mm.finish(cs);
@@ -292,11 +284,11 @@ __global__ void __launch_bounds__((TMA_CONSUMER_WARPS + 1) * 32)
       const uint32_t s = k % stages, ph = (k / stages) & 1u;
       if (!warp_wait_full(&full[s], ph, a.st, &abort_flag, a.wait_polls)) return;
       const uint8_t* stage = smem + (size_t)s * STAGE_BYTES;
-      if (valid) hash_segment<U, KIND>(stage, row, mm, md, a.one);
+      if (valid) hash_segment<U, KIND>(stage, row, mm, md);
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
     }
-    if (valid) leaf_finish(a, chunk, finish_segments<KIND>(mm, md, a.cs, a.one), old);
+    if (valid) leaf_finish(a, chunk, finish_segments<KIND>(mm, md, a.cs), old);
   }
 }
 
@@ -407,12 +399,12 @@ __global__ void __launch_bounds__((TMA_CONSUMER_WARPS + 1) * 32)
       old.w[0] = old.w[1] = old.w[2] = old.w[3] = 0u;
       if (valid) old = prior_digest(with_round(items[it].args), chunk);
     }
-    if (valid) hash_segment<U, KIND>(smem + (size_t)s * STAGE_BYTES, row, mm, md, items[it].args.one);
+    if (valid) hash_segment<U, KIND>(smem + (size_t)s * STAGE_BYTES, row, mm, md);
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
     if (g + 1 == S && valid) {
       const LeafArgs a = with_round(items[it].args);
-      leaf_finish(a, chunk, finish_segments<KIND>(mm, md, a.cs, a.one), old);
+      leaf_finish(a, chunk, finish_segments<KIND>(mm, md, a.cs), old);
     }
   }
 }

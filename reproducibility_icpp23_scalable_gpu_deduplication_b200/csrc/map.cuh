@@ -5,29 +5,37 @@
 //   insert(key, value): insert-if-absent; reports inserted vs existing plus the slot;
 //   the slot's value stays mutable for the lowest-index update (tree_approach.cpp:85,339).
 //
-// Table layout (24 bytes per slot, in one allocation of cap + 1 slots):
-//   keys[i] : the 128-bit digest, claimed with one 128-bit atomicCAS (EMPTY = all ones); the
-//             keys sit together (eight to a 128-byte line), so a probe sequence reads only keys
-//   vals[i] : u64 = priority << 45 | checkpoint << 32 | node.  Every insert of the current
-//             checkpoint applies atomicMin to it; within one checkpoint the checkpoint field is
-//             the same, so the value left behind is the one the reference's sequential
-//             execution order inserts first (leaves by index, then first-occurrence parents by
-//             level and index, then the baseline's per-level inserts).  One atomic sets the
-//             owner and its checkpoint together.  All ones (checkpoint field MAP_TREE_PENDING)
-//             while the inserting thread has claimed the key but not yet merged its value:
-//             readers treat that as "this checkpoint".  Checkpoint ids are below
-//             MAP_TREE_PENDING.
-// The digest equal to the EMPTY pattern is kept in the extra slot `cap`: present once its
-// value is no longer all ones.
+// Table layout (cap + 1 slots in one allocation), one of two, chosen at build time:
+//   B2D_MAP_SPLIT 0 (default): a 32-byte slot per entry, the 128-bit key then its u64 value, so
+//     an insert's value update lands in the sector its key claim already brought in;
+//   B2D_MAP_SPLIT 1: all keys, then all values (24 bytes per slot): a probe reads only keys,
+//     eight to a line, but every value update is a second DRAM access (measured slower on the
+//     checkpoint path, which inserts or looks up every changed chunk).
+// keys: the 128-bit digest, claimed with one 128-bit atomicCAS (EMPTY = all ones).
+// values: u64 = priority << 45 | checkpoint << 32 | node.  Every insert of the current
+//   checkpoint applies atomicMin to it; within one checkpoint the checkpoint field is the same,
+//   so the value left behind is the one the reference's sequential execution order inserts first
+//   (leaves by index, then first-occurrence parents by level and index, then the baseline's
+//   per-level inserts).  One atomic sets the owner and its checkpoint together.  All ones
+//   (checkpoint field MAP_TREE_PENDING) while the inserting thread has claimed the key but not
+//   yet merged its value: readers treat that as "this checkpoint".  Checkpoint ids are below
+//   MAP_TREE_PENDING.
+// The digest equal to the EMPTY pattern is kept in the extra slot `cap`: present once its value
+// is no longer all ones.
 #pragma once
 #include "common.cuh"
+
+#ifndef B2D_MAP_SPLIT
+#define B2D_MAP_SPLIT 0
+#endif
 
 namespace b2d {
 
 struct __align__(16) Key128 {
   unsigned long long lo, hi;
 };
-constexpr uint64_t MAP_SLOT_BYTES = sizeof(Key128) + sizeof(unsigned long long);
+constexpr uint64_t MAP_SLOT_BYTES = B2D_MAP_SPLIT ? sizeof(Key128) + sizeof(unsigned long long) : 32;
+constexpr uint64_t MAP_STRIDE = B2D_MAP_SPLIT ? 1 : 2;   // Key128 units from one slot's key to the next
 
 constexpr unsigned long long MAP_EMPTY = ~0ull;
 constexpr uint32_t MAP_TREE_BITS = 13;
@@ -43,8 +51,8 @@ __device__ __forceinline__ uint32_t map_val_tree(unsigned long long v) {
 }
 
 struct MapView {
-  Key128* keys;               // cap + 1 keys
-  unsigned long long* vals;   // cap + 1 values, right behind the keys
+  Key128* keys;               // the first slot's key (slot i's: map_key)
+  unsigned long long* vals;   // the first slot's value (slot i's: map_val)
   uint64_t cap;               // any positive count (homes are mapped onto [0, cap) by a multiply)
   unsigned long long* size;   // device counter of occupied slots
 };
@@ -53,10 +61,15 @@ struct MapView {
 __host__ __device__ __forceinline__ MapView map_at(void* mem, uint64_t cap, unsigned long long* size) {
   MapView m;
   m.keys = static_cast<Key128*>(mem);
-  m.vals = reinterpret_cast<unsigned long long*>(m.keys + cap + 1);
+  m.vals = B2D_MAP_SPLIT ? reinterpret_cast<unsigned long long*>(m.keys + cap + 1)
+                         : reinterpret_cast<unsigned long long*>(m.keys) + 2;
   m.cap = cap;
   m.size = size;
   return m;
+}
+__host__ __device__ __forceinline__ Key128* map_key(const MapView& m, uint64_t i) { return m.keys + i * MAP_STRIDE; }
+__host__ __device__ __forceinline__ unsigned long long* map_val(const MapView& m, uint64_t i) {
+  return m.vals + (B2D_MAP_SPLIT ? i : 4 * i);
 }
 
 struct MapRef {
@@ -89,10 +102,10 @@ __device__ __forceinline__ uint64_t map_next(uint64_t i, uint64_t cap) { return 
 // before the launch).  Returns cap+1 when absent.
 __device__ __forceinline__ uint64_t map_find(const MapView& m, const Digest& d) {
   const Key128 k = digest_key(d);
-  if (key_is_empty_pattern(k)) return m.vals[m.cap] != MAP_EMPTY ? m.cap : m.cap + 1;
+  if (key_is_empty_pattern(k)) return *map_val(m, m.cap) != MAP_EMPTY ? m.cap : m.cap + 1;
   uint64_t i = map_home(k, m.cap);
   for (uint64_t probe = 0; probe < m.cap; probe++) {
-    const Key128 s = m.keys[i];
+    const Key128 s = *map_key(m, i);
     if (s.lo == k.lo && s.hi == k.hi) return i;
     if (s.lo == MAP_EMPTY && s.hi == MAP_EMPTY) return m.cap + 1;
     i = map_next(i, m.cap);
@@ -117,7 +130,7 @@ __device__ __forceinline__ MapRef map_insert_packed(const MapView& m, const Dige
   MapRef r{0, false, false, ~0ull};
   if (key_is_empty_pattern(k)) {
     // the extra slot: the first value merged into it inserts the key
-    r.prev = atomicMin(&m.vals[m.cap], val);
+    r.prev = atomicMin(map_val(m, m.cap), val);
     r.slot = m.cap;
     r.found = true;
     r.inserted = r.prev == MAP_EMPTY;
@@ -129,7 +142,7 @@ __device__ __forceinline__ MapRef map_insert_packed(const MapView& m, const Dige
   const Key128 empty{MAP_EMPTY, MAP_EMPTY};
   uint64_t i = map_home(k, m.cap);
   for (uint64_t probe = 0; probe < m.cap; probe++) {
-    Key128* s = &m.keys[i];
+    Key128* s = map_key(m, i);
     bool try_cas = true;
     if (!cas_only) {
       const unsigned long long lo = *reinterpret_cast<volatile unsigned long long*>(&s->lo);
@@ -145,7 +158,7 @@ __device__ __forceinline__ MapRef map_insert_packed(const MapView& m, const Dige
     if (try_cas) {
       const Key128 old = atomicCAS(s, empty, k);
       if (old.lo == MAP_EMPTY && old.hi == MAP_EMPTY) {
-        r.prev = atomicMin(&m.vals[i], val);
+        r.prev = atomicMin(map_val(m, i), val);
         count_insert(m.size);
         r.slot = i; r.found = true; r.inserted = true;
         return r;
@@ -173,7 +186,7 @@ __device__ __forceinline__ MapRef map_insert(const MapView& m, const Digest& d, 
 // older checkpoint is never changed by this one, so its id cannot change under the test.
 __device__ __forceinline__ bool map_merge_current(const MapView& m, uint64_t slot, unsigned long long val,
                                                   uint32_t cur, unsigned long long* prev = nullptr) {
-  unsigned long long* v = &m.vals[slot];
+  unsigned long long* v = map_val(m, slot);
   const uint32_t t = map_val_tree(*reinterpret_cast<volatile unsigned long long*>(v));
   if (t == (cur & MAP_TREE_PENDING) || t == MAP_TREE_PENDING) {
     const unsigned long long p = atomicMin(v, map_pack(val, cur));
@@ -184,10 +197,10 @@ __device__ __forceinline__ bool map_merge_current(const MapView& m, uint64_t slo
 }
 
 __device__ __forceinline__ uint32_t map_node(const MapView& m, uint64_t slot) {
-  return (uint32_t)(m.vals[slot] & 0xffffffffull);
+  return (uint32_t)(*map_val(m, slot) & 0xffffffffull);
 }
 __device__ __forceinline__ uint32_t map_tree(const MapView& m, uint64_t slot) {
-  return map_val_tree(m.vals[slot]);
+  return map_val_tree(*map_val(m, slot));
 }
 
 }  // namespace b2d
