@@ -319,7 +319,8 @@ def run_batched(args, rank, world, dev, emit=True):
             h.close()
         del ss
         torch.cuda.empty_cache()
-    tuned = {k: batch.get_param(k) for k in ("shared", "leaf_stages", "leaf_ctas_per_sm", "tiles_per_pop")}
+    tuned = {k: batch.get_param(k) for k in ("shared", "leaf_stages", "leaf_ctas_per_sm", "tiles_per_pop",
+                                              "warp_bands", "map_headroom_pct")}
 
     def batch_step(hs, bufs, base):
         batch.checkpoint(hs, bufs)
@@ -523,14 +524,14 @@ def run_served(args, rank, world, dev, emit=True):
 
 def bounded_forms(args, rank, world, dev):
     """The batched form (all 256 buffers, 2 warm-up and --forms-steps timed batches after at most
-    6 autotuning batches) and the served form (64 clients, --forms-requests Poisson requests, 2
+    8 autotuning batches: a baseline and the tuner's 7) and the served form (64 clients, --forms-requests Poisson requests, 2
     capacity waves), summarised as two keys of the plain line."""
     import copy
 
     import torch
 
     b_args = copy.copy(args)
-    b_args.warmup, b_args.steps, b_args.tune_batches = 2, max(1, args.forms_steps), 6
+    b_args.warmup, b_args.steps, b_args.tune_batches = 2, max(1, args.forms_steps), 8
     b = run_batched(b_args, rank, world, dev, emit=False)
     torch.cuda.empty_cache()
     s_args = copy.copy(args)

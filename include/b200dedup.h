@@ -88,6 +88,10 @@ int b2d_set_stream(b2d_dedup* d, void* cuda_stream);
  *                       when the map's entries plus every node of the tree fit under it
  *   "map_headroom_pct"  size of a baseline's map over that minimum, 100..1000 (default 150);
  *                       more headroom = fewer growths (allocate + rehash) in a long series
+ *   "warp_bands"        forest phases whose lowest levels run as warp tasks (7 levels per task
+ *                       in phase 1, 9 in phase 2) instead of CTA bands (10 and 12 levels): bit 0
+ *                       phase 1, bit 1 phase 2, 0..3 (default 3); trees whose chunk count is not
+ *                       a power of two always use CTA bands
  *   "graph"             0 = launch a checkpoint's kernels one by one on the handle's stream
  *                       (default; measured faster), 1 = replay them as one CUDA graph, 2 = graph
  *                       without the phase-timing events (b2d_phase_times then reads 0) */
@@ -250,15 +254,20 @@ int b2d_batch_set_stream(b2d_batch* b, void* cuda_stream);
 /* Tuning: "leaf_stages" (staging ring depth, 0 = 64 KB ring), "leaf_ctas_per_sm" (0 = 3),
  * "tiles_per_pop" (work-queue granule, tiles of 256 chunks), "streams" (graph branches for the
  * per-handle work when "shared" is 0), "shared" (1 = the shared segmented forest/diff launches,
- * default; 0 = per-handle launches on "streams" branches), "autotune" (1: coordinate descent over
- * shared, tiles_per_pop and staging, one setting per incremental batch -- five batches --
- * measured by device time; "tuned" reads 1 once it has
+ * default; 0 = per-handle launches on "streams" branches), "warp_bands" (the fused levels of the
+ * first forest band, as the handle parameter of that name, default 3), "map_headroom_pct" (the
+ * digest-map load factor: table size over its minimum, default 150; a handle whose table was
+ * sized otherwise is resized before its next batch), "autotune" (1: coordinate descent over
+ * shared, tiles_per_pop, staging, warp_bands {3, 0} and map_headroom_pct {150, 125}, one setting
+ * per incremental batch -- seven batches -- measured by device time, a value kept when it is at
+ * least 1 % faster; "tuned" reads 1 once it has
  * settled and the knobs then read the chosen values), "graph" (2 = launch a composition directly
  * the first time and as a captured graph from its second batch on, default; 1 = always a graph;
  * 0 = never), "graph_cache" (instantiated graphs kept, one per batch composition, default 16),
  * "batch_diff" (1 = every handle's diff assembly in 12-13 shared launches after all trees are
  * labelled, default; 0 = per handle in its own branch), "batch_forest" (1 = every handle's
  * Merkle-forest phases in shared launches, one per tree step, default; needs batch_diff).
+ * A batch applies its warp_bands and map_headroom_pct to every handle it checkpoints.
  * Output never depends on them. */
 int b2d_batch_set_param(b2d_batch* b, const char* name, int64_t value);
 int b2d_batch_get_param(b2d_batch* b, const char* name, int64_t* value);

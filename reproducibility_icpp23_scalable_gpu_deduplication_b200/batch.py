@@ -15,8 +15,8 @@ __all__ = ["CheckpointBatch"]
 
 
 class CheckpointBatch:
-    PARAMS = ("leaf_stages", "leaf_ctas_per_sm", "tiles_per_pop", "streams", "shared", "autotune", "graph_cache",
-              "graph", "batch_diff", "batch_forest")
+    PARAMS = ("leaf_stages", "leaf_ctas_per_sm", "tiles_per_pop", "streams", "shared", "warp_bands",
+              "map_headroom_pct", "autotune", "graph_cache", "graph", "batch_diff", "batch_forest")
 
     def __init__(self, autotune=False, **params):
         h = ctypes.c_void_p()

@@ -163,6 +163,8 @@ struct b2d_dedup {
   bool use_graph = false;
   bool graph_timing = true;       // phase timing events inside the graph
   double map_headroom = MAP_HEADROOM;   // baseline table size over its minimum (entries + N at max load)
+  bool map_retune = false;              // resize an existing table to map_headroom at the next checkpoint
+  int warp_bands = B2D_WARP_BANDS;      // forest phases that start with a warp band (bit 0: 1, bit 1: 2)
 
   cudaStream_t own_stream = nullptr;
   cudaStream_t cap_stream = nullptr;   // graph capture only
@@ -353,8 +355,19 @@ uint64_t map_capacity(uint64_t need, double max_load, double headroom) {
 
 int map_ensure(b2d_dedup* d) {
   const uint64_t need = d->map_size_host + d->N;
-  if (d->map_mem && (double)need <= d->map_max_load * (double)d->map_cap) return B2D_OK;
-  const uint64_t cap = map_capacity(need, d->map_max_load, MAP_GROWTH);
+  // a retune (the batch tuner's load-factor knob) resizes the table to map_headroom over its
+  // minimum, unless it is already within 10 % of that
+  uint64_t cap = 0;
+  if (d->map_retune && d->map_mem && d->map_size_host > 0) {
+    const uint64_t want = map_capacity(need, d->map_max_load, d->map_headroom);
+    if (want * 10 < d->map_cap * 9 || want * 9 > d->map_cap * 10) cap = want;
+  }
+  d->map_retune = false;
+  const bool grow = cap == 0;
+  if (grow) {
+    if (d->map_mem && (double)need <= d->map_max_load * (double)d->map_cap) return B2D_OK;
+    cap = map_capacity(need, d->map_max_load, MAP_GROWTH);
+  }
   if (!d->map_mem || d->map_size_host == 0) return map_reset(d, cap);
   const auto t0 = std::chrono::high_resolution_clock::now();
   void* fresh = nullptr;
@@ -379,7 +392,7 @@ int map_ensure(b2d_dedup* d) {
   std::swap(d->map_size.n, cnt.n);
   d->map_cap = cap;
   d->map_grow_s += secs(t0, std::chrono::high_resolution_clock::now());
-  d->map_grows += 1;
+  if (grow) d->map_grows += 1;
   return B2D_OK;
 }
 
@@ -502,7 +515,7 @@ void graph_key(const b2d_dedup* d, const RoundState* rs_dev, std::vector<uint64_
             (uint64_t)d->state.p, (uint64_t)d->state_h.p, (uint64_t)d->round_h.p, (uint64_t)rs_dev, d->bcap,
             (uint64_t)d->tune.allow_tma, (uint64_t)d->tune.stages, (uint64_t)d->tune.ctas_per_sm, (uint64_t)d->graph_timing,
             (uint64_t)d->tune.unit, (uint64_t)d->tune.wait_polls,
-            (uint64_t)d->sm_count, (uint64_t)d->list});
+            (uint64_t)d->sm_count, (uint64_t)d->list, (uint64_t)d->warp_bands});
 }
 
 // Device work of one checkpoint on `s`.  `rs_dev` is where the kernels read this checkpoint's
@@ -549,12 +562,12 @@ int enqueue_checkpoint(b2d_dedup* d, cudaStream_t s, RoundState* rs_dev, bool up
     B2D_CU(launch_list_label(forest_args(d, rs_dev), d->sm_count, s));
   } else if (!skip_forest) {
     const ForestArgs fa = forest_args(d, rs_dev);
-    B2D_CU(launch_forest(fa, 1, s, d->sm_count));
+    B2D_CU(launch_forest(fa, 1, s, d->sm_count, d->warp_bands));
     // the zero-digest probe matters to baselines only; launches issued one by one for a single
     // handle skip it otherwise (a captured graph or a batch keeps it: it serves both kinds)
     if (managed || d->use_graph || d->round_h.p->baseline) B2D_CU(launch_zero_exists(&ds->zero_exists, rs_dev, s));
     else zero_probe_skipped = true;
-    B2D_CU(launch_forest(fa, 2, s, d->sm_count));
+    B2D_CU(launch_forest(fa, 2, s, d->sm_count, d->warp_bands));
   }
   if (timing) B2D_CU(record_timing(d->ev[1], s));
   // collect_diff (:511-710; list approach src/list_approach.cpp:79-257, single-chunk regions in
@@ -573,7 +586,8 @@ int enqueue_checkpoint(b2d_dedup* d, cudaStream_t s, RoundState* rs_dev, bool up
     d->launches = (skip_leaves ? 0 : 1) + 1 + (skip_diff ? 0 : 10);
   else
     d->launches = (skip_leaves ? 0 : 1) +
-                  (skip_forest ? 0 : forest_launch_count(d->n, d->D, 1) + forest_launch_count(d->n, d->D, 2) +
+                  (skip_forest ? 0 : forest_launch_count(d->n, d->D, 1, d->warp_bands) +
+                                         forest_launch_count(d->n, d->D, 2, d->warp_bands) +
                                          (zero_probe_skipped ? 0 : 1)) +
                   (skip_diff ? 0 : 12);
   return B2D_OK;
@@ -1038,38 +1052,49 @@ __global__ void batch_collect_kernel(DevState* const* states, uint32_t count, De
 
 struct BatchCand {
   int stages, ctas, tiles_per_pop, streams, shared;
+  int warp;       // forest phases starting with a warp band (B2D_WARP_BANDS mask): fused levels
+  int headroom;   // digest-map size over its minimum, percent: the load factor
 };
 
 // Online coordinate-descent tuner.  Each incremental batch (same bytes every time) measures one
 // setting by its graph's device time: first the current setting, then, one knob at a time,
-// each other value of that knob, keeping a value whenever it is faster.  Knobs: shared
-// segmented forest/diff launches for all handles or per-handle launches on 32 graph branches,
-// tiles (of 256 chunks) per work-queue pop, and staging (ring depth x CTAs per SM) of the
-// hashing kernel.  1 + 1 + 2 + 1 = 5 measured batches.
+// each other value of that knob, keeping a value when it is at least 1 % faster (batches
+// differ in content, so smaller gains are not trusted).  Knobs:
+//   shared      segmented forest/diff launches for all handles, or per-handle launches on 32
+//               graph branches;
+//   tiles/pop   chunk ranges (tiles of 256 chunks) a hashing CTA takes per work-queue pop: 4, 1, 16;
+//   staging     ring depth x CTAs per SM of the hashing kernel;
+//   fused       levels fused in the first forest band: warp bands (7 + 9) or CTA bands (10 + 12);
+//   load        digest-map headroom 1.5 or 1.25 (load 0.25 or 0.3 after a baseline; both leave
+//               room for dozens of checkpoints before a growth); a change resizes every
+//               handle's table before the next batch (outside the timed graph).
+// 1 + 1 + 2 + 1 + 1 + 1 = 7 measured batches.
 struct BatchTuner {
-  static constexpr int KNOBS = 3;
-  BatchCand base{0, 3, 4, 32, 1};
+  static constexpr int KNOBS = 5;
+  BatchCand base{0, 3, 4, 32, 1, B2D_WARP_BANDS, 150};
   double base_score = 0;
   bool have_base = false, done = false;
   int knob = 0;
   size_t idx = 0;
-  BatchCand pending{0, 3, 4, 32, 1};
+  BatchCand pending = base;
 
   static size_t nvalues(int k) { return k == 1 ? 3 : 2; }
   static BatchCand with_value(BatchCand c, int k, size_t i) {
     static const int tpp[3] = {4, 1, 16};
     static const int stages[2] = {0, 3}, ctas[2] = {3, 2};
+    static const int warp[2] = {B2D_WARP_BANDS, 0}, headroom[2] = {150, 125};
     if (k == 0) c.shared = i == 0 ? 1 : 0;
     else if (k == 1) c.tiles_per_pop = tpp[i];
-    else {
+    else if (k == 2) {
       c.stages = stages[i];
       c.ctas = ctas[i];
-    }
+    } else if (k == 3) c.warp = warp[i];
+    else c.headroom = headroom[i];
     return c;
   }
   static bool same(const BatchCand& a, const BatchCand& b) {
     return a.stages == b.stages && a.ctas == b.ctas && a.tiles_per_pop == b.tiles_per_pop &&
-           a.streams == b.streams && a.shared == b.shared;
+           a.streams == b.streams && a.shared == b.shared && a.warp == b.warp && a.headroom == b.headroom;
   }
   void reset(const BatchCand& start) {
     *this = BatchTuner();
@@ -1096,7 +1121,7 @@ struct BatchTuner {
       base_score = score;
       return;
     }
-    if (score > base_score) {
+    if (score > 1.01 * base_score) {
       base = pending;
       base_score = score;
     }
@@ -1150,7 +1175,7 @@ struct b2d_batch {
   bool fl_scoring = false, fl_any_baseline = false;
   std::chrono::high_resolution_clock::time_point fl_t0;
   // tuning: current values, and the online tuner
-  BatchCand cur{0, 3, 4, 32, 1};
+  BatchCand cur{0, 3, 4, 32, 1, B2D_WARP_BANDS, 150};
   bool autotune = false;
   BatchTuner tuner;
   // last batch
@@ -1229,6 +1254,12 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
   uint64_t bytes = 0;
   for (uint32_t i = 0; i < count; i++) {
     b2d_dedup* d = hs[i];
+    // the batch's fused levels and map headroom apply to every handle it checkpoints
+    d->warp_bands = cand.warp;
+    if (d->map_headroom != cand.headroom / 100.0) {
+      d->map_headroom = cand.headroom / 100.0;
+      d->map_retune = true;
+    }
     cudaStream_t keep = d->stream;
     d->stream = b->stream;
     const bool mb = make_baseline && make_baseline[i];
@@ -1307,7 +1338,7 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
       fsteps[ph].resize(count);
       uint32_t K = 0;
       for (uint32_t i = 0; i < count; i++) {
-        if (!hs[i]->list) forest_steps_batch(hs[i]->n, hs[i]->D, hs[i]->N, ph + 1, fsteps[ph][i]);
+        if (!hs[i]->list) forest_steps_batch(hs[i]->n, hs[i]->D, hs[i]->N, ph + 1, fsteps[ph][i], hs[i]->warp_bands);
         K = std::max<uint32_t>(K, (uint32_t)fsteps[ph][i].size());
       }
       for (uint32_t k = 0; k < K; k++)
@@ -1437,7 +1468,8 @@ int batch_launch(b2d_batch* b, b2d_dedup* const* hs, const void* const* data, co
   key.insert(key.end(), {(uint64_t)B, (uint64_t)H, L.total, (uint64_t)seg_diff, (uint64_t)seg_forest,
                          (uint64_t)b->coll.p,
                          (uint64_t)b->coll_h.p, (uint64_t)cand.stages,
-                         (uint64_t)cand.ctas, (uint64_t)cand.tiles_per_pop, (uint64_t)cand.streams});
+                         (uint64_t)cand.ctas, (uint64_t)cand.tiles_per_pop, (uint64_t)cand.streams,
+                         (uint64_t)cand.shared, (uint64_t)cand.warp});
 
   const uint64_t kh = key_hash(key);
   b2d_batch::GraphEntry* ge = nullptr;
@@ -1881,6 +1913,7 @@ int b2d_set_param(b2d_dedup* d, const char* name, int64_t value) {
   else if (k == "leaf_wait_polls" && value >= 0 && value <= (1 << 20)) d->tune.wait_polls = (int)value;
   else if (k == "map_max_load_pct" && value >= 10 && value <= 90) d->map_max_load = value / 100.0;
   else if (k == "map_headroom_pct" && value >= 100 && value <= 1000) d->map_headroom = value / 100.0;
+  else if (k == "warp_bands" && value >= 0 && value <= 3) d->warp_bands = (int)value;
   else if (k == "graph" && value >= 0 && value <= 2) {
     d->use_graph = value != 0;
     d->graph_timing = value != 2;
@@ -2076,6 +2109,8 @@ int b2d_batch_set_param(b2d_batch* b, const char* name, int64_t value) {
   else if (k == "tiles_per_pop" && value >= 1 && value <= 1024) b->cur.tiles_per_pop = (int)value;
   else if (k == "streams" && value >= 1 && value <= 64) b->cur.streams = (int)value;
   else if (k == "shared" && (value == 0 || value == 1)) b->cur.shared = (int)value;
+  else if (k == "warp_bands" && value >= 0 && value <= 3) b->cur.warp = (int)value;
+  else if (k == "map_headroom_pct" && value >= 100 && value <= 1000) b->cur.headroom = (int)value;
   else if (k == "graph_cache" && value >= 1 && value <= 4096) b->graph_cap = (size_t)value;
   else if (k == "graph" && value >= 0 && value <= 2) b->graph_mode = (int)value;
   else if (k == "batch_diff" && (value == 0 || value == 1)) b->batch_diff = value != 0;
@@ -2095,6 +2130,8 @@ int b2d_batch_get_param(b2d_batch* b, const char* name, int64_t* value) {
   else if (k == "tiles_per_pop") *value = b->cur.tiles_per_pop;
   else if (k == "streams") *value = b->cur.streams;
   else if (k == "shared") *value = b->cur.shared;
+  else if (k == "warp_bands") *value = b->cur.warp;
+  else if (k == "map_headroom_pct") *value = b->cur.headroom;
   else if (k == "autotune") *value = b->autotune ? 1 : 0;
   else if (k == "tuned") *value = b->tuner.done ? 1 : 0;
   else if (k == "graph_cache") *value = (int64_t)b->graph_cap;

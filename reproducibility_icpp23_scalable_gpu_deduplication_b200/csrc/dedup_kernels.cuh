@@ -179,8 +179,15 @@ int batch_leaf_item(const LeafArgs& a, BatchLeafItem& item);
 cudaError_t launch_leaves_batch(const BatchLeafItem* d_items, uint32_t nitems, uint32_t total_tiles, int U, int kind,
                                 unsigned int* queue, DevStatus* st, int sm_count, const LeafTuning& tune,
                                 uint32_t tiles_per_pop, cudaStream_t stream);
-// sm_count > 0: the first band runs on a resident grid (see forest.cu)
-cudaError_t launch_forest(const ForestArgs& a, int phase, cudaStream_t stream, int sm_count = 0);
+// Which forest phases start with a warp band (7 levels per task in phase 1, 9 in phase 2)
+// instead of a CTA band (10 and 12 levels): bit 0 phase 1, bit 1 phase 2.  The default of the
+// handle parameter "warp_bands" and of the batch tuner's fused-levels knob.
+#ifndef B2D_WARP_BANDS
+#define B2D_WARP_BANDS 3
+#endif
+// sm_count > 0: the first band runs on a resident grid (see forest.cu); warp_mask as above
+cudaError_t launch_forest(const ForestArgs& a, int phase, cudaStream_t stream, int sm_count = 0,
+                          int warp_mask = B2D_WARP_BANDS);
 
 // CTA b of a segmented launch belongs to the handle h with beg[h] <= b < beg[h+1]
 __device__ __forceinline__ uint32_t seg_find(const uint32_t* beg, uint32_t n, uint32_t& bid, uint32_t& nb) {
@@ -204,7 +211,8 @@ void forest_steps(uint32_t D, uint64_t N, int phase, std::vector<ForestStep>& ou
 // the steps of the batched form: a warp band first where the tree allows one (kind 2: p0 = D,
 // one warp per task of 128 (phase 1) or 512 (phase 2) leaves, 8 tasks per CTA), then the bands
 // above it
-void forest_steps_batch(uint32_t n, uint32_t D, uint64_t N, int phase, std::vector<ForestStep>& out);
+void forest_steps_batch(uint32_t n, uint32_t D, uint64_t N, int phase, std::vector<ForestStep>& out,
+                        int warp_mask = B2D_WARP_BANDS);
 // the same step of many handles' trees in one launch (batched form); handles without this
 // step have no CTAs
 struct ForestSeg {
@@ -216,7 +224,7 @@ struct ForestSeg {
 };
 cudaError_t launch_forest_seg(const ForestSeg& s, int phase, int kind, uint32_t ctas, cudaStream_t stream);
 cudaError_t launch_zero_exists_seg(const ForestArgs* args, uint32_t n, cudaStream_t stream);
-int forest_launch_count(uint32_t n, uint32_t D, int phase);
+int forest_launch_count(uint32_t n, uint32_t D, int phase, int warp_mask = B2D_WARP_BANDS);
 cudaError_t launch_zero_exists(int* flag, const RoundState* rs, cudaStream_t stream);
 // bcap: bucket capacity the scratch was sized for (>= rs->buckets of every checkpoint run).
 // node_order: the region lists stay in node order (the list approach's order, whose regions

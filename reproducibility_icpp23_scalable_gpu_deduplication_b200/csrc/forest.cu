@@ -492,16 +492,21 @@ __global__ void __launch_bounds__(FAST_THREADS, B2D_FAST_MINB) forest_fast_seg(F
 // A task writes its root's label to `lab` for the band above (which is a CTA band again: few
 // nodes are left there).  Same per-node rules as the CTA bands, so the labels, digests, map
 // entries and push flags are the same.
-// bit 0: phase 1 starts with a warp band, bit 1: phase 2 does
-#ifndef B2D_WARP_BANDS
-#define B2D_WARP_BANDS 3
-#endif
+// Which phases start with one is a runtime mask (B2D_WARP_BANDS, the default, in dedup_kernels.cuh).
 constexpr uint32_t WB1_LEVELS = 7;
 constexpr uint32_t WB2_LEVELS = 9;
 constexpr uint32_t WB_THREADS = 256;
+// resident CTAs per SM the warp bands are compiled for (phase 1: 5, 48 registers; phase 2: 4,
+// 64 registers)
+#ifndef B2D_WB1_MINB
+#define B2D_WB1_MINB 5
+#endif
+#ifndef B2D_WB2_MINB
+#define B2D_WB2_MINB 4
+#endif
 
-static bool warp_bands(uint32_t n, uint32_t D, int phase) {
-  return (B2D_WARP_BANDS & (phase == 1 ? 1 : 2)) && n >= 2u && (n & (n - 1u)) == 0 &&
+static bool warp_bands(uint32_t n, uint32_t D, int phase, int mask) {
+  return (mask & (phase == 1 ? 1 : 2)) && n >= 2u && (n & (n - 1u)) == 0 &&
          D >= (phase == 1 ? WB1_LEVELS : WB2_LEVELS);
 }
 
@@ -538,12 +543,26 @@ __device__ __forceinline__ void warp1_task(const ForestArgs& a, uint32_t task, u
     if (lane == 0) band_output<1>(a, root, DONE);
     return;
   }
-  if (m0 && *reinterpret_cast<const uint32_t*>(a.dupflag + c0)) {
-    // lowest-index relabel of the first occurrences the leaf stage flagged as sharing a digest
+  // the leaf digests of both pairs are loaded together with the duplicate flags (a relabel
+  // below only drops pairs, and rarely)
+  Digest lv[4];
 #pragma unroll
-    for (int j = 0; j < 4; j++)
-      if ((m0 >> j) & 1u)
-        if (leaf_view<1>(a, (uint32_t)(x0 + j), FIRST_OCUR) != FIRST_OCUR) m0 &= ~(1u << j);
+  for (int j = 0; j < 4; j++) lv[j].w[0] = lv[j].w[1] = lv[j].w[2] = lv[j].w[3] = 0u;
+  if (m0) {
+    const uint32_t df = *reinterpret_cast<const uint32_t*>(a.dupflag + c0);
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+      if (((m0 >> (2 * j)) & 3u) == 3u) {
+        lv[2 * j] = a.tree[x0 + 2 * j];
+        lv[2 * j + 1] = a.tree[x0 + 2 * j + 1];
+      }
+    if (df) {
+      // lowest-index relabel of the first occurrences the leaf stage flagged as sharing a digest
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        if ((m0 >> j) & 1u)
+          if (leaf_view<1>(a, (uint32_t)(x0 + j), FIRST_OCUR) != FIRST_OCUR) m0 &= ~(1u << j);
+    }
   }
   // height 1: nodes p0, p0 + 1; height 2: node y
   const uint64_t p0 = (x0 - 1ull) >> 1;
@@ -553,7 +572,7 @@ __device__ __forceinline__ void warp1_task(const ForestArgs& a, uint32_t task, u
   for (int j = 0; j < 2; j++) {
     d1[j].w[0] = d1[j].w[1] = d1[j].w[2] = d1[j].w[3] = 0u;
     if (((m0 >> (2 * j)) & 3u) == 3u) {
-      d1[j] = hash_pair(a.kind, a.tree[x0 + 2 * j], a.tree[x0 + 2 * j + 1]);
+      d1[j] = hash_pair(a.kind, lv[2 * j], lv[2 * j + 1]);
       a.tree[p0 + j] = d1[j];
       wi_add(wi, (uint32_t)(p0 + j), d1[j]);
       m1 |= 1u << j;
@@ -630,7 +649,25 @@ __device__ __forceinline__ void warp2_task(const ForestArgs& a, uint32_t task, u
   if (lane == 0) band_output<2>(a, root, lab);
 }
 
-// Resident grid of warps; warp g takes tasks g, g + G, ... and loads the next one's labels first.
+// Resident grid of warps over the tasks.  B2D_WARP_QUEUE 1 (default): two passes per CTA.
+//   scan: warp w of the grid tests tasks w, w + G, w + 2G, ... four at a time (their labels
+//         loaded while the previous four are handled), writes the output of every task without
+//         work and queues the others in the CTA's shared memory;
+//   work: after one CTA barrier the CTA's 8 warps take the queued tasks in turn.
+// A run of changed chunks covers consecutive tasks, which the stride spreads over warps, and
+// the queue evens out each CTA's share of work tasks over its warps: with one fixed task per
+// warp and step, a launch waited for the warps that drew the most work.  Groups of consecutive
+// tasks taken from a global counter measured slower than either (a run's tasks then fall to one
+// warp).  Where a CTA's tasks could overflow its queue (more than WB_QUEUE, from 2^27 chunks at
+// a resident grid) and with B2D_WARP_QUEUE 0, warp w runs tasks w, w + G, ... itself, the next
+// one's labels loaded first.
+#ifndef B2D_WARP_QUEUE
+#define B2D_WARP_QUEUE 1
+#endif
+constexpr uint32_t WB_QUEUE = 1024;   // queued tasks per CTA
+constexpr uint32_t WB_SCAN = 4;       // tasks tested per scan step of a warp
+constexpr uint32_t WB_FULL = 0xffffffffu;
+
 #define B2D_WARP_INSERT_BUFFERS                                                                 \
   __shared__ uint32_t wi_node_[WB_THREADS / 32u][128];                                          \
   __shared__ Digest wi_dig_[WB_THREADS / 32u][128];                                             \
@@ -638,36 +675,142 @@ __device__ __forceinline__ void warp2_task(const ForestArgs& a, uint32_t task, u
   const WarpInserts wi{wi_node_[threadIdx.x >> 5], wi_dig_[threadIdx.x >> 5], &wi_count_[threadIdx.x >> 5]}; \
   if ((threadIdx.x & 31u) == 0) *wi.count = 0;                                                  \
   __syncwarp();
-__global__ void __launch_bounds__(WB_THREADS) forest_warp1_kernel(ForestArgs a0, uint32_t ntasks) {
-  griddep_enter();
-  B2D_WARP_INSERT_BUFFERS
-  const ForestArgs a = with_round(a0);
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t G = (gridDim.x * WB_THREADS) >> 5;
-  uint32_t task = (blockIdx.x * WB_THREADS + threadIdx.x) >> 5;
-  const uint32_t* lab32 = reinterpret_cast<const uint32_t*>(a.leaflab);
-  uint32_t w = task < ntasks ? lab32[task * 32u + lane] : 0u;
-  for (; task < ntasks; task += G) {
-    const uint32_t next = task + G;
-    const uint32_t wn = next < ntasks ? lab32[next * 32u + lane] : 0u;
-    warp1_task(a, task, lane, w, wi);
-    w = wn;
+
+// the CTA's task queue: entries, reserved count, taken count
+#define B2D_WARP_QUEUE_BUFFERS                                                                  \
+  __shared__ uint32_t wq_[WB_QUEUE];                                                            \
+  __shared__ uint32_t wq_n_, wq_h_;                                                             \
+  if (threadIdx.x == 0) {                                                                       \
+    wq_n_ = 0;                                                                                  \
+    wq_h_ = 0;                                                                                  \
+  }                                                                                             \
+  __syncthreads();
+
+__device__ __forceinline__ bool has_zero_byte(uint32_t w) {
+  return ((w - 0x01010101u) & ~w & 0x80808080u) != 0u;
+}
+// lane 0 queues `task` (the launch guarantees room: at most WB_QUEUE tasks per CTA)
+__device__ __forceinline__ void wq_push(uint32_t* q, uint32_t* n, uint32_t task, uint32_t lane) {
+  if (lane == 0) {
+    const uint32_t pos = atomicAdd(n, 1u);
+    if (pos < WB_QUEUE) q[pos] = task;
   }
 }
-__global__ void __launch_bounds__(WB_THREADS) forest_warp2_kernel(ForestArgs a0, uint32_t ntasks) {
+// next queued task for this warp, or ~0 once the queue is drained
+__device__ __forceinline__ uint32_t wq_pop(const uint32_t* q, uint32_t* h, uint32_t n, uint32_t lane) {
+  uint32_t i = 0;
+  if (lane == 0) i = atomicAdd(h, 1u);
+  i = __shfl_sync(WB_FULL, i, 0);
+  return i < (n < WB_QUEUE ? n : WB_QUEUE) ? q[i] : ~0u;
+}
+// tasks of one CTA of a resident grid of `grid` CTAs fit its queue
+static bool wq_fits(uint32_t ntasks, uint32_t grid) {
+  const uint64_t warps = (uint64_t)grid * (WB_THREADS / 32u);
+  return B2D_WARP_QUEUE && ((uint64_t)ntasks + warps - 1u) / warps * (WB_THREADS / 32u) <= WB_QUEUE;
+}
+
+__global__ void __launch_bounds__(WB_THREADS, B2D_WB1_MINB)
+    forest_warp1_kernel(ForestArgs a0, uint32_t ntasks, uint32_t queue) {
   griddep_enter();
+  B2D_WARP_INSERT_BUFFERS
+  B2D_WARP_QUEUE_BUFFERS
   const ForestArgs a = with_round(a0);
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t G = (gridDim.x * WB_THREADS) >> 5;
-  uint32_t task = (blockIdx.x * WB_THREADS + threadIdx.x) >> 5;
-  const uint4* lab128 = reinterpret_cast<const uint4*>(a.leaflab);
-  uint4 w = task < ntasks ? lab128[task * 32u + lane] : make_uint4(0, 0, 0, 0);
-  for (; task < ntasks; task += G) {
-    const uint32_t next = task + G;
-    const uint4 wn = next < ntasks ? lab128[next * 32u + lane] : make_uint4(0, 0, 0, 0);
-    warp2_task(a, task, lane, w);
-    w = wn;
+  const uint32_t w0 = (blockIdx.x * WB_THREADS + threadIdx.x) >> 5;
+  const uint32_t* lab32 = reinterpret_cast<const uint32_t*>(a.leaflab);
+  if (!queue) {
+    uint32_t w = w0 < ntasks ? lab32[w0 * 32u + lane] : 0u;
+    for (uint32_t task = w0; task < ntasks; task += G) {
+      const uint32_t next = task + G;
+      const uint32_t wn = next < ntasks ? lab32[next * 32u + lane] : 0u;
+      warp1_task(a, task, lane, w, wi);
+      w = wn;
+    }
+    return;
   }
+  const uint64_t root0 = (1ull << (a.D - WB1_LEVELS)) - 1ull;
+  uint32_t wn[WB_SCAN];
+#pragma unroll
+  for (uint32_t k = 0; k < WB_SCAN; k++) {
+    const uint32_t t = w0 + k * G;
+    wn[k] = t < ntasks ? lab32[t * 32u + lane] : 0x01010101u;
+  }
+  for (uint32_t t0 = w0; t0 < ntasks; t0 += WB_SCAN * G) {
+    uint32_t work = 0;   // bit k: task t0 + kG holds a first occurrence
+#pragma unroll
+    for (uint32_t k = 0; k < WB_SCAN; k++)
+      if (__any_sync(WB_FULL, has_zero_byte(wn[k]))) work |= 1u << k;
+#pragma unroll
+    for (uint32_t k = 0; k < WB_SCAN; k++) {
+      const uint32_t t = t0 + (WB_SCAN + k) * G;
+      wn[k] = t < ntasks ? lab32[t * 32u + lane] : 0x01010101u;
+    }
+#pragma unroll
+    for (uint32_t k = 0; k < WB_SCAN; k++) {
+      const uint32_t t = t0 + k * G;
+      if (t >= ntasks) break;
+      if ((work >> k) & 1u) wq_push(wq_, &wq_n_, t, lane);
+      else if (lane == 0) band_output<1>(a, root0 + t, DONE);
+    }
+  }
+  __syncthreads();
+  const uint32_t qn = wq_n_;
+  for (uint32_t t = wq_pop(wq_, &wq_h_, qn, lane); t != ~0u; t = wq_pop(wq_, &wq_h_, qn, lane))
+    warp1_task(a, t, lane, lab32[t * 32u + lane], wi);
+}
+__global__ void __launch_bounds__(WB_THREADS, B2D_WB2_MINB)
+    forest_warp2_kernel(ForestArgs a0, uint32_t ntasks, uint32_t queue) {
+  griddep_enter();
+  B2D_WARP_QUEUE_BUFFERS
+  const ForestArgs a = with_round(a0);
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t G = (gridDim.x * WB_THREADS) >> 5;
+  const uint32_t w0 = (blockIdx.x * WB_THREADS + threadIdx.x) >> 5;
+  const uint4* lab128 = reinterpret_cast<const uint4*>(a.leaflab);
+  if (!queue) {
+    uint4 w = w0 < ntasks ? lab128[w0 * 32u + lane] : make_uint4(0, 0, 0, 0);
+    for (uint32_t task = w0; task < ntasks; task += G) {
+      const uint32_t next = task + G;
+      const uint4 wn = next < ntasks ? lab128[next * 32u + lane] : make_uint4(0, 0, 0, 0);
+      warp2_task(a, task, lane, w);
+      w = wn;
+    }
+    return;
+  }
+  const uint64_t root0 = (1ull << (a.D - WB2_LEVELS)) - 1ull;
+  const uint4 fixed4 = make_uint4(0x01010101u, 0x01010101u, 0x01010101u, 0x01010101u);
+  uint4 wn[WB_SCAN];
+#pragma unroll
+  for (uint32_t k = 0; k < WB_SCAN; k++) {
+    const uint32_t t = w0 + k * G;
+    wn[k] = t < ntasks ? lab128[t * 32u + lane] : fixed4;
+  }
+  for (uint32_t t0 = w0; t0 < ntasks; t0 += WB_SCAN * G) {
+    uint32_t work = 0;   // bit k: task t0 + kG has a leaf that is not FIXED (every task of a baseline)
+#pragma unroll
+    for (uint32_t k = 0; k < WB_SCAN; k++) {
+      const bool fast = !a.baseline && wn[k].x == 0x01010101u && wn[k].y == 0x01010101u &&
+                        wn[k].z == 0x01010101u && wn[k].w == 0x01010101u;
+      if (!__all_sync(WB_FULL, fast)) work |= 1u << k;
+    }
+#pragma unroll
+    for (uint32_t k = 0; k < WB_SCAN; k++) {
+      const uint32_t t = t0 + (WB_SCAN + k) * G;
+      wn[k] = t < ntasks ? lab128[t * 32u + lane] : fixed4;
+    }
+#pragma unroll
+    for (uint32_t k = 0; k < WB_SCAN; k++) {
+      const uint32_t t = t0 + k * G;
+      if (t >= ntasks) break;
+      if ((work >> k) & 1u) wq_push(wq_, &wq_n_, t, lane);
+      else if (lane == 0) band_output<2>(a, root0 + t, FIXED_DUPL);
+    }
+  }
+  __syncthreads();
+  const uint32_t qn = wq_n_;
+  for (uint32_t t = wq_pop(wq_, &wq_h_, qn, lane); t != ~0u; t = wq_pop(wq_, &wq_h_, qn, lane))
+    warp2_task(a, t, lane, lab128[t * 32u + lane]);
 }
 
 // Segmented warp bands (batched form): CTA b of a handle's range holds its tasks 8b .. 8b+7,
@@ -761,8 +904,9 @@ static void forest_steps_from(uint32_t D, uint32_t in, uint64_t N, int phase, st
 void forest_steps(uint32_t D, uint64_t N, int phase, std::vector<ForestStep>& out) {
   forest_steps_from(D, D, N, phase, out);
 }
-void forest_steps_batch(uint32_t n, uint32_t D, uint64_t N, int phase, std::vector<ForestStep>& out) {
-  if (!warp_bands(n, D, phase)) {
+void forest_steps_batch(uint32_t n, uint32_t D, uint64_t N, int phase, std::vector<ForestStep>& out,
+                        int warp_mask) {
+  if (!warp_bands(n, D, phase, warp_mask)) {
     forest_steps(D, N, phase, out);
     return;
   }
@@ -785,11 +929,11 @@ static uint32_t resident_ctas(K kernel) {
   return (uint32_t)nb;
 }
 
-cudaError_t launch_forest(const ForestArgs& a, int phase, cudaStream_t stream, int sm_count) {
+cudaError_t launch_forest(const ForestArgs& a, int phase, cudaStream_t stream, int sm_count, int warp_mask) {
   static const uint32_t res_first = resident_ctas(forest_first_kernel);
   static const uint32_t res_fast = resident_ctas(forest_fast_kernel<2>);
   std::vector<ForestStep> steps;
-  if (warp_bands(a.n, a.D, phase)) {
+  if (warp_bands(a.n, a.D, phase, warp_mask)) {
     static const uint32_t res_w1 = resident_ctas(forest_warp1_kernel);
     static const uint32_t res_w2 = resident_ctas(forest_warp2_kernel);
     const uint32_t levels = phase == 1 ? WB1_LEVELS : WB2_LEVELS;
@@ -797,8 +941,9 @@ cudaError_t launch_forest(const ForestArgs& a, int phase, cudaStream_t stream, i
     const uint32_t want = (ntasks + WB_THREADS / 32u - 1u) / (WB_THREADS / 32u);
     const uint32_t cap = (phase == 1 ? res_w1 : res_w2) * (uint32_t)(sm_count > 0 ? sm_count : 1);
     const uint32_t grid = want < cap ? want : cap;
-    cudaError_t e = phase == 1 ? launch_dependent(forest_warp1_kernel, grid, WB_THREADS, 0, stream, a, ntasks)
-                               : launch_dependent(forest_warp2_kernel, grid, WB_THREADS, 0, stream, a, ntasks);
+    const uint32_t queue = wq_fits(ntasks, grid) ? 1u : 0u;
+    cudaError_t e = phase == 1 ? launch_dependent(forest_warp1_kernel, grid, WB_THREADS, 0, stream, a, ntasks, queue)
+                               : launch_dependent(forest_warp2_kernel, grid, WB_THREADS, 0, stream, a, ntasks, queue);
     if (e != cudaSuccess) return e;
     forest_steps_from(a.D, a.D - levels, a.N, phase, steps);
   } else {
@@ -821,9 +966,9 @@ cudaError_t launch_forest(const ForestArgs& a, int phase, cudaStream_t stream, i
   return cudaSuccess;
 }
 
-int forest_launch_count(uint32_t n, uint32_t D, int phase) {
+int forest_launch_count(uint32_t n, uint32_t D, int phase, int warp_mask) {
   std::vector<ForestStep> steps;
-  if (warp_bands(n, D, phase)) {
+  if (warp_bands(n, D, phase, warp_mask)) {
     forest_steps_from(D, D - (phase == 1 ? WB1_LEVELS : WB2_LEVELS), 2, phase, steps);
     return 1 + (int)steps.size();
   }

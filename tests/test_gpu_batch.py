@@ -127,13 +127,16 @@ def test_batch_autotune_keeps_output(cuda):
     """the tuner measures one setting per incremental round; output never changes"""
     specs = SPECS[:3] + SPECS[5:7]
     with CheckpointBatch(autotune=True) as b:
-        # one baseline round (not scored), five scored incremental rounds, then the result
-        rounds = 8
+        # one baseline round (not scored), seven scored incremental rounds (one of them resizes
+        # every map for the load-factor knob), then the result
+        rounds = 9
         baselines = [[True] * len(specs)] + [[False] * len(specs) for _ in range(rounds - 1)]
         got, _, _ = run_batch(specs, rounds, baselines, b)
         assert b.get_param("tuned") == 1
-        for k in ("shared", "leaf_stages", "leaf_ctas_per_sm", "tiles_per_pop", "streams"):
+        for k in ("shared", "leaf_stages", "leaf_ctas_per_sm", "tiles_per_pop", "streams", "warp_bands",
+                  "map_headroom_pct"):
             b.get_param(k)
+        assert b.get_param("warp_bands") in (0, 3) and b.get_param("map_headroom_pct") in (125, 150)
     want = diffs_alone(specs, rounds, baselines)
     assert got == want
 
