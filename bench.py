@@ -87,8 +87,14 @@ def parse():
     p.add_argument("--map-reserve", type=float, default=20e9,
                    help="device bytes kept mapped for digest-map growth after the warm-up (all forms)")
     p.add_argument("--hbm-budget", type=float, default=150e9, help="served form: device bytes for client state")
+    p.add_argument("--map-headroom", type=int, default=None,
+                   help="plain form: digest-map size at the baseline over its minimum, percent (default: 400 for "
+                        "md5_f32_8g, whose series adds about 0.3 N entries per checkpoint, so the baseline's table "
+                        "holds all 20 checkpoints; the library default 150 otherwise)")
     a = p.parse_args()
     md5 = a.workload == "md5_f32_8g"
+    if a.map_headroom is None:
+        a.map_headroom = 400 if md5 else 0
     if a.chunk_size is None:
         a.chunk_size = 256 if md5 else 128
     if a.nbytes is None:
@@ -609,6 +615,8 @@ def main():
         dd.set_param("leaf_unit", args.leaf_unit)
     if args.graph is not None:
         dd.set_param("graph", args.graph)
+    if args.map_headroom:
+        dd.set_param("map_headroom_pct", args.map_headroom)
     dd.checkpoint_device(series.next(), make_baseline=True)          # checkpoint 0: baseline
     for _ in range(args.warmup):
         dd.checkpoint_device(series.next())
@@ -766,7 +774,8 @@ def main():
         "config": {"workload": args.workload, "nbytes": nbytes, "chunk_size": cs, "hash": "md5" if md5 else "murmur3",
                    "approach": args.approach, "checkpoints": 1 + args.warmup + args.steps,
                    "timed_groups": f"{len(group_ms)} (inputs of a group resident in HBM before it is timed)",
-                   "map_growth": {"reserved_bytes": int(args.map_reserve), "grows_in_timed_steps": grows_timed},
+                   "map_growth": {"reserved_bytes": int(args.map_reserve), "grows_in_timed_steps": grows_timed,
+                                  "baseline_headroom_pct": args.map_headroom or 150},
                    "l2": (f"inputs {nbytes / 2**30:.2f} GiB > L2, no flush" if nbytes >= (256 << 20) else
                           "L2 flushed (512 MiB write) before each step, outside the timed spans"),
                    "parallelism": f"replicas x{world}"},

@@ -172,6 +172,12 @@ __device__ __forceinline__ uint32_t swz(uint32_t o) {
   else return o;
 }
 
+// MD5 data blocks with part of each step on the multiply-add pipe (md5_compress_t); 0: all of
+// it on the integer ALU
+#ifndef B2D_MD5_SPLIT
+#define B2D_MD5_SPLIT 1
+#endif
+
 // fold the U-byte segment of row `row` of a staged tile into a lane's running digest state
 template <int U, int KIND>
 __device__ __forceinline__ void hash_segment(const uint8_t* stage, uint32_t row, Murmur3& mm, uint32_t md[4]) {
@@ -185,7 +191,7 @@ __device__ __forceinline__ void hash_segment(const uint8_t* stage, uint32_t row,
         const uint4 v = *reinterpret_cast<const uint4*>(stage + swz<U>(base + blk * 64u + 16u * j));
         m[4 * j + 0] = v.x; m[4 * j + 1] = v.y; m[4 * j + 2] = v.z; m[4 * j + 3] = v.w;
       }
-      md5_compress(md, m);
+      md5_compress_t<B2D_MD5_SPLIT>(md, m);
     }
   } else {
 #pragma unroll

@@ -124,12 +124,14 @@ __device__ __forceinline__ void count_insert(unsigned long long* size) {
   if (lane == (unsigned)(__ffs(am) - 1)) atomicAdd(size, (unsigned long long)__popc(am));
 }
 
+__device__ __forceinline__ MapRef map_probe_from(const MapView& m, const Key128& k, unsigned long long val,
+                                                 uint64_t i, uint64_t probe, DevStatus* st);
+
 // Insert-if-absent of an already packed value (map_pack).  On success the value is merged
 // with atomicMin.  On an existing key nothing is written here; the caller decides (through
 // map_merge_current) whether the entry belongs to the current checkpoint.
-__device__ __forceinline__ MapRef map_insert_packed(const MapView& m, const Digest& d, unsigned long long val,
-                                                    DevStatus* st) {
-  const Key128 k = digest_key(d);
+__device__ __forceinline__ MapRef map_insert_key(const MapView& m, const Key128& k, unsigned long long val,
+                                                 DevStatus* st) {
   MapRef r{0, false, false, ~0ull};
   if (key_is_empty_pattern(k)) {
     // the extra slot: the first value merged into it inserts the key
@@ -146,10 +148,21 @@ __device__ __forceinline__ MapRef map_insert_packed(const MapView& m, const Dige
   // in one round trip): measured slower, the hashing kernel 0.861 against 0.829 ms and the
   // forest 0.238 against 0.210 ms per 4 GiB step, as atomics on slots that hold other keys or
   // this key cost more than the reads they replace.
+  return map_probe_from(m, k, val, map_home(k, m.cap), 0, st);
+}
+__device__ __forceinline__ MapRef map_insert_packed(const MapView& m, const Digest& d, unsigned long long val,
+                                                    DevStatus* st) {
+  return map_insert_key(m, digest_key(d), val, st);
+}
+
+// The probe loop of an insert from slot i, `probe` slots after the key's home (those hold other
+// keys).  The key is not the EMPTY pattern.
+__device__ __forceinline__ MapRef map_probe_from(const MapView& m, const Key128& k, unsigned long long val,
+                                                 uint64_t i, uint64_t probe, DevStatus* st) {
+  MapRef r{0, false, false, ~0ull};
   const bool cas_only = B2D_MAP_CAS_FIRST || (k.lo == MAP_EMPTY) || (k.hi == MAP_EMPTY);
   const Key128 empty{MAP_EMPTY, MAP_EMPTY};
-  uint64_t i = map_home(k, m.cap);
-  for (uint64_t probe = 0; probe < m.cap; probe++) {
+  for (; probe < m.cap; probe++) {
     Key128* s = map_key(m, i);
     bool try_cas = true;
     if (!cas_only) {
@@ -180,6 +193,77 @@ __device__ __forceinline__ MapRef map_insert_packed(const MapView& m, const Dige
   }
   set_error(st, DERR_MAP_FULL, 0);
   return r;
+}
+
+// Up to G inserts of one thread at once, with the results of G calls of map_insert_packed.  The
+// home slots of all keys are read before any is examined and the claims of all empty homes are
+// issued before any result is used, so the thread waits for about one DRAM read and one atomic
+// round trip for the group instead of one of each per key.  Keys whose home holds another key
+// (rare below the load limit) and keys with an all-ones half continue one at a time.
+template <int G>
+__device__ __forceinline__ void map_insert_group(const MapView& m, const Key128 (&k)[G],
+                                                 const unsigned long long (&val)[G], uint32_t cnt, MapRef (&r)[G],
+                                                 DevStatus* st) {
+  const Key128 empty{MAP_EMPTY, MAP_EMPTY};
+  uint64_t home[G];
+  unsigned long long lo[G], hi[G];
+#pragma unroll
+  for (int j = 0; j < G; j++) {
+    r[j] = MapRef{0, false, false, ~0ull};
+    if ((uint32_t)j < cnt) {
+      home[j] = map_home(k[j], m.cap);
+      const Key128* s = map_key(m, home[j]);
+      lo[j] = *reinterpret_cast<const volatile unsigned long long*>(&s->lo);
+      hi[j] = *reinterpret_cast<const volatile unsigned long long*>(&s->hi);
+    }
+  }
+  uint32_t cas = 0, slow = 0, ins = 0;
+#pragma unroll
+  for (int j = 0; j < G; j++) {
+    if ((uint32_t)j >= cnt) continue;
+    if (B2D_MAP_CAS_FIRST || k[j].lo == MAP_EMPTY || k[j].hi == MAP_EMPTY) {
+      slow |= 1u << j;   // the one-at-a-time path from the home slot
+      home[j] = ~0ull;
+    } else if (lo[j] == k[j].lo && hi[j] == k[j].hi) {
+      r[j].slot = home[j];
+      r[j].found = true;
+    } else if (lo[j] == MAP_EMPTY || hi[j] == MAP_EMPTY) {
+      cas |= 1u << j;
+    } else {
+      slow |= 1u << j;
+    }
+  }
+  Key128 old[G];
+#pragma unroll
+  for (int j = 0; j < G; j++)
+    if ((cas >> j) & 1u) old[j] = atomicCAS(map_key(m, home[j]), empty, k[j]);
+#pragma unroll
+  for (int j = 0; j < G; j++) {
+    if (!((cas >> j) & 1u)) continue;
+    if (old[j].lo == MAP_EMPTY && old[j].hi == MAP_EMPTY) {
+      ins |= 1u << j;
+      r[j].slot = home[j];
+      r[j].found = r[j].inserted = true;
+    } else if (old[j].lo == k[j].lo && old[j].hi == k[j].hi) {
+      r[j].slot = home[j];
+      r[j].found = true;
+    } else {
+      slow |= 1u << j;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < G; j++)
+    if ((ins >> j) & 1u) r[j].prev = atomicMin(map_val(m, home[j]), val[j]);
+  if (ins) {
+    const unsigned am = __activemask();
+    const uint32_t c = __reduce_add_sync(am, (uint32_t)__popc(ins));
+    if ((threadIdx.x & 31u) == (unsigned)(__ffs(am) - 1)) atomicAdd(m.size, (unsigned long long)c);
+  }
+#pragma unroll
+  for (int j = 0; j < G; j++)
+    if ((slow >> j) & 1u)
+      r[j] = home[j] == ~0ull ? map_insert_key(m, k[j], val[j], st)
+                              : map_probe_from(m, k[j], val[j], map_next(home[j], m.cap), 1, st);
 }
 
 // insert with `val` = priority << 32 | node, stored for checkpoint `cur`
