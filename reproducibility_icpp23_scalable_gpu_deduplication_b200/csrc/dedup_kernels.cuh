@@ -247,13 +247,13 @@ struct SegGrid {
   const uint32_t* bcap;   // per handle: bucket capacity of its scratch
   uint32_t n;
 };
-// grid sizes of one handle's diff assembly; variant = data-gather kernel (0..5: 16-byte copies
-// with 32/16/8/4/2/1 lanes per chunk, 6: byte copies)
+// grid sizes of one handle's diff assembly; variant = data-gather kernel (0: 16-byte
+// copies, 1: byte copies)
 struct DiffGrids {
   uint32_t g, gs, gl, gp, gg;
   int variant;
 };
-constexpr int GATHER_VARIANTS = 7;
+constexpr int GATHER_VARIANTS = 2;
 DiffGrids diff_grids(const DiffArgs& a, int sm_count);
 struct DiffBatch {
   SegGrid base;                     // beg unused

@@ -18,11 +18,6 @@
 
 namespace b2d {
 
-// chunk groups each lane keeps in flight in the data gather
-#ifndef B2D_GATHER_UNROLL
-#define B2D_GATHER_UNROLL 4
-#endif
-
 constexpr uint32_t COMPACT_THREADS = 512;
 
 // Every kernel below is a body over a virtual grid (bid of nb CTAs) with two launchers: one
@@ -505,12 +500,20 @@ __device__ __forceinline__ uint32_t find_region(const uint32_t* off, uint32_t F,
   return lo;
 }
 
-// Data section: each warp owns a contiguous range of diff chunks.  The chunks of one region are
-// contiguous in both the buffer and the diff, so the warp finds the region of its first chunk
-// once and then walks forward; LPC lanes copy one chunk with 16-byte vectors (chunk size a
-// multiple of 16, both sides 16-byte aligned); the short last chunk is zero-padded (:643-645).
-template <uint32_t LPC>
+// Data section.  Each warp owns a contiguous range [k0, k1) of diff chunks (the same share for
+// every warp) and copies it with 16-byte vectors, lane after lane over consecutive 16-byte units
+// of the range, GATHER_UNROLL units per lane in flight (chunk size a multiple of 16, both sides
+// 16-byte aligned), whatever the region boundaries: many regions are a few chunks long.  A unit's
+// source follows from its chunk's region (start in the diff, root node).  The starts and roots
+// of 32 regions at a time are held one per lane, and each unit finds its region among them by a
+// five-step shuffle search, so no load waits on another: looked up in memory, each group of
+// chunks waited for two dependent loads before its data load could issue.  The short last chunk
+// is zero-padded (:643-645).
+#ifndef B2D_GATHER_UNROLL
+#define B2D_GATHER_UNROLL 4
+#endif
 __device__ __forceinline__ void gather_vec_body(const DiffArgs& a, uint32_t bid, uint32_t nb) {
+  constexpr uint32_t U = B2D_GATHER_UNROLL;
   const DevMeta m = *a.meta;
   uint8_t* dst_base = a.diff + m.data_off;
   uint32_t* first_meta = reinterpret_cast<uint32_t*>(a.diff + m.first_off);
@@ -518,91 +521,79 @@ __device__ __forceinline__ void gather_vec_body(const DiffArgs& a, uint32_t bid,
   const uint64_t nthr = (uint64_t)nb * blockDim.x;
   for (uint64_t i = gtid; i < m.F; i += nthr) first_meta[i] = a.first_list[i] - a.id_bias;
   if (m.T == 0) return;
-  constexpr uint32_t CPW = 32u / LPC;   // chunks per warp iteration
   const uint32_t lane = threadIdx.x & 31u;
   const uint64_t warp = gtid >> 5, nwarps = nthr >> 5;
   uint64_t k0, k1;
   cta_range(m.T, (uint32_t)warp, (uint32_t)nwarps, k0, k1);
   if (k0 >= k1) return;
-  const uint32_t units = a.cs / 16u;
-  uint32_t r = find_region(a.region_off, m.F, k0);
-  if (units == LPC) {
-    // one 16-byte unit per lane per chunk: GATHER_UNROLL chunk groups per iteration, loads
-    // first then stores, so each lane keeps several loads in flight (large diffs, baselines)
-    constexpr uint32_t U = B2D_GATHER_UNROLL;
-    const uint32_t sub = lane % LPC;
-    for (; k0 + (uint64_t)CPW * U <= k1; k0 += (uint64_t)CPW * U) {
-      uint4 val[U];
-      uint4* dst[U];
-      bool full[U];
-      uint32_t rr = r;
+  const uint64_t T = m.T;
+  const uint32_t F = m.F;
+  const uint32_t units = a.cs / 16u;   // 16-byte units per chunk
+  const bool pow2 = (units & (units - 1u)) == 0u;
+  const uint32_t ush = __ffs(units) - 1u;
+  const uint64_t last = a.n - 1ull;
+  const bool short_last = (a.len % a.cs) != 0;
+  const uint4* src = reinterpret_cast<const uint4*>(a.data);
+  uint4* dst = reinterpret_cast<uint4*>(dst_base);
+  // largest r with region_off[r] <= k0 (region_off[0] = 0)
+  uint32_t r = warp_lower_bound(a.region_off, F, k0 + 1u) - 1u;
+  uint64_t k = k0;
+  while (k < k1) {
+    // regions r .. r + 31, one per lane; chunks before `bend` lie in them
+    const uint32_t rl = r + lane;
+    const uint32_t off_l = rl < F ? a.region_off[rl] : (uint32_t)T;
+    const uint32_t node_l = rl < F ? a.first_list[rl] : 0u;
+    const uint64_t bend = r + 32u < F ? a.region_off[r + 32u] : T;
+    const uint64_t kend = bend < k1 ? bend : k1;
+    const uint64_t u_end = kend * units;
+    for (uint64_t base = k * units; base < u_end; base += 32ull * U) {
+      uint4 v[U];
+      uint32_t st = 0;   // bit i: unit i is this lane's to copy
 #pragma unroll
-      for (uint32_t u = 0; u < U; u++) {
-        const uint64_t kk = k0 + (uint64_t)u * CPW + lane / LPC;
-        while (rr + 1u < m.F && a.region_off[rr + 1u] <= kk) rr++;
-        const uint64_t chunk = (uint64_t)(leftmost_leaf(a.first_list[rr], a.N) - (a.n - 1u)) + (kk - a.region_off[rr]);
-        full[u] = chunk < a.n - 1u;   // the last chunk (maybe short) goes through the general path
-        dst[u] = reinterpret_cast<uint4*>(dst_base + kk * a.cs) + sub;
-        if (full[u]) val[u] = __ldg(reinterpret_cast<const uint4*>(a.data + chunk * a.cs) + sub);
-      }
-      bool all_full = true;
+      for (uint32_t i = 0; i < U; i++) {
+        const uint64_t g = base + lane + 32ull * i;
+        const bool act = g < u_end;
+        const uint64_t kk = act ? (pow2 ? g >> ush : g / units) : k;
+        uint32_t j = 0;   // largest j with region start j <= kk
 #pragma unroll
-      for (uint32_t u = 0; u < U; u++) {
-        if (full[u]) *dst[u] = val[u];
-        all_full = all_full && full[u];
-      }
-      const uint32_t r_next = __reduce_max_sync(0xffffffffu, rr);
-      if (!__all_sync(0xffffffffu, all_full)) break;   // the general loop redoes this group from r
-      r = r_next;
-    }
-  }
-  for (uint64_t k = k0; k < k1; k += CPW) {
-    const uint64_t kk = k + lane / LPC;
-    const uint32_t sub = lane % LPC;
-    uint32_t rr = r;
-    while (rr + 1u < m.F && a.region_off[rr + 1u] <= kk) rr++;
-    if (kk < k1) {
-      const uint32_t node = a.first_list[rr];
-      const uint64_t chunk = (uint64_t)(leftmost_leaf(node, a.N) - (a.n - 1u)) + (kk - a.region_off[rr]);
-      if (chunk >= a.n) {
-        set_error(a.st, DERR_INTERNAL, 40);
-      } else {
-        const uint64_t src_off = chunk * a.cs;
-        const uint4* src = reinterpret_cast<const uint4*>(a.data + src_off);
-        uint4* dst = reinterpret_cast<uint4*>(dst_base + kk * a.cs);
-        const uint64_t avail = (chunk == a.n - 1u) ? a.len - src_off : a.cs;
-        if (avail == a.cs) {
-          for (uint32_t u = sub; u < units; u += LPC) dst[u] = __ldg(src + u);
+        for (uint32_t step = 16; step >= 1; step >>= 1) {
+          const uint32_t o = __shfl_sync(0xffffffffu, off_l, j + step);
+          if (o <= kk) j += step;
+        }
+        const uint32_t off = __shfl_sync(0xffffffffu, off_l, j);
+        const uint32_t node = __shfl_sync(0xffffffffu, node_l, j);
+        if (!act) continue;
+        const uint64_t chunk = (uint64_t)(leftmost_leaf(node, a.N) - (a.n - 1u)) + (kk - off);
+        const uint64_t su = chunk * units + (g - kk * units);
+        if (chunk > last) {
+          set_error(a.st, DERR_INTERNAL, 40);
+        } else if (short_last && chunk == last) {   // bytes past the buffer's end are zero
+          uint8_t tmp[16];
+          for (uint32_t b = 0; b < 16; b++) tmp[b] = 16ull * su + b < a.len ? a.data[16ull * su + b] : 0u;
+          uint4 w;
+          memcpy(&w, tmp, 16);
+          dst[g] = w;
         } else {
-          const uint32_t full = (uint32_t)(avail / 16u);
-          for (uint32_t u = sub; u < units; u += LPC) {
-            if (u < full) {
-              dst[u] = __ldg(src + u);
-            } else {
-              uint8_t tmp[16];
-              const uint8_t* s8 = a.data + src_off + 16ull * u;
-              for (uint32_t b = 0; b < 16; b++) tmp[b] = (16ull * u + b < avail) ? s8[b] : 0u;
-              uint4 v;
-              memcpy(&v, tmp, 16);
-              dst[u] = v;
-            }
-          }
+          st |= 1u << i;
+          v[i] = __ldg(src + su);
         }
       }
+#pragma unroll
+      for (uint32_t i = 0; i < U; i++)
+        if ((st >> i) & 1u) dst[base + lane + 32ull * i] = v[i];
     }
-    r = __reduce_max_sync(0xffffffffu, rr);
+    k = kend;
+    r += 32u;
   }
 }
-template <uint32_t LPC>
 __global__ void __launch_bounds__(256) gather_vec_kernel(DiffArgs a0) {
   griddep_enter();
-  gather_vec_body<LPC>(with_round(a0), blockIdx.x, gridDim.x);
+  gather_vec_body(with_round(a0), blockIdx.x, gridDim.x);
 }
-template <uint32_t LPC>
 __global__ void __launch_bounds__(256) gather_vec_seg(SegGrid s) {
   uint32_t bid, nb;
   const uint32_t h = seg_locate(s, bid, nb);
-  gather_vec_body<LPC>(with_round(s.args[h]), bid, nb);
+  gather_vec_body(with_round(s.args[h]), bid, nb);
 }
 
 // any chunk size / alignment: one thread per chunk, byte copies
@@ -656,8 +647,7 @@ DiffGrids diff_grids(const DiffArgs& a, int sm_count) {
   r.gg = grid_for((uint64_t)a.n * a.cs, 32768, (uint32_t)sm_count * 4u);
   const bool vec = (a.cs % 16u == 0) && ((reinterpret_cast<uintptr_t>(a.data) & 15u) == 0) &&
                    ((reinterpret_cast<uintptr_t>(a.diff) & 15u) == 0);
-  const uint32_t units = a.cs / 16u;
-  r.variant = !vec ? 6 : units >= 32 ? 0 : units >= 16 ? 1 : units >= 8 ? 2 : units >= 4 ? 3 : units >= 2 ? 4 : 5;
+  r.variant = vec ? 0 : 1;
   return r;
 }
 
@@ -680,15 +670,8 @@ cudaError_t launch_collect_diff_batch(const DiffBatch& b, cudaStream_t stream, u
   for (int v = 0; v < GATHER_VARIANTS; v++) {
     if (!b.tot_gather[v]) continue;
     s.beg = b.beg_gather[v];
-    switch (v) {
-      case 0: gather_vec_seg<32><<<b.tot_gather[v], 256, 0, stream>>>(s); break;
-      case 1: gather_vec_seg<16><<<b.tot_gather[v], 256, 0, stream>>>(s); break;
-      case 2: gather_vec_seg<8><<<b.tot_gather[v], 256, 0, stream>>>(s); break;
-      case 3: gather_vec_seg<4><<<b.tot_gather[v], 256, 0, stream>>>(s); break;
-      case 4: gather_vec_seg<2><<<b.tot_gather[v], 256, 0, stream>>>(s); break;
-      case 5: gather_vec_seg<1><<<b.tot_gather[v], 256, 0, stream>>>(s); break;
-      default: gather_bytes_seg<<<b.tot_gather[v], 256, 0, stream>>>(s); break;
-    }
+    if (v == 0) gather_vec_seg<<<b.tot_gather[v], 256, 0, stream>>>(s);
+    else gather_bytes_seg<<<b.tot_gather[v], 256, 0, stream>>>(s);
     c++;
   }
   if (launches) *launches = c;
@@ -728,13 +711,7 @@ cudaError_t launch_collect_diff(const DiffArgs& args, uint32_t bcap, int sm_coun
   const bool vec = (a.cs % 16u == 0) && ((reinterpret_cast<uintptr_t>(a.data) & 15u) == 0) &&
                    ((reinterpret_cast<uintptr_t>(a.diff) & 15u) == 0);
   if (vec) {
-    const uint32_t units = a.cs / 16u;
-    if (units >= 32) { B2D_LD(gather_vec_kernel<32>, gblocks, 256, 0, stream, a) }
-    else if (units >= 16) { B2D_LD(gather_vec_kernel<16>, gblocks, 256, 0, stream, a) }
-    else if (units >= 8) { B2D_LD(gather_vec_kernel<8>, gblocks, 256, 0, stream, a) }
-    else if (units >= 4) { B2D_LD(gather_vec_kernel<4>, gblocks, 256, 0, stream, a) }
-    else if (units >= 2) { B2D_LD(gather_vec_kernel<2>, gblocks, 256, 0, stream, a) }
-    else { B2D_LD(gather_vec_kernel<1>, gblocks, 256, 0, stream, a) }
+    B2D_LD(gather_vec_kernel, gblocks, 256, 0, stream, a)
   } else {
     B2D_LD(gather_bytes_kernel, gblocks, 256, 0, stream, a)
   }
