@@ -56,6 +56,103 @@ __device__ __forceinline__ void leaf_finish(const LeafArgs& a, uint32_t chunk, c
   a.leaflab[chunk] = label;
 }
 
+// Map insert of a lane's changed chunk spread over the lane's next tiles (B2D_LEAF_PIPE 1): the
+// read of the digest's home slot is issued once the chunk is hashed and examined after the next
+// tile is hashed (a claim, if the slot is empty, then costs an atomic round trip on a line already
+// in L2); the owner update's old value, which only the shared-digest flags need, is examined one
+// tile later still.  Inserting where the chunk is hashed, a lane with many changed chunks (30 % on
+// the MD5 series, 10 % on the batched workload) waited a DRAM read and two atomic round trips per
+// changed chunk with its hashing stopped.  (Issuing the claim itself ahead, as a CAS whose old
+// value tells an empty slot, this key and another apart, was much slower: the MD5 series' moved
+// zero pages all share one digest, and their claims serialise on its slot, where reads do not.)
+// Labels, digests, map contents and flags are those of leaf_finish: the map merges values by
+// atomicMin and tells a checkpoint's own entries from older ones by their checkpoint field,
+// whatever the order of the inserts.
+#ifndef B2D_LEAF_PIPE
+#define B2D_LEAF_PIPE 1
+#endif
+struct LeafPipe {
+  bool c_on, c_fixed, m_on;   // an insert in flight (and its FIXED test); an owner update in flight
+  uint32_t c_chunk, m_chunk;
+  Digest c_d;
+  uint64_t c_home;
+  unsigned long long c_lo, c_hi;   // the home slot's key as read
+  unsigned long long m_prev;
+};
+__device__ __forceinline__ void pipe_init(LeafPipe& p) { p.c_on = p.c_fixed = p.m_on = false; }
+// the owner update issued a tile ago: flag shared digests
+__device__ __forceinline__ void pipe_flags(const LeafArgs& a, LeafPipe& p) {
+  if (p.m_on) flag_shared(a, p.m_chunk, p.m_prev);
+  p.m_on = false;
+}
+// the insert whose home slot was read a tile ago: claim, label, tree digest, owner update
+__device__ __forceinline__ void pipe_claim(const LeafArgs& a, LeafPipe& p) {
+  if (!p.c_on) return;
+  p.c_on = false;
+  const uint32_t chunk = p.c_chunk, leaf = a.n - 1u + chunk;
+  const unsigned long long val = map_pack((unsigned long long)leaf, a.cur);
+  const Key128 k = digest_key(p.c_d);
+  MapRef r{p.c_home, true, false, ~0ull};
+  bool next = false;   // the home slot holds another key: probe on
+  if (p.c_lo != k.lo || p.c_hi != k.hi) {
+    if (p.c_lo == MAP_EMPTY || p.c_hi == MAP_EMPTY) {   // empty or being claimed: resolved by the CAS
+      const Key128 old = atomicCAS(map_key(a.map, p.c_home), Key128{MAP_EMPTY, MAP_EMPTY}, k);
+      if (old.lo == MAP_EMPTY && old.hi == MAP_EMPTY) r.inserted = true;
+      else next = old.lo != k.lo || old.hi != k.hi;
+    } else {
+      next = true;
+    }
+  }
+  if (next) r = map_probe_from(a.map, k, val, map_next(p.c_home, a.map.cap), 1, a.st);
+  uint8_t label = DONE;
+  if (r.inserted && !next) {   // claimed the home slot: the owner update's old value is read later
+    p.m_prev = atomicMin(map_val(a.map, p.c_home), val);
+    count_insert(a.map.size);
+    label = FIRST_OCUR;
+    p.m_on = !p.c_fixed;
+    p.m_chunk = chunk;
+  } else {
+    unsigned long long prev = ~0ull;
+    if (r.inserted) {
+      label = FIRST_OCUR;
+      prev = r.prev;
+    } else if (r.found) {
+      label = map_merge_current(a.map, r.slot, leaf, a.cur, &prev) ? FIRST_OCUR : SHIFT_DUPL;
+    }
+    if (label == FIRST_OCUR && !p.c_fixed) flag_shared(a, chunk, prev);
+  }
+  if (r.found || p.c_fixed) a.tree[leaf] = p.c_d;   // the baseline keeps a FIXED (zero) digest too
+  a.leaflab[chunk] = p.c_fixed ? FIXED_DUPL : label;
+}
+// a hashed chunk: FIXED at once, else the read of its home slot is issued (keys with an all-ones
+// half, which a read cannot tell from a slot being claimed, take leaf_finish)
+__device__ __forceinline__ void pipe_issue(const LeafArgs& a, LeafPipe& p, uint32_t chunk, const Digest& d,
+                                           const Digest& old) {
+  const bool fixed = a.baseline ? digest_zero(d) : digest_eq(d, old);
+  if (fixed && !a.baseline) {
+    a.leaflab[chunk] = FIXED_DUPL;
+    return;
+  }
+  const Key128 k = digest_key(d);
+  if (k.lo == MAP_EMPTY || k.hi == MAP_EMPTY) {
+    leaf_finish(a, chunk, d, old);
+    return;
+  }
+  p.c_on = true;
+  p.c_fixed = fixed;
+  p.c_chunk = chunk;
+  p.c_d = d;
+  p.c_home = map_home(k, a.map.cap);
+  const Key128* slot = map_key(a.map, p.c_home);
+  p.c_lo = *reinterpret_cast<const volatile unsigned long long*>(&slot->lo);
+  p.c_hi = *reinterpret_cast<const volatile unsigned long long*>(&slot->hi);
+}
+__device__ __forceinline__ void pipe_drain(const LeafArgs& a, LeafPipe& p) {
+  pipe_flags(a, p);
+  pipe_claim(a, p);
+  pipe_flags(a, p);
+}
+
 // prior digest of a leaf (the incremental FIXED test); the baseline compares against zero
 __device__ __forceinline__ Digest prior_digest(const LeafArgs& a, uint64_t chunk) {
   Digest z;
@@ -273,6 +370,11 @@ __global__ void __launch_bounds__((TMA_CONSUMER_WARPS + 1) * 32)
   }
 
   // ---------------- consumer warps: lane = chunk row of the tile
+  // MD5's hashing of a tile is long enough to hide an insert; Murmur3's is not, and its registers
+  // are better spent on the loads in flight
+  constexpr bool PIPE = B2D_LEAF_PIPE && KIND == HASH_MD5;
+  LeafPipe pipe;
+  pipe_init(pipe);
   uint32_t k = 0;
   const uint32_t row = warp * 32u + lane;
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -294,8 +396,15 @@ __global__ void __launch_bounds__((TMA_CONSUMER_WARPS + 1) * 32)
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
     }
-    if (valid) leaf_finish(a, chunk, finish_segments<KIND>(mm, md, a.cs), old);
+    if (PIPE) {
+      pipe_flags(a, pipe);
+      pipe_claim(a, pipe);
+      if (valid) pipe_issue(a, pipe, chunk, finish_segments<KIND>(mm, md, a.cs), old);
+    } else if (valid) {
+      leaf_finish(a, chunk, finish_segments<KIND>(mm, md, a.cs), old);
+    }
   }
+  if (PIPE) pipe_drain(a, pipe);
 }
 
 // Batched form: one persistent launch hashes the chunks of many buffers.  The producer lane
