@@ -411,7 +411,7 @@ LeafArgs leaf_args(const b2d_dedup* d, const RoundState* rs_dev) {
   const MapView m = map_at(d->map_mem, d->map_cap, d->map_size.p);
   return LeafArgs{static_cast<const uint8_t*>(d->data), d->data_len, d->chunk_size, d->n, d->kind, 0, 0,
                   d->tree.p, d->leaflab.p, d->dupflag.p, m, &d->state.p->status, rs_dev,
-                  (uint32_t)d->tune.wait_polls};
+                  (uint32_t)d->tune.wait_polls, 1u};
 }
 
 // ------------------------------------------------------------------------------------------

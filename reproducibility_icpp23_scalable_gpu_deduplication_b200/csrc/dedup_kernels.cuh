@@ -48,6 +48,7 @@ struct LeafArgs {
   const RoundState* rs;
   uint32_t wait_polls;   // 0: the barrier waits' normal bound; else give up after this many
                          // non-blocking polls (a test of the give-up path)
+  uint32_t one;          // 1: the MD5 rounds' multiply-add factor (md5_pre_add)
 };
 
 struct ForestArgs {

@@ -69,36 +69,35 @@ struct Murmur3 {
 // the chain runs through f, one three-input add, the rotate and the add of b; `a` is four steps
 // old, and a + x can be formed off the chain.
 #define B2D_MD5_STEP(f, a, b, c, d, x, t, s) \
-  a = md5_pre_add<SPLIT>(a, (x));            \
+  a = md5_pre_add<SPLIT>(a, (x), one);       \
   a += f(b, c, d) + (t);                     \
   a = ((a << (s)) | (a >> (32 - (s))));      \
   a += b;
 
 // The staged hashing kernels are bound by the integer ALU pipe on MD5 (its logic ops, adds and
-// funnel shifts), while the multiply-add pipe idles.  With SPLIT, a + x is a multiply-add by
-// one, whose factor comes from constant memory so the compiler cannot fold it back into an add;
-// its longer latency is hidden because `a` is ready steps before the chain reaches it.  Measured
-// on the 8 GiB float32 series (256 B chunks): 2.945 against 3.041 ms per hashing launch.  Two
-// other splits were slower: also the on-chain add of b as a multiply-add (4.34 against 3.23 ms
-// per step), and also the rotate as a 32x32->64 multiply by 2^s whose two halves add up to the
-// rotated word (3.59 ms per hashing launch).
-#ifdef __CUDACC__
-static __constant__ uint32_t c_md5_one = 1u;
-#endif
+// funnel shifts).  With SPLIT, a + x, which does not wait for the previous step, is written as a
+// multiply-add by `one`, a 1 the kernel reads from its launch arguments so the compiler cannot
+// fold it back into an add (a 1 from constant memory can be folded).  Measured on the 8 GiB
+// float32 series (256 B chunks): 2.89 against 2.97 ms per hashing launch, with the same
+// instruction count and the ALU pipe at 73.6 % and the FMA pipe at 12.7 % of their peaks either
+// way.  Two other splits were slower: also the on-chain add of b as a multiply-add (4.34 against
+// 3.23 ms per step), and also the rotate as a 32x32->64 multiply by 2^s whose two halves add up
+// to the rotated word (3.59 against 2.95 ms per hashing launch).
 template <int SPLIT>
-__host__ __device__ __forceinline__ uint32_t md5_pre_add(uint32_t a, uint32_t x) {
+__host__ __device__ __forceinline__ uint32_t md5_pre_add(uint32_t a, uint32_t x, uint32_t one) {
 #ifdef __CUDA_ARCH__
   if constexpr (SPLIT != 0) {
     uint32_t r;
-    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(x), "r"(c_md5_one), "r"(a));
+    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(x), "r"(one), "r"(a));
     return r;
   }
 #endif
+  (void)one;
   return a + x;
 }
 
 template <int SPLIT>
-__host__ __device__ __forceinline__ void md5_compress_t(uint32_t st[4], const uint32_t m[16]) {
+__host__ __device__ __forceinline__ void md5_compress_t(uint32_t st[4], const uint32_t m[16], uint32_t one = 1u) {
   uint32_t a = st[0], b = st[1], c = st[2], d = st[3];
   B2D_MD5_STEP(B2D_MD5_F, a, b, c, d, m[0], 0xd76aa478u, 7)
   B2D_MD5_STEP(B2D_MD5_F, d, a, b, c, m[1], 0xe8c7b756u, 12)
@@ -167,7 +166,7 @@ __host__ __device__ __forceinline__ void md5_compress_t(uint32_t st[4], const ui
   st[0] += a; st[1] += b; st[2] += c; st[3] += d;
 }
 __host__ __device__ __forceinline__ void md5_compress(uint32_t st[4], const uint32_t m[16]) {
-  md5_compress_t<0>(st, m);
+  md5_compress_t<0>(st, m, 1u);
 }
 
 

@@ -277,7 +277,8 @@ __device__ __forceinline__ uint32_t swz(uint32_t o) {
 
 // fold the U-byte segment of row `row` of a staged tile into a lane's running digest state
 template <int U, int KIND>
-__device__ __forceinline__ void hash_segment(const uint8_t* stage, uint32_t row, Murmur3& mm, uint32_t md[4]) {
+__device__ __forceinline__ void hash_segment(const uint8_t* stage, uint32_t row, Murmur3& mm, uint32_t md[4],
+                                             uint32_t one) {
   const uint32_t base = row * U;
   if constexpr (KIND == HASH_MD5) {
 #pragma unroll
@@ -288,7 +289,7 @@ __device__ __forceinline__ void hash_segment(const uint8_t* stage, uint32_t row,
         const uint4 v = *reinterpret_cast<const uint4*>(stage + swz<U>(base + blk * 64u + 16u * j));
         m[4 * j + 0] = v.x; m[4 * j + 1] = v.y; m[4 * j + 2] = v.z; m[4 * j + 3] = v.w;
       }
-      md5_compress_t<B2D_MD5_SPLIT>(md, m);
+      md5_compress_t<B2D_MD5_SPLIT>(md, m, one);
     }
   } else {
 #pragma unroll
@@ -392,7 +393,7 @@ __global__ void __launch_bounds__((TMA_CONSUMER_WARPS + 1) * 32)
       const uint32_t s = k % stages, ph = (k / stages) & 1u;
       if (!warp_wait_full(&full[s], ph, a.st, &abort_flag, a.wait_polls)) return;
       const uint8_t* stage = smem + (size_t)s * STAGE_BYTES;
-      if (valid) hash_segment<U, KIND>(stage, row, mm, md);
+      if (valid) hash_segment<U, KIND>(stage, row, mm, md, a.one);
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
     }
@@ -494,6 +495,7 @@ __global__ void __launch_bounds__((TMA_CONSUMER_WARPS + 1) * 32)
   }
 
   const uint32_t row = warp * 32u + lane;
+  const uint32_t one = items[0].args.one;
   Murmur3 mm;
   uint32_t md[4];
   Digest old;
@@ -514,7 +516,7 @@ __global__ void __launch_bounds__((TMA_CONSUMER_WARPS + 1) * 32)
       old.w[0] = old.w[1] = old.w[2] = old.w[3] = 0u;
       if (valid) old = prior_digest(with_round(items[it].args), chunk);
     }
-    if (valid) hash_segment<U, KIND>(smem + (size_t)s * STAGE_BYTES, row, mm, md);
+    if (valid) hash_segment<U, KIND>(smem + (size_t)s * STAGE_BYTES, row, mm, md, one);
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
     if (g + 1 == S && valid) {
