@@ -471,7 +471,11 @@ __device__ __forceinline__ void forest_fast_body(const ForestArgs& a, uint32_t b
     for (int width = 8; width >= 1; width >>= 1) {
       first = (first - 1ull) >> 1;
 #pragma unroll
-      for (int j = 0; j < width; j++) v[j] = combine<PHASE>(a, first + j, v[2 * j], v[2 * j + 1]);
+      for (int j = 0; j < width; j++) {
+        // two FIXED children: an inner node, FIXED in an incremental checkpoint (fixed_or_node)
+        if (PHASE == 2 && !a.baseline && v[2 * j] == FIXED_DUPL && v[2 * j + 1] == FIXED_DUPL) v[j] = FIXED_DUPL;
+        else v[j] = combine<PHASE>(a, first + j, v[2 * j], v[2 * j + 1]);
+      }
     }
     lab = v[0];
   }
@@ -672,6 +676,15 @@ __device__ __forceinline__ void warp1_task(const ForestArgs& a, uint32_t task, u
   wi_flush(a, wi, lane);
 }
 
+// Phase-2 parent of two FIXED children in an incremental checkpoint: FIXED, with nothing pushed
+// or looked up, so the call is skipped.  A task of 512 leaves almost always holds a few scattered
+// shifted copies (0.5 % of the plain series' chunks), so most tasks take the slow path, and most
+// of their nodes are still FIXED pairs.
+__device__ __forceinline__ uint8_t fixed_or_node(const ForestArgs& a, uint32_t x, uint8_t ll, uint8_t rl) {
+  if (!a.baseline && ll == FIXED_DUPL && rl == FIXED_DUPL) return FIXED_DUPL;
+  return forest_node<2>(a, x, ll, rl);
+}
+
 __device__ __forceinline__ void warp2_task(const ForestArgs& a, uint32_t task, uint32_t lane, const uint4& w) {
   const uint64_t root = ((1ull << (a.D - WB2_LEVELS)) - 1ull) + task;
   const uint32_t c0 = task * 512u + 16u * lane;
@@ -693,7 +706,7 @@ __device__ __forceinline__ void warp2_task(const ForestArgs& a, uint32_t task, u
     for (int width = 8; width >= 1; width >>= 1) {
       first = (first - 1ull) >> 1;
 #pragma unroll
-      for (int j = 0; j < width; j++) v[j] = forest_node<2>(a, (uint32_t)(first + j), v[2 * j], v[2 * j + 1]);
+      for (int j = 0; j < width; j++) v[j] = fixed_or_node(a, (uint32_t)(first + j), v[2 * j], v[2 * j + 1]);
     }
     lab = v[0];
   }
