@@ -76,3 +76,17 @@ def test_help_lists_every_option():
     assert r.returncode == 0, r.stderr
     for opt in ("--gpus", "--steps", "--warmup", "--impl", "--form", "--approach", "--workload"):
         assert opt in r.stdout, opt
+
+
+def test_map_headroom_defaults(monkeypatch):
+    """The MD5 series sizes its digest map for all 20 checkpoints at the baseline (about 0.3 N new
+    entries per checkpoint), so no rehash falls in its timed steps; other workloads keep the
+    library's default; an explicit value wins."""
+    bench = load_bench()
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--workload", "md5_f32_8g"])
+    a = bench.parse()
+    assert (a.map_headroom, a.chunk_size, a.nbytes) == (400, 256, 8 << 30)
+    monkeypatch.setattr(sys, "argv", ["bench.py"])
+    assert bench.parse().map_headroom == 0
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--workload", "md5_f32_8g", "--map-headroom", "250"])
+    assert bench.parse().map_headroom == 250
